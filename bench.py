@@ -1,0 +1,337 @@
+"""Throughput benchmark of the B200 RSA worldline packer.
+
+Metric: candidates tested per second (a candidate counts once its
+accept/reject is decided) on seeded synthetic candidate streams.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c3]
+                    [--precision mixed|fp64] [--impl ours|reference]
+
+A step is one complete packing job of the workload (every universe run from
+an empty packing to its stop rule).  Multi-GPU: one process per GPU under
+torchrun; universes / replicas are independent, so ranks shard them with no
+data-path collective (weak scaling) and time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "universe-generator_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+
+
+def workloads(name: str, ug, seed0: int):
+    """Universes of one job.  All inputs are generated from seeds."""
+    U = ug.Universe
+    if name == "c0":  # 1+1D, F=T=16, 20k candidates, seed 0
+        return [U(dim=1, T=16, zgrid=1, excl=1, cross1d=1, seed=seed0, attempts=20000,
+                  round_size=4096)], {"dim": 1, "F": 16, "T": 16, "candidates": 20000}
+    if name == "c1":  # 2+1D, F=T=64, 1M candidates, rounds of 16k
+        return [U(dim=2, T=64, zgrid=1, excl=1, seed=seed0, attempts=1_000_000,
+                  round_size=16384)], {"dim": 2, "F": 64, "T": 64, "candidates": 1_000_000,
+                                       "round": 16384}
+    if name == "c2":  # 3+1D, F=T=128, 5M candidates, rounds of 64k
+        return [U(dim=3, T=128, zgrid=1, excl=1, seed=seed0, attempts=5_000_000,
+                  round_size=65536)], {"dim": 3, "F": 128, "T": 128, "candidates": 5_000_000,
+                                       "round": 65536}
+    if name == "c3":  # 256 universes, d in {1,2,3}, F log-uniform [16,256], caps log-uniform [1e4,1e6]
+        rng = np.random.default_rng(12345)
+        us = []
+        for k in range(256):
+            dim = int(rng.integers(1, 4))
+            F = int(round(math.exp(rng.uniform(math.log(16), math.log(256)))))
+            F = max(16, min(256, F))
+            cap = int(round(math.exp(rng.uniform(math.log(1e4), math.log(1e6)))))
+            us.append(U(dim=dim, T=F, zgrid=1, excl=1, cross1d=int(dim == 1),
+                        seed=(seed0 * 1000003 + k) & (2**64 - 1), attempts=cap,
+                        round_size=16384))
+        tot = sum(u.attempts for u in us)
+        return us, {"universes": 256, "dims": [1, 2, 3], "F": "log-uniform[16,256]",
+                    "caps": "log-uniform[1e4,1e6]", "candidates": tot}
+    if name == "c4":  # 2+1D unique-group mode at F=256, 2M candidates
+        return [U(dim=2, T=256, zgrid=1, excl=1, group_mode=2, seed=seed0, attempts=2_000_000,
+                  round_size=16384)], {"dim": 2, "F": 256, "T": 256, "candidates": 2_000_000,
+                                       "mode": "unique-group"}
+    raise SystemExit(f"unknown workload {name}")
+
+
+def peaks():
+    try:
+        with open(PEAKS_PATH) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return FALLBACK, "fallback"
+
+
+def start_clock_sampler(out_path: str):
+    try:
+        return subprocess.Popen(
+            ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+             "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200",
+             "-i", str(int(os.environ.get("LOCAL_RANK", "0")))],
+            stdout=open(out_path, "w"), stderr=subprocess.DEVNULL)
+    except Exception:
+        return None
+
+
+def clocks_summary(path: str):
+    sm, mx, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    try:
+        for line in open(path):
+            v = [x.strip() for x in line.split(",")]
+            if len(v) < 9:
+                continue
+            try:
+                sm.append(float(v[1]))
+                mx.append(float(v[2]))
+            except ValueError:
+                continue
+            for n, val in zip(names, v[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(n)
+    except FileNotFoundError:
+        pass
+    if not sm:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+    return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def cpu_baseline(us, budget_s: float = 20.0):
+    """The oracle (plain-C restatement of the reference path), threaded batch
+    prefilter + in-order recheck on all host cores, on a bounded sample."""
+    import oracle as O
+
+    u = us[0]
+    m = O.Model(dim=u.dim, T=u.T, rng=u.rng, zgrid=u.zgrid, excl=u.excl, cross1d=u.cross1d,
+                pin=u.pin_sin1, seed=u.seed)
+    cores = os.cpu_count() or 1
+    n = 20000
+    while True:
+        t0 = time.perf_counter()
+        O.pack(m, n, nthreads=cores, round_size=16384)
+        dt = time.perf_counter() - t0
+        if dt > budget_s / 4 or n >= u.attempts:
+            break
+        n = min(u.attempts, int(n * max(2.0, budget_s / 4 / max(dt, 1e-3))))
+    return {"value": n / dt, "unit": "candidates/s", "cores": cores, "kind": "port",
+            "sample": f"first {n} candidates of universe 0 (dim={u.dim}, F=T={u.T}), "
+                      f"oracle threaded prefilter + in-order recheck, {dt:.1f} s"}
+
+
+def reference_arm(args, rank, world):
+    """The reference's own CPU path: reference cuda/braid_knot.cu propose() compiled
+    from the reference source (oracle/_ref/knot_host), all host threads."""
+    if rank != 0:
+        return 0
+    import oracle as O
+    import ugb200
+
+    us, cfg = workloads(args.workload, ugb200, 0)
+    u = us[0]
+    exe = os.path.join(O.REF_DIR, "knot_host")
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/knot_host not built"}))
+        return 0
+    cores = os.cpu_count() or 1
+    n = 20000
+    vals = []
+    for step in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        r = subprocess.run([exe, "--mode", "pack", "-t", str(u.T), "--dim", str(max(1, u.dim)),
+                            "--seed", str(step), "--attempts", str(n), "--threads", str(cores),
+                            "--round", "16384"], capture_output=True, text=True, check=True)
+        dt = time.perf_counter() - t0
+        if step == 0:  # size the sample to ~10 s of CPU work
+            n = max(20000, min(u.attempts, int(n * 10.0 / max(dt, 1e-3))))
+            continue
+        if step >= args.warmup:
+            vals.append(n / dt)
+    v = float(np.median(vals)) if vals else 0.0
+    line = {"metric": "candidates tested/s", "value": v, "unit": "candidates/s",
+            "higher_is_better": True, "impl": "reference", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, **cfg},
+            "cpu_baseline": {"value": v, "unit": "candidates/s", "cores": cores,
+                             "kind": "reference",
+                             "sample": f"{n} candidates per step of universe 0 (dim={u.dim}, T={u.T}); "
+                                       "reference braid_knot.cu propose() + its eval/collide "
+                                       "loop, threaded prefilter + in-order recheck"},
+            "e2e": {"value": v, "unit": "candidates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="c1")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+
+    import torch
+
+    import ugb200
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    prec = ugb200.PREC_MIXED if args.precision == "mixed" else ugb200.PREC_FP64
+    us, cfg = workloads(args.workload, ugb200, 1000 * rank)
+    if len(us) > 1 and world > 1:  # shard universes across ranks (weak: each rank the full list)
+        pass
+    stream = torch.cuda.Stream()
+    try:
+        packer = ugb200.Packer(us, precision=prec, device=local, stream=stream.cuda_stream,
+                               rounds_per_sync=8, use_graph=True)
+    except ugb200.UgError as e:
+        if prec == ugb200.PREC_MIXED and e.code == ugb200._lib.UG_ENOTSUP:
+            prec = ugb200.PREC_FP64
+            packer = ugb200.Packer(us, precision=prec, device=local, stream=stream.cuda_stream,
+                                   rounds_per_sync=8, use_graph=True)
+        else:
+            raise
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    total_cands = sum(u.attempts for u in us)
+
+    def seeds(step):
+        return [(u.seed + 7919 * (step + 1)) & (2**64 - 1) for u in us]
+
+    # warm-up
+    for w in range(args.warmup):
+        packer.reset(seeds(w)).run()
+    torch.cuda.synchronize()
+
+    # device-timed steps (inputs resident, L2 flushed between steps)
+    clk_path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "/tmp",
+                            f"clocks_rank{rank}.csv")
+    sampler = start_clock_sampler(clk_path)
+    times = []
+    cands = 0
+    launches0 = packer.counters()[0]
+    for s in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.random_(0, 255)
+        stream.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        packer.reset(seeds(args.warmup + s)).run()
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+        cands += sum(packer.stats(k).attempts for k in range(len(us)))
+    launches = packer.counters()[0] - launches0
+    if sampler:
+        sampler.terminate()
+        sampler.wait()
+    t_ms = float(sum(times))
+    if dist:
+        t = torch.tensor([t_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+        c = torch.tensor([float(cands)], device="cuda")
+        dist.all_reduce(c)
+        cands = int(c.item())
+    value = cands / (t_ms / 1000.0)
+
+    # end to end through the public API with host buffers
+    e2e_t = 0.0
+    e2e_c = 0
+    _, h2d0, d2h0 = packer.counters()
+    for s in range(max(1, args.steps // 2)):
+        t0 = time.perf_counter()
+        packer.reset(seeds(100 + s)).run()
+        acc = [packer.accepted(k)[0] for k in range(len(us))]
+        e2e_t += time.perf_counter() - t0
+        e2e_c += sum(packer.stats(k).attempts for k in range(len(us)))
+        del acc
+    _, h2d1, d2h1 = packer.counters()
+    nrep = max(1, args.steps // 2)
+    e2e = {"value": e2e_c / e2e_t, "unit": "candidates/s",
+           "h2d_bytes_per_step": (h2d1 - h2d0) // nrep, "d2h_bytes_per_step": (d2h1 - d2h0) // nrep}
+
+    # per-kernel timing pass (events around each launch on the packer's stream)
+    timer = ugb200.Packer(us, precision=prec, device=local, stream=stream.cuda_stream,
+                          rounds_per_sync=8, use_graph=False, kernel_timing=True)
+    timer.reset(seeds(args.warmup)).run()
+    kt = timer.kernel_times()
+    st = [timer.stats(k) for k in range(len(us))]
+    timer.close()
+    pk_name = "k_prefilter_mixed" if prec == ugb200.PREC_MIXED else "k_prefilter64"
+    pk_ms, pk_n = kt.get(pk_name, (0.0, 0))
+    evals = sum(s.evals for s in st)
+    flops = sum(2 * u.dim * ((u.T - 1) + u.T // 2) * s.evals for u, s in zip(us, st))
+    P, src = peaks()
+    achieved = flops / (pk_ms / 1000.0) / 1e12 if pk_ms > 0 else 0.0
+    peak = P["bf16_tflops"]
+    roofline = {"bound": "tensor", "kernel": pk_name, "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
+                "peak_source": f"{src} bf16 dense (burst)",
+                "launches": pk_n, "avg_launch_ms": pk_ms / max(pk_n, 1),
+                "evals": evals, "kernel_share": {k: v[0] for k, v in kt.items()}}
+
+    if rank == 0:
+        line = {"metric": "candidates tested/s", "value": value, "unit": "candidates/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None,
+                "dtype": "bf16x3+f32+f64" if prec == ugb200.PREC_MIXED else "f64",
+                "data": "synthetic (seeded Philox candidate streams)",
+                "config": {"workload": args.workload, **cfg,
+                           "precision": "mixed" if prec == ugb200.PREC_MIXED else "fp64",
+                           "l2": "flushed between steps (256 MiB write)",
+                           "parallelism": f"replicas x{world}"},
+                "e2e": e2e, "gpu_launches": launches,
+                "roofline": roofline,
+                "clocks": clocks_summary(clk_path)}
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(us)
+        print(json.dumps(line))
+    packer.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

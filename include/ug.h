@@ -1,0 +1,177 @@
+/* ug.h -- C ABI of the B200 RSA worldline packer (libug.so).
+ *
+ * Plain C types only; no torch or CUDA types in the signatures.  Every call
+ * returns a status (UG_OK or a UG_E* code) and never exits the process; the
+ * message of the last failure on the calling thread is in ug_last_error().
+ *
+ * Each entry point replaces one interface of the reference engines
+ * (universe-analysis/universe-generator); the reference location is cited
+ * beside it.  The reference engines are standalone programs driven through
+ * argv, stderr and CSV files (braidlab/engine.py:50-112); this library is the
+ * in-process form of the same contract, and ugb200.cli wraps it back into a
+ * braid_cuda-compatible command line.
+ */
+#ifndef UG_H
+#define UG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the engines' fail-fast exits, cuda/braid_cuda.cu:597-636) */
+#define UG_OK 0
+#define UG_EINVAL 1     /* bad configuration (flag validation, braid_cuda.cu:597-636) */
+#define UG_ENOMEM 2     /* device allocation failed */
+#define UG_ECAP 3       /* a capacity was exceeded (never a silent drop) */
+#define UG_ECUDA 4      /* CUDA runtime error */
+#define UG_ETIMEDOUT 5  /* a bounded device wait gave up */
+#define UG_ENOTSUP 6    /* combination not supported */
+
+/* ---- model conventions */
+#define UG_RNG_PHILOX 0 /* counter-based Philox4x32-10 candidate stream (this packer) */
+#define UG_RNG_KNOT 1   /* xoshiro256** per attempt index, cuda/braid_knot.cu:207 */
+#define UG_ZGRID_REF 0  /* z_t = (t+1) pi / (T+1), cuda/braid_cuda.cu:653-660 */
+#define UG_ZGRID_MID 1  /* z_t = (t+1/2) pi / T */
+#define UG_EXCL_REF 0   /* Chebyshev |d| <= 2/T per timestep, cuda/braid_cuda.cu:451,604 */
+#define UG_EXCL_OPEN 1  /* Chebyshev |d| <  1/F per timestep */
+#define UG_GROUP_NONE 0    /* unique packing */
+#define UG_GROUP_SUBPATH 1 /* uniques, then subpaths joining one group (--subpaths,
+                              cuda/braid_cuda.cu:46-58, 949-1043) */
+#define UG_GROUP_UNIQUE 2  /* one phase: no contact founds a group, one group joins,
+                              two or more reject */
+#define UG_PREC_FP64 0  /* plain FP64 single-pass prefilter */
+#define UG_PREC_MIXED 1 /* tensor-core split-BF16 prefilter + FP64 guard-band retest */
+
+/* One universe (one reference engine run).  Mirrors the engine flags
+ * -t, --terms, --seed, --attempts, --max-n, --until-accept-rate, --pin-sin1,
+ * --subpaths, --sub-attempts, --sub-until-accept-rate
+ * (cuda/braid_cuda.cu:534-584; cuda/braid_cuda3d.cu:862-913). */
+typedef struct ug_universe_cfg {
+    int32_t dim;        /* spatial axes, 1..3 (braid_cuda: 2, braid_cuda3d: 3) */
+    int32_t T;          /* timesteps; the max frequency is T (braid_cuda.cu:597-603) */
+    int32_t terms;      /* sinusoid terms per axis incl. sin1; 0 = full band (T) */
+    int32_t rng;        /* UG_RNG_* */
+    int32_t zgrid;      /* UG_ZGRID_* */
+    int32_t excl;       /* UG_EXCL_* */
+    int32_t cross1d;    /* 1+1D: also reject a sign change of the separation between steps */
+    int32_t pin_sin1;   /* --pin-sin1 (braid_cuda.cu:170-188) */
+    int32_t group_mode; /* UG_GROUP_* */
+    int32_t round_size; /* candidates per round; 0 = 65536.  Results do not depend on it */
+    uint64_t seed;
+    int64_t attempts;     /* candidate budget of phase 1 */
+    int64_t max_n;        /* --max-n: phase-1 unique cap (0 = off) */
+    int64_t sub_attempts; /* --sub-attempts (0 = same as attempts) */
+    double accept_rate;   /* --until-accept-rate (0 = off), braid_cuda.cu:931-943 */
+    double sub_accept_rate;
+} ug_universe_cfg;
+
+typedef struct ug_run_opts {
+    int32_t precision;       /* UG_PREC_* */
+    int32_t device;          /* CUDA device ordinal (-1 = current) */
+    int32_t rounds_per_sync; /* rounds per CUDA-graph replay / host status check (0 = 8) */
+    int32_t use_graph;       /* capture the round sequence as a CUDA graph */
+    int32_t kernel_timing;   /* record per-kernel CUDA events (no graph) */
+    int32_t force_hash;      /* 1 = hashed collision grid even where a dense one fits */
+    uint64_t stream;         /* cudaStream_t to run on (0 = library-owned stream) */
+    int64_t slot_hint;       /* initial accepted-path capacity per universe (0 = auto) */
+} ug_run_opts;
+
+/* Per-universe result (the engine's stderr "done:" line and curve end point,
+ * braid_cuda.cu:945, 1039-1042). */
+typedef struct ug_stats {
+    int64_t n;          /* accepted paths (uniques + subpaths) */
+    int64_t n_unique;   /* uniques / groups founded */
+    int64_t n_sub;      /* subpaths */
+    int64_t attempts;   /* candidates decided (all phases) */
+    int64_t phase1_end; /* first candidate index of the subpath phase */
+    int64_t rounds;
+    int64_t gray;       /* mixed precision: candidates re-tested in FP64 */
+    int64_t evals;      /* prefilter position evaluations (candidate x timestep) */
+    int64_t evals_fp64; /* of which in FP64 */
+    int32_t state;      /* 1 = done */
+    int32_t grid_kind;  /* 0 dense, 1 hash */
+} ug_stats;
+
+/* Per-kernel device time accumulated while kernel_timing is on. */
+typedef struct ug_kernel_times {
+    double ms[12];
+    int64_t launches[12];
+    const char* names[12];
+} ug_kernel_times;
+
+/* Library version (ABI revision). */
+int ug_version(void);
+
+/* Message of the last failure on this thread; returns its length. */
+int ug_last_error(char* buf, size_t len);
+
+/* Create a batch of independent universes on one GPU (replaces one engine
+ * process per job, braidlab/orchestrator.py:85-147).  The library owns all
+ * device memory inside the handle. */
+int ug_batch_create(const ug_universe_cfg* cfgs, int32_t n, const ug_run_opts* opts, void** out);
+
+/* Run every universe to its stop rule (the round loops of
+ * cuda/braid_cuda.cu:885-944 and :949-1043, cuda/braid_knot.cu:401-469).
+ * max_rounds > 0 bounds the number of rounds; returns UG_OK while work
+ * remains (check ug_batch_done). */
+int ug_batch_run(void* h, int64_t max_rounds);
+
+/* Restart every universe from an empty packing, keeping all allocations;
+ * seeds (n values, may be NULL) replace the candidate-stream seeds.  A fresh
+ * engine run per job (braidlab/orchestrator.py:85-147) without re-allocation. */
+int ug_batch_reset(void* h, const uint64_t* seeds);
+
+/* 1 when every universe has stopped, 0 otherwise (negative on error). */
+int ug_batch_done(void* h);
+
+/* Result counters of universe u (braid_cuda.cu:945 "done: N=.. in .. attempts"). */
+int ug_batch_stats(void* h, int32_t u, ug_stats* out);
+
+/* Accepted candidate indices (admission order) and group ids of universe u.
+ * Size query: pass cap = 0 and read *n. */
+int ug_batch_accepted(void* h, int32_t u, int64_t* idx, int32_t* gid, int64_t cap, int64_t* n);
+
+/* Wrapped comoving positions [n][dim][T] of the accepted paths (FP64),
+ * the trajectories evalPath fills (braid_cuda.cu:831-862). */
+int ug_batch_positions(void* h, int32_t u, double* pos, int64_t cap_paths);
+
+/* Worldline parameters of the accepted paths, the --dump-params content
+ * (braid_cuda.cu:1062-1104; braid_cuda3d.cu:1578-1613): per path and axis
+ * a2, then nw terms of (a, b, f) in term order. a2 [n][dim], a/f [n][dim][nw],
+ * b [n][dim][nw]. */
+int ug_batch_params(void* h, int32_t u, double* a2, double* a, int32_t* b, double* f,
+                    int64_t cap_paths);
+
+/* Per-kernel device times (kernel_timing = 1). */
+int ug_batch_kernel_times(void* h, ug_kernel_times* out);
+
+/* Kernels launched by the batch so far and bytes it copied host->device and
+ * device->host (cumulative). */
+int ug_batch_counters(void* h, int64_t* launches, int64_t* h2d_bytes, int64_t* d2h_bytes);
+
+/* Reset the per-kernel timers. */
+int ug_batch_reset_times(void* h);
+
+/* Maximum |X_mixed - X_fp64| of the tensor-core evaluation over the first
+ * `count` candidates of universe u (all timesteps and axes): the achieved
+ * position error of the mixed-precision prefilter against FP64.  Also
+ * returns the guard margin the prefilter applies. */
+int ug_batch_mixed_error(void* h, int32_t u, int64_t first, int64_t count, double* max_err,
+                         double* margin);
+
+/* Release all device memory of the batch. */
+int ug_batch_destroy(void* h);
+
+/* ---- single-universe convenience: a batch of one (the ug_pack_* surface) */
+int ug_pack_create(const ug_universe_cfg* cfg, const ug_run_opts* opts, void** out);
+int ug_pack_run(void* h);
+int ug_pack_stats(void* h, ug_stats* out);
+int ug_pack_destroy(void* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,132 @@
+"""GPU parity: the packer's accepted sets against the CPU oracle (exact),
+trajectories and parameters within FP64 tolerance."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+POS_TOL = 1e-12   # FP64: device libm vs host libm, fma vs separate mul/add
+PAR_TOL = 1e-14
+
+
+def _model(O, u):
+    return O.Model(dim=u.dim, T=u.T, terms=u.terms, rng=u.rng, zgrid=u.zgrid, excl=u.excl,
+                   cross1d=u.cross1d, pin=u.pin_sin1, seed=u.seed)
+
+
+def _check(ug, O, u, precision=0, **kw):
+    res = O.pack(_model(O, u), u.attempts, max_n=u.max_n, group_mode=u.group_mode,
+                 sub_attempts=u.sub_attempts)
+    with ug.Packer([u], precision=precision, **kw) as p:
+        p.run()
+        st = p.stats(0)
+        idx, gid = p.accepted(0)
+        assert st.done
+        assert np.array_equal(idx, res.acc_idx), (len(idx), len(res.acc_idx))
+        assert st.attempts == res.attempts
+        if u.group_mode:
+            assert np.array_equal(gid, res.gid)
+            assert (st.n_unique, st.n_sub) == (res.n_unique, res.n_sub)
+        pos = p.positions(0)
+        m = _model(O, u)
+        for k in range(0, len(idx), max(1, len(idx) // 16)):
+            ref = O.positions(m, int(idx[k]))
+            dd = np.abs(pos[k] - ref)
+            dd = np.minimum(dd, 2 - dd)   # wrapped coordinates
+            assert dd.max() < POS_TOL
+        par = p.params(0)
+        for k in range(0, len(idx), max(1, len(idx) // 8)):
+            c = O.candidate(m, int(idx[k]))
+            assert np.array_equal(par["b"][k], c["b"])
+            np.testing.assert_allclose(par["a"][k], c["a"], rtol=PAR_TOL, atol=1e-300)
+            np.testing.assert_allclose(par["f"][k], c["f"], rtol=PAR_TOL, atol=1e-300)
+            np.testing.assert_allclose(par["a2"][k], c["a2"], rtol=0, atol=1e-15)
+        return st, idx
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+@pytest.mark.parametrize("rng", [0, 1])
+def test_parity_ref_conventions(ug, oracle, dim, rng):
+    u = ug.Universe(dim=dim, T=16, rng=rng, seed=100 + dim, attempts=30000, round_size=4096)
+    _check(ug, oracle, u)
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+def test_parity_open_mid_conventions(ug, oracle, dim):
+    u = ug.Universe(dim=dim, T=16, zgrid=1, excl=1, cross1d=int(dim == 1), seed=7 * dim,
+                    attempts=20000, round_size=2048)
+    _check(ug, oracle, u)
+
+
+def test_parity_reference_golden_knot(ug, oracle):
+    """The reference's own deterministic packer stream and accepted set (fixture)."""
+    import json
+    import os
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "knot_reference.json")))
+    for p in gold["packs"]:
+        u = ug.Universe(dim=p["dim"], T=p["T"], terms=p["terms"], rng=1, pin_sin1=p["pin"],
+                        seed=p["seed"], attempts=p["attempts"], round_size=4096)
+        with ug.Packer([u]) as pk:
+            pk.run()
+            idx, _ = pk.accepted(0)
+        assert list(idx) == p["idx"], (p["T"], p["dim"])
+
+
+def test_round_size_independence(ug, oracle):
+    u = ug.Universe(dim=2, T=24, seed=5, attempts=60000, round_size=65536)
+    _, a = _check(ug, oracle, u)
+    for rs in (128, 1024):
+        u2 = ug.Universe(dim=2, T=24, seed=5, attempts=60000, round_size=rs)
+        with ug.Packer([u2]) as p:
+            p.run()
+            b, _ = p.accepted(0)
+        assert np.array_equal(a, b)
+
+
+def test_hash_grid_and_growth(ug, oracle):
+    u = ug.Universe(dim=3, T=20, seed=9, attempts=30000, round_size=8192)
+    _check(ug, oracle, u, force_hash=True, slot_hint=1024)
+
+
+def test_graph_and_eager_agree(ug, oracle):
+    u = ug.Universe(dim=2, T=16, seed=3, attempts=40000, round_size=1024)
+    s1, a = _check(ug, oracle, u, use_graph=True, rounds_per_sync=4)
+    s2, b = _check(ug, oracle, u, use_graph=False)
+    assert np.array_equal(a, b)
+
+
+def test_max_n_stop(ug, oracle):
+    u = ug.Universe(dim=2, T=16, seed=1, attempts=100000, max_n=20, round_size=2048)
+    st, idx = _check(ug, oracle, u)
+    assert st.n == 20
+
+
+def test_group_subpath_mode(ug, oracle):
+    u = ug.Universe(dim=2, T=12, seed=4, attempts=3000, group_mode=1, sub_attempts=20000,
+                    round_size=1024)
+    st, _ = _check(ug, oracle, u)
+    assert st.n_sub > 0
+
+
+def test_group_unique_mode(ug, oracle):
+    u = ug.Universe(dim=2, T=16, zgrid=1, excl=1, seed=8, attempts=20000, group_mode=2,
+                    round_size=2048)
+    st, _ = _check(ug, oracle, u)
+    assert st.n_sub > 0
+
+
+def test_batched_universes_match_single(ug, oracle):
+    rng = np.random.default_rng(0)
+    us = []
+    for k in range(12):
+        dim = int(rng.integers(1, 4))
+        T = int(rng.choice([8, 12, 16, 24]))
+        us.append(ug.Universe(dim=dim, T=T, zgrid=1, excl=1, cross1d=int(dim == 1), seed=k,
+                              attempts=int(rng.integers(2000, 20000)), round_size=2048))
+    with ug.Packer(us) as p:
+        p.run()
+        for k, u in enumerate(us):
+            idx, _ = p.accepted(k)
+            ref = oracle.pack(_model(oracle, u), u.attempts)
+            assert np.array_equal(idx, ref.acc_idx), k

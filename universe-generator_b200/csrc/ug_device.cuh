@@ -1,0 +1,419 @@
+// ug_device.cuh -- device-side model of the RSA worldline packer.
+//
+// A worldline axis is x(z) = sum_b a_b [sin(b z + f_b) - sin f_b] + a2 sin z
+// (cuda/braid_cuda.cu:8-16).  The packer evaluates the comoving position
+// X(z_t) = x(z_t) / sin z_t in the sine basis
+//     X_t = wrap( a2 + invsinz_t * sum_{b=2..F} (alpha_b S_bt + beta_b Cm_bt) )
+// with alpha_b = a_b cos f_b, beta_b = a_b sin f_b (zero for odd b),
+// S_bt = sin(b z_t) and Cm_bt = cos(b z_t) - 1 (host-built FP64 tables, the
+// table form of cuda/braid_knot.cu:211-230).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ug {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr int kMaxF = 256;        // max frequency / timesteps per universe
+constexpr int kTile = 128;        // candidates per prefilter tile
+enum : int { kConflictCap = 48 };  // earlier in-round conflicts kept per survivor
+enum : int { kSmaxCap = 4096 };    // survivors resolved per universe per round (max)
+constexpr uint32_t kEmptyKey32 = 0xffffffffu;
+constexpr uint64_t kEmptyKey = ~0ull;
+
+enum RngMode : int32_t { RNG_PHILOX = 0, RNG_KNOT = 1 };
+enum GroupMode : int32_t { GROUP_NONE = 0, GROUP_SUBPATH = 1, GROUP_UNIQUE = 2 };
+enum GridKind : int32_t { GRID_DENSE = 0, GRID_HASH = 1 };
+
+// Universe state flags (UniCtl::state)
+enum : int32_t { ST_ACTIVE = 0, ST_DONE = 1, ST_GROW = 2, ST_ERROR = 3 };
+
+// One accepted (or in-round survivor) point: FP64 position, chain link, group.
+struct __align__(32) Pt64 {
+    double c[3];
+    int32_t next;
+    int32_t gid;
+};
+// FP32 copy used by the mixed-precision prefilter.
+struct __align__(16) Pt32 {
+    float c[3];
+    int32_t next;
+};
+
+// Read-only per-universe description (device copy lives in UniDev array).
+struct UniDev {
+    // model
+    int32_t dim, T, F, nw;
+    int32_t rng, inclusive, cross1d, pin;
+    int32_t group_mode;  // GroupMode; GROUP_SUBPATH runs phase 1 as NONE then 2 as SUBPATH
+    int32_t gw;          // cells per axis
+    uint64_t seed;
+    double cell;         // exclusion radius == cell width
+    uint32_t modmax;     // knot: frequencies drawn in [2, modmax+1]
+    int32_t B_max;       // candidates per round cap
+    int32_t S_max;       // survivors per round cap
+    int32_t pad0;
+    // tables
+    const double* S;       // [(F+1) * T]
+    const double* Cm;      // [(F+1) * T]
+    const double* invsinz; // [T]
+    const int32_t* order;  // [T] endpoint-first
+    // main grid
+    int32_t grid_kind;
+    int32_t pad1;
+    int32_t* heads;        // dense: [T * gw^dim]; hash: values [hcap]
+    uint64_t* hkeys;       // hash keys [hcap]
+    uint64_t hmask;        // hcap - 1
+    // accepted points
+    Pt64* pts;             // [slot_cap * T]
+    Pt32* ptf;             // [slot_cap * T]
+    int64_t slot_cap;
+    // per-round buffers
+    uint32_t* surv_bits;   // [B_max / 32]
+    uint32_t* gray_bits;   // [B_max / 32]
+    int32_t* g0;           // [B_max]  group mode: single pre-round group touched (-1 none)
+    int32_t* surv_off;     // [S_max]  candidate offset within the round
+    Pt64* spos;            // [S_max * T]
+    uint64_t* rkeys;       // round hash keys [rcap]: epoch<<40 | t<<31 | cell
+    uint64_t* rvals;       // [rcap]: epoch<<32 | head survivor rank
+    uint64_t rmask;
+    int32_t* ccount;       // [S_max]
+    int32_t* clist;        // [S_max * kConflictCap]
+    int32_t* sgid;         // [S_max]  resolved group / -1 rejected, -2 unresolved
+    int32_t* acc_rank;     // [S_max]  slot offset of accepted survivors, -1 otherwise
+    int64_t* acc_idx;      // [slot_cap] candidate index of each accepted slot
+};
+
+// Mutable per-universe control block (device).
+struct UniCtl {
+    int64_t next_cand;     // first candidate of the next round
+    int64_t phase_end;     // candidate index where the current phase ends
+    int64_t sub_budget;    // GROUP_SUBPATH: candidates of phase 2
+    int64_t max_n;         // phase-1 unique cap (0 = off)
+    int64_t round_base;    // this round: candidates [round_base, round_base + B)
+    int64_t n_slots;       // accepted paths (== slots used)
+    int64_t n_unique, n_sub;
+    int64_t attempts;      // candidates fully decided
+    int64_t phase1_end;
+    int32_t B;             // this round's candidate count
+    int32_t round_B;       // adaptive round size
+    int32_t S;             // survivors this round (after truncation)
+    int32_t S_raw;         // survivors found by the prefilter
+    int32_t trunc;         // survivor rank where the round was truncated (S if none)
+    int32_t phase;         // 1 or 2
+    int32_t state;         // ST_*
+    int32_t epoch;         // round-hash epoch
+    int32_t n_gray;        // mixed: candidates sent to the FP64 retest this round
+    int32_t accepted_round;
+    int64_t gray_total;    // mixed: FP64 retests over the run
+    int64_t rounds;
+    int64_t hash_used;     // main grid hash entries in use
+    int64_t n_slots_prev;  // n_slots before this round's commit
+    int64_t evals;         // prefilter (candidate, timestep) position evaluations
+    int64_t evals_fp64;    // of which evaluated in FP64 (plain path / guard-band retest)
+    int32_t stop_at;       // survivors [0, stop_at) resolved this round
+    int32_t pad2;
+    int32_t B_min, B_cap;  // round-size adaptation bounds
+    int32_t err_code;
+    int32_t pad;
+    // windowed accept-rate stop (braid_cuda.cu:931-943): a ring of buckets of
+    // (attempts, admitted); a bucket closes once it holds win_target/32 attempts
+    double accept_rate;     // phase 1 threshold (0 = off)
+    double sub_accept_rate; // phase 2 threshold (0 = off)
+    int64_t win_target, win_att, win_adm;
+    int32_t win_head, win_len;
+    int64_t win_b[64];
+    int64_t win_a[64];
+};
+
+// ------------------------------------------------------------------ helpers
+
+__host__ __device__ __forceinline__ double torus_wrap(double x) {
+    return x - 2.0 * floor((x + 1.0) * 0.5);
+}
+__host__ __device__ __forceinline__ double torus_delta(double d) {
+    if (d > 1.0) return d - 2.0;
+    if (d < -1.0) return d + 2.0;
+    return d;
+}
+__device__ __forceinline__ float torus_wrapf(float x) {
+    return x - 2.0f * floorf((x + 1.0f) * 0.5f);
+}
+__device__ __forceinline__ float torus_deltaf(float d) {
+    if (d > 1.0f) return d - 2.0f;
+    if (d < -1.0f) return d + 2.0f;
+    return d;
+}
+__device__ __forceinline__ int cell_of(double X, double cell, int gw) {
+    int c = (int)floor((X + 1.0) / cell);
+    return c >= gw ? gw - 1 : (c < 0 ? 0 : c);
+}
+__device__ __forceinline__ bool hit1(double d, double cell, int inclusive) {
+    const double ad = fabs(d);
+    return inclusive ? ad <= cell : ad < cell;
+}
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: as
+// easy as 1, 2, 3", SC'11): 10 rounds of the 4x32 S-box with Weyl key bumps.
+__host__ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        if (r) {
+            k.x += 0x9E3779B9u;
+            k.y += 0xBB67AE85u;
+        }
+#ifdef __CUDA_ARCH__
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+#else
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c.x, p1 = (uint64_t)0xCD9E8D57u * c.z;
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+#endif
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    }
+    return c;
+}
+
+// Counter layout of the Philox candidate stream: block p of axis ax of
+// candidate idx.  Block 0 carries a2; block p >= 1 the frequency pair (2p, 2p+1).
+__host__ __device__ __forceinline__ uint4 philox_block(uint64_t seed, uint64_t idx, int ax, int p) {
+    return philox4x32_10(make_uint4((uint32_t)idx, (uint32_t)(idx >> 32),
+                                    ((uint32_t)ax << 16) | (uint32_t)p, 0u),
+                         make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+}
+
+// xoshiro256** + splitmix64 seeding: the reference's per-candidate stream
+// (cuda/braid_knot.cu:56-90, seeded per attempt index as braid_knot.cu:207).
+struct Xo {
+    uint64_t s[4];
+    __device__ __forceinline__ void seed(uint64_t sd) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            sd += 0x9E3779B97F4A7C15ULL;
+            uint64_t z = sd;
+            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+            z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+            s[i] = z ^ (z >> 31);
+        }
+    }
+    __device__ __forceinline__ uint64_t next() {
+        const uint64_t x = s[1] * 5;
+        const uint64_t result = ((x << 7) | (x >> 57)) * 9;
+        const uint64_t t = s[1] << 17;
+        s[2] ^= s[0];
+        s[3] ^= s[1];
+        s[1] ^= s[2];
+        s[0] ^= s[3];
+        s[2] ^= t;
+        s[3] = (s[3] << 45) | (s[3] >> 19);
+        return result;
+    }
+    __device__ __forceinline__ double f64() { return (double)(next() >> 11) * (1.0 / 9007199254740992.0); }
+    __device__ __forceinline__ uint32_t below(uint32_t n) { return (uint32_t)(next() % n); }
+    __device__ __forceinline__ bool flip() { return next() & 1ULL; }
+};
+__device__ __forceinline__ uint64_t knot_seed(uint64_t seed, uint64_t idx) {
+    return seed ^ (idx * 0x9E3779B97F4A7C15ULL + 0x1234567ULL);
+}
+
+// ------------------------------------------------- FP64 candidate generation
+// Writes the canonical coefficients of one axis into alpha/beta [F+1]
+// (indices 2..F used) and returns a2.  `stride` lets the arrays live in
+// shared memory interleaved across threads.
+
+// Philox stream: E_b = -log((r + 1/2) 2^-32), w_b = E_b / sum_b E_b (ascending
+// b), a_b = +-w_b / b, f_b = (r >> 1) 2^-31 pi on even b, a2 = r 2^-31 - 1.
+__device__ __forceinline__ double gen_philox64(const UniDev& U, uint64_t idx, int ax, double* alpha,
+                                               double* beta, int stride) {
+    const int F = U.F;
+    double a2 = 0.0;
+    double sum = 0.0;
+    for (int p = 0; 2 * p <= F; p++) {
+        const uint4 o = philox_block(U.seed, idx, ax, p);
+        if (p == 0) {
+            a2 = U.pin ? 0.0 : (double)o.x * (1.0 / 2147483648.0) - 1.0;
+            continue;
+        }
+        const int be = 2 * p, bo = 2 * p + 1;
+        const double Ee = -log(((double)o.x + 0.5) * (1.0 / 4294967296.0));
+        sum += Ee;
+        alpha[be * stride] = (o.z & 1u) ? -Ee : Ee;  // sign folded in, phase parked in beta
+        beta[be * stride] = (double)(o.z >> 1) * (1.0 / 2147483648.0) * kPi;
+        if (bo <= F) {
+            const double Eo = -log(((double)o.y + 0.5) * (1.0 / 4294967296.0));
+            sum += Eo;
+            alpha[bo * stride] = (o.w & 1u) ? -Eo : Eo;
+        }
+    }
+    for (int b = 2; b <= F; b++) {
+        const double e = alpha[b * stride];
+        double amp = fabs(e) / sum / (double)b;
+        if (e < 0.0 || (e == 0.0 && signbit(e))) amp = -amp;
+        if (b & 1) {
+            alpha[b * stride] = amp;
+            beta[b * stride] = 0.0;
+        } else {
+            double sf, cf;
+            sincos(beta[b * stride], &sf, &cf);
+            alpha[b * stride] = amp * cf;
+            beta[b * stride] = amp * sf;
+        }
+    }
+    return a2;
+}
+
+// Knot stream (reference draw order, cuda/braid_knot.cu:111-166) for ALL axes.
+// bj/aj/fj: scratch [nw] per axis (stride applies), coefficients accumulated
+// into alpha/beta [dim][F+1] (row pitch F+1, stride applies).
+__device__ inline void gen_knot64(const UniDev& U, uint64_t idx, double* alpha, double* beta,
+                                  double* a2, int32_t* bj, double* wj, int stride) {
+    Xo r;
+    r.seed(knot_seed(U.seed, idx));
+    const int nw = U.nw, F = U.F;
+    for (int ax = 0; ax < U.dim; ax++) {
+        double* al = alpha + (size_t)ax * (F + 1) * stride;
+        double* bt = beta + (size_t)ax * (F + 1) * stride;
+        for (int b = 0; b <= F; b++) al[b * stride] = bt[b * stride] = 0.0;
+        if ((uint32_t)nw == U.modmax) {
+            for (int j = 0; j < nw; j++) bj[j * stride] = j + 2;
+            for (int j = nw - 1; j > 0; j--) {
+                const int k = (int)r.below((uint32_t)(j + 1));
+                const int32_t tmp = bj[j * stride];
+                bj[j * stride] = bj[k * stride];
+                bj[k * stride] = tmp;
+            }
+        } else {
+            for (int j = 0; j < nw; j++) {
+                int bnew = 0;
+                bool dup = true;
+                for (int guard = 0; dup && guard < 64; guard++) {
+                    bnew = (int)r.below(U.modmax) + 2;
+                    dup = false;
+                    for (int k = 0; k < j; k++)
+                        if (bj[k * stride] == bnew) dup = true;
+                }
+                bj[j * stride] = bnew;
+            }
+        }
+        double sum = 0.0;
+        for (int j = 0; j < nw; j++) {
+            wj[j * stride] = -log(1.0 - r.f64());
+            sum += wj[j * stride];
+        }
+        for (int j = 0; j < nw; j++) wj[j * stride] /= sum;
+        for (int j = 0; j < nw; j++) {
+            const int b = bj[j * stride];
+            double amp = wj[j * stride] / (double)b;
+            if (r.flip()) amp = -amp;
+            if (b % 2 == 0) {
+                const double f = r.f64() * kPi;
+                double sf, cf;
+                sincos(f, &sf, &cf);
+                al[b * stride] += amp * cf;
+                bt[b * stride] += amp * sf;
+            } else {
+                al[b * stride] += amp;
+            }
+        }
+        a2[ax] = U.pin ? 0.0 : (r.f64() * 2.0 - 1.0);
+    }
+}
+
+// FP64 position of one axis at timestep t from canonical coefficients.
+__device__ __forceinline__ double eval64(const UniDev& U, const double* alpha, const double* beta,
+                                         int stride, double a2, int t) {
+    const int T = U.T, F = U.F;
+    const double* S = U.S + t;
+    const double* Cm = U.Cm + t;
+    double acc = 0.0;
+    for (int b = 2; b <= F; b += 2) {
+        acc = fma(alpha[b * stride], __ldg(S + (size_t)b * T), acc);
+        acc = fma(beta[b * stride], __ldg(Cm + (size_t)b * T), acc);
+        if (b + 1 <= F) acc = fma(alpha[(b + 1) * stride], __ldg(S + (size_t)(b + 1) * T), acc);
+    }
+    return torus_wrap(fma(acc, __ldg(U.invsinz + t), a2));
+}
+
+// ------------------------------------------------------------ grid access
+
+__device__ __forceinline__ uint64_t mix64(uint64_t k) {
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdULL;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ULL;
+    k ^= k >> 33;
+    return k;
+}
+
+__device__ __forceinline__ int64_t lin_cell(const int* c, int dim, int gw) {
+    int64_t lin = 0;
+    for (int ax = 0; ax < dim; ax++) lin = lin * gw + c[ax];
+    return lin;
+}
+
+// Head of the chain of accepted points in cell `lin` at timestep t (-1 none).
+__device__ __forceinline__ int32_t grid_head(const UniDev& U, int t, int64_t lin, int64_t cells_per_t) {
+    if (U.grid_kind == GRID_DENSE) return __ldcg(U.heads + (int64_t)t * cells_per_t + lin);
+    const uint64_t key = ((uint64_t)t << 40) | (uint64_t)lin;
+    uint64_t h = mix64(key) & U.hmask;
+    for (uint64_t probe = 0; probe <= U.hmask; probe++) {
+        const uint64_t k = __ldcg(U.hkeys + h);
+        if (k == key) return __ldcg(U.heads + h);
+        if (k == kEmptyKey) return -1;
+        h = (h + 1) & U.hmask;
+    }
+    return -1;
+}
+
+__device__ __forceinline__ int64_t cells_per_t(const UniDev& U) {
+    int64_t n = 1;
+    for (int ax = 0; ax < U.dim; ax++) n *= U.gw;
+    return n;
+}
+
+// Contacts of the point P (dim coords) at timestep t with the accepted
+// packing.  Unique mode: returns true on the first contact.  Group mode:
+// accumulates the single touched group in *g and returns true when a second
+// distinct group appears.
+__device__ __forceinline__ bool contacts64(const UniDev& U, int t, const double* P, bool group,
+                                           int32_t* g, int64_t cpt) {
+    int c[3];
+    for (int ax = 0; ax < U.dim; ax++) c[ax] = cell_of(P[ax], U.cell, U.gw);
+    int nb = U.dim == 1 ? 3 : (U.dim == 2 ? 9 : 27);
+    for (int k = 0; k < nb; k++) {
+        int cc[3], r = k;
+        for (int ax = U.dim - 1; ax >= 0; ax--) {
+            const int dd = r % 3 - 1;
+            r /= 3;
+            int v = c[ax] + dd;
+            v = v < 0 ? v + U.gw : (v >= U.gw ? v - U.gw : v);
+            cc[ax] = v;
+        }
+        int32_t p = grid_head(U, t, lin_cell(cc, U.dim, U.gw), cpt);
+        while (p >= 0) {
+            const Pt64* q = U.pts + (int64_t)p * U.T + t;
+            bool hit = true;
+            for (int ax = 0; ax < U.dim && hit; ax++)
+                hit = hit1(torus_delta(P[ax] - __ldcg(&q->c[ax])), U.cell, U.inclusive);
+            if (hit) {
+                if (!group) return true;
+                const int32_t gq = __ldcg(&q->gid);
+                if (*g == -1)
+                    *g = gq;
+                else if (*g != gq)
+                    return true;
+            }
+            p = __ldcg(&q->next);
+        }
+    }
+    return false;
+}
+
+// 1+1D crossing rule: minimum-image separation changes sign between
+// consecutive timesteps with |d_t| + |d_t+1| < 1.  No reference counterpart.
+__device__ __forceinline__ bool crosses_step(double d0, double d1) {
+    return ((d0 < 0.0) != (d1 < 0.0)) && fabs(d0) + fabs(d1) < 1.0;
+}
+
+}  // namespace ug

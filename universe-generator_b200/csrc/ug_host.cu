@@ -1,0 +1,731 @@
+// ug_host.cu -- host runtime and C ABI of the packer (include/ug.h).
+//
+// One handle = one batch of independent universes on one GPU.  The host
+// allocates every universe's tables, grid, point store and round buffers,
+// then replays the round pipeline (ug_kernels.cu) -- optionally captured as
+// a CUDA graph of `rounds_per_sync` rounds -- and reads back the small
+// control blocks between replays to grow capacities and detect completion.
+// Nothing per candidate crosses PCIe.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ug.h"
+#include "ug_kernels.cuh"
+#include "ug_mixed.cuh"
+
+namespace ug {
+
+static thread_local std::string g_err;
+
+static int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CKR(x)                                                                                \
+    do {                                                                                      \
+        cudaError_t e_ = (x);                                                                 \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(e_ == cudaErrorMemoryAllocation ? UG_ENOMEM : UG_ECUDA, "%s:%d %s: %s", \
+                        __FILE__, __LINE__, #x, cudaGetErrorString(e_));                      \
+    } while (0)
+
+enum KernelId { K_PLAN, K_PRE, K_MIXED, K_CONFIRM, K_COMPACT, K_SEVAL, K_CONFL, K_GREEDY, K_COMMIT, K_NK };
+static const char* kKernelNames[12] = {"k_plan",    "k_prefilter64", "k_prefilter_mixed",
+                                       "k_confirm64", "k_compact",   "k_surv_eval",
+                                       "k_conflicts", "k_greedy",    "k_commit",
+                                       "",           "",            ""};
+
+struct UniHost {
+    ug_universe_cfg cfg;
+    UniDev d;
+    std::vector<void*> owned;  // fixed-size allocations
+    int64_t dense_bytes = 0;
+    int64_t hcap = 0;
+    MixedTables mt;            // tensor-core operand tables (mixed precision)
+};
+
+struct Batch {
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    int n = 0;
+    int nsm = 148;
+    ug_run_opts opts{};
+    std::vector<UniHost> U;
+    UniDev* dU = nullptr;
+    UniCtl* dCtl = nullptr;
+    std::vector<UniCtl> hCtl;
+    RoundInfo* dInfo = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int graph_rounds = 0;
+    cudaEvent_t ev[2 * K_NK]{};
+    double kms[K_NK]{};
+    int64_t klaunch[K_NK]{};
+    bool synced = false;
+    int max_T = 0;
+    bool any_mixed = false;
+    int64_t launches = 0;  // kernels issued (graph replays count every node)
+    int64_t h2d = 0, d2h = 0;  // bytes copied between host and device
+    int kernels_per_round = 7;
+};
+
+static int64_t pow2_at_least(int64_t v) {
+    int64_t p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+template <class T>
+static int dalloc(UniHost& h, T** p, size_t n, int fill = -2) {
+    void* q = nullptr;
+    if (n == 0) n = 1;
+    CKR(cudaMalloc(&q, n * sizeof(T)));
+    if (fill != -2) CKR(cudaMemset(q, fill, n * sizeof(T)));
+    h.owned.push_back(q);
+    *p = (T*)q;
+    return UG_OK;
+}
+
+static int validate(const ug_universe_cfg& c) {
+    if (c.dim < 1 || c.dim > 3) return fail(UG_EINVAL, "dim must be 1, 2 or 3 (got %d)", c.dim);
+    if (c.T < 4 || c.T > kMaxF) return fail(UG_EINVAL, "T must be in [4, %d] (got %d)", kMaxF, c.T);
+    const int terms = c.terms ? c.terms : c.T;
+    const int modmax = c.T - 1 > 2 ? c.T - 1 : 2;
+    if (terms < 2 || terms - 1 > modmax)
+        return fail(UG_EINVAL, "--terms %d exceeds unique-frequency pool %d (max terms %d)", terms,
+                    modmax, modmax + 1);
+    if (c.rng == UG_RNG_PHILOX && terms != c.T)
+        return fail(UG_EINVAL, "the Philox stream is full band only (terms must be T)");
+    if (c.rng != UG_RNG_PHILOX && c.rng != UG_RNG_KNOT) return fail(UG_EINVAL, "bad rng %d", c.rng);
+    if (c.zgrid != UG_ZGRID_REF && c.zgrid != UG_ZGRID_MID) return fail(UG_EINVAL, "bad zgrid");
+    if (c.excl != UG_EXCL_REF && c.excl != UG_EXCL_OPEN) return fail(UG_EINVAL, "bad excl");
+    if (c.group_mode < 0 || c.group_mode > 2) return fail(UG_EINVAL, "bad group_mode");
+    if (c.attempts < 0 || c.max_n < 0 || c.sub_attempts < 0) return fail(UG_EINVAL, "negative budget");
+    if (c.round_size < 0 || c.round_size > (1 << 20) || (c.round_size % kTile))
+        return fail(UG_EINVAL, "round_size must be a multiple of %d up to 2^20", kTile);
+    if (c.cross1d && c.dim != 1) return fail(UG_EINVAL, "cross1d applies to dim 1 only");
+    return UG_OK;
+}
+
+// Host FP64 tables: z grid, 1/sin z, sin(b z), cos(b z) - 1, endpoint-first order.
+static void host_tables(const ug_universe_cfg& c, std::vector<double>& S, std::vector<double>& Cm,
+                        std::vector<double>& inv, std::vector<int32_t>& order) {
+    const int T = c.T, F = c.T;
+    std::vector<double> z(T);
+    inv.resize(T);
+    for (int i = 0; i < T; i++) {
+        z[i] = c.zgrid == UG_ZGRID_REF ? (i + 1) * kPi / (T + 1) : (i + 0.5) * kPi / T;
+        inv[i] = 1.0 / sin(z[i]);
+    }
+    S.assign((size_t)(F + 1) * T, 0.0);
+    Cm.assign((size_t)(F + 1) * T, 0.0);
+    for (int b = 0; b <= F; b++)
+        for (int t = 0; t < T; t++) {
+            S[(size_t)b * T + t] = sin(b * z[t]);
+            Cm[(size_t)b * T + t] = cos(b * z[t]) - 1.0;
+        }
+    order.resize(T);
+    for (int i = 0; i < T; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return std::min(a, T - 1 - a) < std::min(b, T - 1 - b);
+    });
+}
+
+static int alloc_points(UniHost& h, int64_t cap) {
+    const int T = h.cfg.T;
+    Pt64* p = nullptr;
+    Pt32* f = nullptr;
+    int64_t* ai = nullptr;
+    CKR(cudaMalloc(&p, (size_t)cap * T * sizeof(Pt64)));
+    CKR(cudaMalloc(&f, (size_t)cap * T * sizeof(Pt32)));
+    CKR(cudaMalloc(&ai, (size_t)cap * sizeof(int64_t)));
+    h.d.pts = p;
+    h.d.ptf = f;
+    h.d.acc_idx = ai;
+    h.d.slot_cap = cap;
+    return UG_OK;
+}
+
+static int alloc_hash(UniHost& h, int64_t cap) {
+    uint64_t* k = nullptr;
+    int32_t* v = nullptr;
+    CKR(cudaMalloc(&k, (size_t)cap * sizeof(uint64_t)));
+    CKR(cudaMalloc(&v, (size_t)cap * sizeof(int32_t)));
+    CKR(cudaMemset(k, 0xff, (size_t)cap * sizeof(uint64_t)));
+    CKR(cudaMemset(v, 0xff, (size_t)cap * sizeof(int32_t)));
+    h.d.hkeys = k;
+    h.d.heads = v;
+    h.d.hmask = (uint64_t)(cap - 1);
+    h.hcap = cap;
+    return UG_OK;
+}
+
+static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* dense_used) {
+    const ug_universe_cfg& c = h.cfg;
+    UniDev& d = h.d;
+    memset(&d, 0, sizeof d);
+    d.dim = c.dim;
+    d.T = c.T;
+    d.F = c.T;
+    d.nw = (c.terms ? c.terms : c.T) - 1;
+    d.rng = c.rng;
+    d.cross1d = c.cross1d;
+    d.pin = c.pin_sin1;
+    d.group_mode = c.group_mode;
+    d.seed = c.seed;
+    d.modmax = (uint32_t)(c.T - 1 > 2 ? c.T - 1 : 2);
+    if (c.excl == UG_EXCL_REF) {
+        d.cell = 2.0 / c.T;
+        d.gw = c.T;
+        d.inclusive = 1;
+    } else {
+        d.cell = 1.0 / c.T;
+        d.gw = 2 * c.T;
+        d.inclusive = 0;
+    }
+    d.B_max = c.round_size ? c.round_size : 65536;
+    const int T = c.T;
+    d.S_max = (int)std::min<int64_t>(kSmaxCap, std::max<int64_t>(256, (1 << 18) / T));
+    d.S_max = std::min(d.S_max, d.B_max);
+    // tables
+    std::vector<double> S, Cm, inv;
+    std::vector<int32_t> order;
+    host_tables(c, S, Cm, inv, order);
+    double *dS, *dC, *dI;
+    int32_t* dO;
+    int rc;
+    if ((rc = dalloc(h, &dS, S.size())) || (rc = dalloc(h, &dC, Cm.size())) ||
+        (rc = dalloc(h, &dI, inv.size())) || (rc = dalloc(h, &dO, order.size())))
+        return rc;
+    CKR(cudaMemcpy(dS, S.data(), S.size() * 8, cudaMemcpyHostToDevice));
+    CKR(cudaMemcpy(dC, Cm.data(), Cm.size() * 8, cudaMemcpyHostToDevice));
+    CKR(cudaMemcpy(dI, inv.data(), inv.size() * 8, cudaMemcpyHostToDevice));
+    CKR(cudaMemcpy(dO, order.data(), order.size() * 4, cudaMemcpyHostToDevice));
+    d.S = dS;
+    d.Cm = dC;
+    d.invsinz = dI;
+    d.order = dO;
+    // grid
+    int64_t cpt = 1;
+    for (int ax = 0; ax < c.dim; ax++) cpt *= d.gw;
+    const int64_t dense = (int64_t)T * cpt * 4;
+    if (!B.opts.force_hash && dense <= (int64_t)4 << 30 && *dense_used + dense <= dense_budget) {
+        d.grid_kind = GRID_DENSE;
+        if ((rc = dalloc(h, &d.heads, (size_t)T * cpt, 0xff))) return rc;
+        h.dense_bytes = dense;
+        *dense_used += dense;
+    } else {
+        d.grid_kind = GRID_HASH;
+        if ((rc = alloc_hash(h, pow2_at_least(std::max<int64_t>(1 << 16, 4LL * d.S_max * T)))))
+            return rc;
+    }
+    // accepted points
+    const int64_t total_budget =
+        c.attempts + (c.group_mode == UG_GROUP_SUBPATH ? (c.sub_attempts ? c.sub_attempts : c.attempts) : 0);
+    int64_t cap = B.opts.slot_hint > 0 ? B.opts.slot_hint : 8192;
+    cap = std::max<int64_t>(std::min<int64_t>(cap, total_budget + 1), 1024);
+    if ((rc = alloc_points(h, cap))) return rc;
+    // round buffers
+    const int Bm = d.B_max, Sm = d.S_max;
+    if ((rc = dalloc(h, &d.surv_bits, Bm / 32, 0)) || (rc = dalloc(h, &d.gray_bits, Bm / 32, 0)) ||
+        (rc = dalloc(h, &d.g0, Bm, 0xff)) || (rc = dalloc(h, &d.surv_off, Sm + 1, 0)) ||
+        (rc = dalloc(h, &d.spos, (size_t)Sm * T, 0)) || (rc = dalloc(h, &d.ccount, Sm, 0)) ||
+        (rc = dalloc(h, &d.clist, (size_t)Sm * kConflictCap, 0)) ||
+        (rc = dalloc(h, &d.sgid, Sm, 0xff)) || (rc = dalloc(h, &d.acc_rank, Sm, 0xff)))
+        return rc;
+    const int64_t rcap = pow2_at_least(2LL * Sm * T);
+    if ((rc = dalloc(h, &d.rkeys, rcap, 0xff)) || (rc = dalloc(h, &d.rvals, rcap, 0xff))) return rc;
+    d.rmask = (uint64_t)(rcap - 1);
+    return UG_OK;
+}
+
+static void init_ctl(const ug_universe_cfg& c, const UniDev& d, UniCtl& k) {
+    memset(&k, 0, sizeof k);
+    k.next_cand = 0;
+    k.phase_end = c.attempts;
+    k.sub_budget = c.sub_attempts ? c.sub_attempts : c.attempts;
+    k.max_n = c.max_n;
+    k.phase = 1;
+    k.state = ST_ACTIVE;
+    k.B_min = std::min(4096, d.B_max);
+    k.B_cap = d.B_max;
+    k.round_B = d.B_max;
+    k.accept_rate = c.accept_rate;
+    k.sub_accept_rate = c.sub_accept_rate;
+    k.win_target = c.accept_rate > 0 ? (int64_t)std::min(5e9, std::max(2e7, 30.0 / c.accept_rate)) : 0;
+}
+
+static int push_unidev(Batch& B) {
+    std::vector<UniDev> v(B.n);
+    for (int i = 0; i < B.n; i++) v[i] = B.U[i].d;
+    CKR(cudaMemcpyAsync(B.dU, v.data(), sizeof(UniDev) * B.n, cudaMemcpyHostToDevice, B.st));
+    B.h2d += sizeof(UniDev) * B.n;
+    CKR(cudaStreamSynchronize(B.st));
+    return UG_OK;
+}
+
+// ---------------------------------------------------------- round launch
+
+static int launch_round(Batch& B, bool timed) {
+    const int g_pre = B.nsm * 8;
+    auto tb = [&](int k) {
+        if (timed) cudaEventRecord(B.ev[2 * k], B.st);
+    };
+    auto te = [&](int k) {
+        if (timed) {
+            cudaEventRecord(B.ev[2 * k + 1], B.st);
+            cudaEventSynchronize(B.ev[2 * k + 1]);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, B.ev[2 * k], B.ev[2 * k + 1]);
+            B.kms[k] += ms;
+            B.klaunch[k]++;
+        }
+    };
+    tb(K_PLAN);
+    k_plan<<<1, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+    te(K_PLAN);
+    if (B.opts.precision == UG_PREC_MIXED && B.any_mixed) {
+        tb(K_MIXED);
+        launch_prefilter_mixed(B.dU, B.dCtl, B.dInfo, B.nsm, B.st);
+        te(K_MIXED);
+        tb(K_CONFIRM);
+        k_confirm64<<<g_pre, kTile, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+        te(K_CONFIRM);
+    } else {
+        tb(K_PRE);
+        k_prefilter64<<<g_pre, kTile, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+        te(K_PRE);
+    }
+    tb(K_COMPACT);
+    k_compact<<<B.n, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+    te(K_COMPACT);
+    tb(K_SEVAL);
+    k_surv_eval<<<B.nsm * 4, 32 * kSurvWarps, kSurvWarps * kSurvSmemPerWarp, B.st>>>(B.dU, B.dCtl,
+                                                                                      B.dInfo);
+    te(K_SEVAL);
+    tb(K_CONFL);
+    k_conflicts<<<B.nsm * 8, 128, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+    te(K_CONFL);
+    tb(K_GREEDY);
+    k_greedy<<<B.n, 32, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+    te(K_GREEDY);
+    tb(K_COMMIT);
+    k_commit<<<B.nsm * 8, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+    te(K_COMMIT);
+    CKR(cudaGetLastError());
+    return UG_OK;
+}
+
+static int build_graph(Batch& B, int rounds) {
+    if (B.gexec) {
+        cudaGraphExecDestroy(B.gexec);
+        B.gexec = nullptr;
+    }
+    cudaGraph_t g;
+    CKR(cudaStreamBeginCapture(B.st, cudaStreamCaptureModeThreadLocal));
+    for (int r = 0; r < rounds; r++) {
+        int rc = launch_round(B, false);
+        if (rc) {
+            cudaStreamEndCapture(B.st, &g);
+            return rc;
+        }
+    }
+    CKR(cudaStreamEndCapture(B.st, &g));
+    CKR(cudaGraphInstantiate(&B.gexec, g, 0));
+    CKR(cudaGraphDestroy(g));
+    B.graph_rounds = rounds;
+    return UG_OK;
+}
+
+static int pull_ctl(Batch& B) {
+    CKR(cudaMemcpyAsync(B.hCtl.data(), B.dCtl, sizeof(UniCtl) * B.n, cudaMemcpyDeviceToHost, B.st));
+    B.d2h += sizeof(UniCtl) * B.n;
+    CKR(cudaStreamSynchronize(B.st));
+    B.synced = true;
+    return UG_OK;
+}
+
+// Grow slot / hash capacity ahead of the next `rounds` rounds.
+static int ensure_capacity(Batch& B, int rounds) {
+    bool changed = false;
+    for (int i = 0; i < B.n; i++) {
+        UniHost& h = B.U[i];
+        UniCtl& k = B.hCtl[i];
+        if (k.state == ST_ERROR) return fail(UG_ECAP, "universe %d: device error %d", i, k.err_code);
+        if (k.state == ST_DONE) continue;
+        const int64_t need = k.n_slots + std::max<int64_t>(h.d.S_max, (int64_t)rounds * h.d.S_max / 4);
+        if (need > h.d.slot_cap || k.state == ST_GROW) {
+            int64_t ncap = std::max<int64_t>(h.d.slot_cap * 2, need);
+            const int T = h.cfg.T;
+            Pt64* op = h.d.pts;
+            Pt32* of = h.d.ptf;
+            int64_t* oi = h.d.acc_idx;
+            const int64_t n = k.n_slots;
+            int rc = alloc_points(h, ncap);
+            if (rc) return rc;
+            CKR(cudaMemcpyAsync(h.d.pts, op, (size_t)n * T * sizeof(Pt64), cudaMemcpyDeviceToDevice, B.st));
+            CKR(cudaMemcpyAsync(h.d.ptf, of, (size_t)n * T * sizeof(Pt32), cudaMemcpyDeviceToDevice, B.st));
+            CKR(cudaMemcpyAsync(h.d.acc_idx, oi, (size_t)n * sizeof(int64_t), cudaMemcpyDeviceToDevice, B.st));
+            CKR(cudaStreamSynchronize(B.st));
+            cudaFree(op);
+            cudaFree(of);
+            cudaFree(oi);
+            if (k.state == ST_GROW) {
+                k.state = ST_ACTIVE;
+                CKR(cudaMemcpyAsync(&B.dCtl[i].state, &k.state, sizeof(int32_t), cudaMemcpyHostToDevice, B.st));
+            }
+            changed = true;
+        }
+        if (h.d.grid_kind == GRID_HASH) {
+            const int64_t need_keys = k.hash_used + (int64_t)rounds * h.d.S_max * h.cfg.T;
+            if (need_keys * 2 > h.hcap) {
+                uint64_t* ok = h.d.hkeys;
+                int32_t* ov = h.d.heads;
+                int rc = alloc_hash(h, pow2_at_least(need_keys * 4));
+                if (rc) return rc;
+                cudaFree(ok);
+                cudaFree(ov);
+                int64_t zero = 0;
+                k.hash_used = 0;
+                CKR(cudaMemcpyAsync(&B.dCtl[i].hash_used, &zero, sizeof zero, cudaMemcpyHostToDevice, B.st));
+                changed = true;
+                int rc2 = push_unidev(B);
+                if (rc2) return rc2;
+                if (k.n_slots > 0)
+                    k_rehash<<<B.nsm * 4, 256, 0, B.st>>>(B.dU, B.dCtl, i, k.n_slots);
+                CKR(cudaGetLastError());
+                CKR(cudaStreamSynchronize(B.st));
+            }
+        }
+    }
+    if (changed) return push_unidev(B);
+    return UG_OK;
+}
+
+static bool all_done(const Batch& B) {
+    for (const UniCtl& k : B.hCtl)
+        if (k.state != ST_DONE) return false;
+    return true;
+}
+
+}  // namespace ug
+
+using namespace ug;
+
+extern "C" {
+
+int ug_version(void) { return 1; }
+
+int ug_last_error(char* buf, size_t len) {
+    if (buf && len) {
+        strncpy(buf, g_err.c_str(), len - 1);
+        buf[len - 1] = 0;
+    }
+    return (int)g_err.size();
+}
+
+int ug_batch_create(const ug_universe_cfg* cfgs, int32_t n, const ug_run_opts* opts, void** out) {
+    if (!cfgs || !out || n < 1 || n > kMaxUni) return fail(UG_EINVAL, "bad batch arguments (n=%d)", n);
+    for (int i = 0; i < n; i++) {
+        int rc = validate(cfgs[i]);
+        if (rc) return rc;
+    }
+    Batch* B = new Batch();
+    if (opts) B->opts = *opts;
+    if (B->opts.rounds_per_sync <= 0) B->opts.rounds_per_sync = 8;
+    if (B->opts.device >= 0) {
+        cudaError_t e = cudaSetDevice(B->opts.device);
+        if (e != cudaSuccess) {
+            delete B;
+            return fail(UG_ECUDA, "cudaSetDevice(%d): %s", B->opts.device, cudaGetErrorString(e));
+        }
+    }
+    cudaGetDevice(&B->dev);
+    cudaDeviceGetAttribute(&B->nsm, cudaDevAttrMultiProcessorCount, B->dev);
+    int rc = UG_OK;
+    auto bail = [&](int code) {
+        ug_batch_destroy(B);
+        return code;
+    };
+    if (B->opts.stream) {
+        B->st = (cudaStream_t)(uintptr_t)B->opts.stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&B->st, cudaStreamNonBlocking) != cudaSuccess)
+            return bail(fail(UG_ECUDA, "stream create failed"));
+        B->own_stream = true;
+    }
+    B->n = n;
+    B->U.resize(n);
+    size_t freeb = 0, totalb = 0;
+    cudaMemGetInfo(&freeb, &totalb);
+    const int64_t dense_budget = (int64_t)(freeb * 0.35);
+    int64_t dense_used = 0;
+    for (int i = 0; i < n; i++) {
+        B->U[i].cfg = cfgs[i];
+        B->max_T = std::max(B->max_T, cfgs[i].T);
+        if ((rc = setup_universe(*B, B->U[i], dense_budget, &dense_used))) return bail(rc);
+        if (B->opts.precision == UG_PREC_MIXED) {
+            if ((rc = mixed_setup(B->U[i].cfg, B->U[i].d, B->U[i].mt))) return bail(rc);
+            B->any_mixed = true;
+        }
+    }
+    if (cudaMalloc(&B->dU, sizeof(UniDev) * n) != cudaSuccess ||
+        cudaMalloc(&B->dCtl, sizeof(UniCtl) * n) != cudaSuccess ||
+        cudaMalloc(&B->dInfo, sizeof(RoundInfo)) != cudaSuccess)
+        return bail(fail(UG_ENOMEM, "control block allocation failed"));
+    B->hCtl.resize(n);
+    for (int i = 0; i < n; i++) init_ctl(cfgs[i], B->U[i].d, B->hCtl[i]);
+    RoundInfo ri;
+    memset(&ri, 0, sizeof ri);
+    ri.n_uni = n;
+    if (cudaMemcpy(B->dCtl, B->hCtl.data(), sizeof(UniCtl) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(B->dInfo, &ri, sizeof ri, cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(fail(UG_ECUDA, "control block upload failed"));
+    if ((rc = push_unidev(*B))) return bail(rc);
+    if (cudaFuncSetAttribute(k_surv_eval, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(kSurvWarps * kSurvSmemPerWarp)) != cudaSuccess)
+        return bail(fail(UG_ECUDA, "smem attribute failed"));
+    if (B->any_mixed && (rc = mixed_init_kernels())) return bail(rc);
+    B->kernels_per_round = B->any_mixed ? 8 : 7;
+    for (int k = 0; k < 2 * K_NK; k++) cudaEventCreate(&B->ev[k]);
+    *out = B;
+    return UG_OK;
+}
+
+int ug_batch_run(void* h, int64_t max_rounds) {
+    Batch* B = (Batch*)h;
+    if (!B) return fail(UG_EINVAL, "null handle");
+    int rc = pull_ctl(*B);
+    if (rc) return rc;
+    int64_t done_rounds = 0;
+    const int R = B->opts.rounds_per_sync;
+    int stalls = 0;
+    while (!all_done(*B)) {
+        int64_t progress_before = 0;
+        for (const UniCtl& k : B->hCtl) progress_before += k.next_cand + k.n_slots;
+        if (max_rounds > 0 && done_rounds >= max_rounds) return UG_OK;
+        if ((rc = ensure_capacity(*B, R))) return rc;
+        if (B->opts.use_graph && !B->opts.kernel_timing) {
+            if (!B->gexec && (rc = build_graph(*B, R))) return rc;
+            CKR(cudaGraphLaunch(B->gexec, B->st));
+        } else {
+            for (int r = 0; r < R; r++)
+                if ((rc = launch_round(*B, B->opts.kernel_timing != 0))) return rc;
+        }
+        B->launches += (int64_t)R * B->kernels_per_round;
+        done_rounds += R;
+        if ((rc = pull_ctl(*B))) return rc;
+        int64_t progress_after = 0;
+        for (const UniCtl& k : B->hCtl) progress_after += k.next_cand + k.n_slots;
+        stalls = progress_after == progress_before ? stalls + 1 : 0;
+        if (stalls > 64) return fail(UG_ETIMEDOUT, "no universe made progress in %d rounds", 64 * R);
+    }
+    return UG_OK;
+}
+
+int ug_batch_reset(void* h, const uint64_t* seeds) {
+    Batch* B = (Batch*)h;
+    if (!B) return fail(UG_EINVAL, "null handle");
+    CKR(cudaStreamSynchronize(B->st));
+    for (int i = 0; i < B->n; i++) {
+        UniHost& u = B->U[i];
+        if (seeds) {
+            u.cfg.seed = seeds[i];
+            u.d.seed = seeds[i];
+        }
+        if (u.d.grid_kind == GRID_DENSE) {
+            int64_t cpt = 1;
+            for (int ax = 0; ax < u.d.dim; ax++) cpt *= u.d.gw;
+            CKR(cudaMemsetAsync(u.d.heads, 0xff, (size_t)u.d.T * cpt * sizeof(int32_t), B->st));
+        } else {
+            CKR(cudaMemsetAsync(u.d.hkeys, 0xff, (size_t)u.hcap * sizeof(uint64_t), B->st));
+            CKR(cudaMemsetAsync(u.d.heads, 0xff, (size_t)u.hcap * sizeof(int32_t), B->st));
+        }
+        const int32_t ep = B->hCtl[i].epoch;
+        init_ctl(u.cfg, u.d, B->hCtl[i]);
+        B->hCtl[i].epoch = ep;  // round-hash entries of earlier epochs stay stale
+    }
+    CKR(cudaMemcpyAsync(B->dCtl, B->hCtl.data(), sizeof(UniCtl) * B->n, cudaMemcpyHostToDevice, B->st));
+    B->h2d += sizeof(UniCtl) * B->n;
+    return push_unidev(*B);
+}
+
+int ug_batch_done(void* h) {
+    Batch* B = (Batch*)h;
+    if (!B) return -UG_EINVAL;
+    if (pull_ctl(*B)) return -UG_ECUDA;
+    return all_done(*B) ? 1 : 0;
+}
+
+int ug_batch_stats(void* h, int32_t u, ug_stats* out) {
+    Batch* B = (Batch*)h;
+    if (!B || u < 0 || u >= B->n || !out) return fail(UG_EINVAL, "bad arguments");
+    int rc = pull_ctl(*B);
+    if (rc) return rc;
+    const UniCtl& k = B->hCtl[u];
+    out->n = k.n_slots;
+    out->n_unique = k.n_unique;
+    out->n_sub = k.n_sub;
+    out->attempts = k.attempts;
+    out->phase1_end = k.phase == 2 ? k.phase1_end : k.attempts;
+    out->rounds = k.rounds;
+    out->gray = k.gray_total;
+    out->evals = k.evals;
+    out->evals_fp64 = k.evals_fp64;
+    out->state = k.state;
+    out->grid_kind = B->U[u].d.grid_kind;
+    return UG_OK;
+}
+
+int ug_batch_accepted(void* h, int32_t u, int64_t* idx, int32_t* gid, int64_t cap, int64_t* n) {
+    Batch* B = (Batch*)h;
+    if (!B || u < 0 || u >= B->n) return fail(UG_EINVAL, "bad arguments");
+    int rc = pull_ctl(*B);
+    if (rc) return rc;
+    const int64_t N = B->hCtl[u].n_slots;
+    if (n) *n = N;
+    if (cap <= 0) return UG_OK;
+    if (cap < N) return fail(UG_ECAP, "accepted buffer too small (%lld < %lld)", (long long)cap, (long long)N);
+    const UniDev& d = B->U[u].d;
+    if (idx && N) CKR(cudaMemcpy(idx, d.acc_idx, N * sizeof(int64_t), cudaMemcpyDeviceToHost));
+    if (idx) B->d2h += N * sizeof(int64_t);
+    if (gid && N) {
+        std::vector<Pt64> tmp(N);
+        CKR(cudaMemcpy2D(tmp.data(), sizeof(Pt64), d.pts, sizeof(Pt64) * d.T, sizeof(Pt64), N,
+                         cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < N; i++) gid[i] = tmp[i].gid;
+    }
+    return UG_OK;
+}
+
+int ug_batch_positions(void* h, int32_t u, double* pos, int64_t cap_paths) {
+    Batch* B = (Batch*)h;
+    if (!B || u < 0 || u >= B->n || !pos) return fail(UG_EINVAL, "bad arguments");
+    int rc = pull_ctl(*B);
+    if (rc) return rc;
+    const int64_t N = B->hCtl[u].n_slots;
+    if (cap_paths < N) return fail(UG_ECAP, "positions buffer too small");
+    const UniDev& d = B->U[u].d;
+    std::vector<Pt64> tmp((size_t)N * d.T);
+    if (N) CKR(cudaMemcpy(tmp.data(), d.pts, tmp.size() * sizeof(Pt64), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < N; i++)
+        for (int ax = 0; ax < d.dim; ax++)
+            for (int t = 0; t < d.T; t++) pos[(i * d.dim + ax) * d.T + t] = tmp[(size_t)i * d.T + t].c[ax];
+    return UG_OK;
+}
+
+int ug_batch_params(void* h, int32_t u, double* a2, double* a, int32_t* b, double* f, int64_t cap_paths) {
+    Batch* B = (Batch*)h;
+    if (!B || u < 0 || u >= B->n) return fail(UG_EINVAL, "bad arguments");
+    int rc = pull_ctl(*B);
+    if (rc) return rc;
+    const int64_t N = B->hCtl[u].n_slots;
+    if (cap_paths < N) return fail(UG_ECAP, "params buffer too small");
+    if (N == 0) return UG_OK;
+    const UniDev& d = B->U[u].d;
+    const int nw = d.nw, D = d.dim;
+    double *da2, *da, *df;
+    int32_t* db;
+    CKR(cudaMalloc(&da2, (size_t)N * D * 8));
+    CKR(cudaMalloc(&da, (size_t)N * D * nw * 8));
+    CKR(cudaMalloc(&df, (size_t)N * D * nw * 8));
+    CKR(cudaMalloc(&db, (size_t)N * D * nw * 4));
+    launch_params(B->dU, u, N, da2, da, db, df, B->st);
+    cudaError_t e = cudaStreamSynchronize(B->st);
+    if (e == cudaSuccess && a2) e = cudaMemcpy(a2, da2, (size_t)N * D * 8, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && a) e = cudaMemcpy(a, da, (size_t)N * D * nw * 8, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && f) e = cudaMemcpy(f, df, (size_t)N * D * nw * 8, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && b) e = cudaMemcpy(b, db, (size_t)N * D * nw * 4, cudaMemcpyDeviceToHost);
+    cudaFree(da2);
+    cudaFree(da);
+    cudaFree(df);
+    cudaFree(db);
+    if (e != cudaSuccess) return fail(UG_ECUDA, "params: %s", cudaGetErrorString(e));
+    return UG_OK;
+}
+
+int ug_batch_kernel_times(void* h, ug_kernel_times* out) {
+    Batch* B = (Batch*)h;
+    if (!B || !out) return fail(UG_EINVAL, "bad arguments");
+    memset(out, 0, sizeof *out);
+    for (int k = 0; k < K_NK; k++) {
+        out->ms[k] = B->kms[k];
+        out->launches[k] = B->klaunch[k];
+        out->names[k] = kKernelNames[k];
+    }
+    return UG_OK;
+}
+
+int ug_batch_counters(void* h, int64_t* launches, int64_t* h2d_bytes, int64_t* d2h_bytes) {
+    Batch* B = (Batch*)h;
+    if (!B) return fail(UG_EINVAL, "null handle");
+    if (launches) *launches = B->launches;
+    if (h2d_bytes) *h2d_bytes = B->h2d;
+    if (d2h_bytes) *d2h_bytes = B->d2h;
+    return UG_OK;
+}
+
+int ug_batch_reset_times(void* h) {
+    Batch* B = (Batch*)h;
+    if (!B) return fail(UG_EINVAL, "bad arguments");
+    for (int k = 0; k < K_NK; k++) {
+        B->kms[k] = 0;
+        B->klaunch[k] = 0;
+    }
+    return UG_OK;
+}
+
+int ug_batch_mixed_error(void* h, int32_t u, int64_t first, int64_t count, double* max_err, double* margin) {
+    Batch* B = (Batch*)h;
+    if (!B || u < 0 || u >= B->n) return fail(UG_EINVAL, "bad arguments");
+    if (B->opts.precision != UG_PREC_MIXED) return fail(UG_ENOTSUP, "batch is not mixed precision");
+    return mixed_error(B->dU, u, B->U[u].d, B->U[u].mt, first, count, max_err, margin, B->st);
+}
+
+int ug_batch_destroy(void* h) {
+    Batch* B = (Batch*)h;
+    if (!B) return UG_OK;
+    if (B->st) cudaStreamSynchronize(B->st);
+    if (B->gexec) cudaGraphExecDestroy(B->gexec);
+    for (UniHost& u : B->U) {
+        for (void* p : u.owned) cudaFree(p);
+        if (u.d.grid_kind == GRID_HASH) {
+            cudaFree(u.d.hkeys);
+            cudaFree(u.d.heads);
+        }
+        cudaFree(u.d.pts);
+        cudaFree(u.d.ptf);
+        cudaFree(u.d.acc_idx);
+        mixed_free(u.mt);
+    }
+    cudaFree(B->dU);
+    cudaFree(B->dCtl);
+    cudaFree(B->dInfo);
+    for (int k = 0; k < 2 * K_NK; k++)
+        if (B->ev[k]) cudaEventDestroy(B->ev[k]);
+    if (B->own_stream && B->st) cudaStreamDestroy(B->st);
+    delete B;
+    return UG_OK;
+}
+
+int ug_pack_create(const ug_universe_cfg* cfg, const ug_run_opts* opts, void** out) {
+    return ug_batch_create(cfg, 1, opts, out);
+}
+int ug_pack_run(void* h) { return ug_batch_run(h, 0); }
+int ug_pack_stats(void* h, ug_stats* out) { return ug_batch_stats(h, 0, out); }
+int ug_pack_destroy(void* h) { return ug_batch_destroy(h); }
+
+}  // extern "C"

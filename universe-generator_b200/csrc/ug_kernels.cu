@@ -1,0 +1,798 @@
+// ug_kernels.cu -- the round pipeline of the batched RSA packer.
+//
+// One round of every active universe:
+//   k_plan         round sizes, phase transitions, tile decomposition
+//   k_prefilter64  FP64 test of every candidate against the committed packing
+//                  (or k_prefilter_mixed + k_confirm64, ug_mixed.cu)
+//   k_compact      survivors in candidate-index order (deterministic)
+//   k_surv_eval    FP64 trajectories of the survivors + round hash insert
+//   k_conflicts    each survivor's contacts with EARLIER survivors of the round
+//   k_greedy       in-order resolution: survivor i is admitted iff it touches
+//                  no admitted earlier survivor (group rules in group modes)
+//   k_commit       admitted trajectories appended to the collision grid
+// Non-survivors collide with the committed packing, which only grows, so they
+// are rejected by sequential RSA as well; survivors are decided in index
+// order against the round's earlier admissions.  The accepted set is
+// therefore exactly sequential RSA over the candidate stream -- the
+// exact-index admission of cuda/braid_knot.cu:433-462, made device-resident.
+#include "ug_kernels.cuh"
+
+#include <algorithm>
+
+namespace ug {
+
+// ------------------------------------------------------------------ plan
+
+__global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info) {
+    __shared__ int32_t ntiles[kMaxUni];
+    const int n = info->n_uni;
+    for (int u = threadIdx.x; u < n; u += blockDim.x) {
+        UniCtl& c = ctl[u];
+        const UniDev& d = U[u];
+        int B = 0;
+        if (c.state == ST_ACTIVE) {
+            for (int guard = 0; guard < 2; guard++) {
+                const bool over = c.next_cand >= c.phase_end ||
+                                  (c.phase == 1 && c.max_n > 0 && c.n_unique >= c.max_n);
+                if (!over) break;
+                if (c.phase == 1 && d.group_mode == GROUP_SUBPATH) {
+                    c.phase = 2;
+                    c.phase1_end = c.next_cand;
+                    c.phase_end = c.next_cand + c.sub_budget;
+                    c.round_B = c.B_cap;  // fresh adaptation (braid_cuda.cu:952)
+                    c.win_att = c.win_adm = 0;
+                    c.win_head = c.win_len = 0;
+                    c.win_target = c.sub_accept_rate > 0
+                                       ? (int64_t)fmin(5e9, fmax(2e7, 30.0 / c.sub_accept_rate))
+                                       : 0;
+                    continue;
+                }
+                c.state = ST_DONE;
+                break;
+            }
+            if (c.state == ST_ACTIVE) {
+                const int64_t left = c.phase_end - c.next_cand;
+                B = (int)(left < (int64_t)c.round_B ? left : (int64_t)c.round_B);
+            }
+        }
+        c.B = B;
+        c.round_base = c.next_cand;
+        c.S = c.S_raw = c.trunc = c.stop_at = 0;
+        c.n_gray = 0;
+        if (B > 0) c.epoch = (c.epoch + 1) & 0xFFFFFF;
+        ntiles[u] = (B + kTile - 1) / kTile;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0, act = 0;
+        for (int u = 0; u < n; u++) {
+            info->tile_off[u] = acc;
+            acc += ntiles[u];
+            act |= ntiles[u] > 0;
+        }
+        info->tile_off[n] = acc;
+        info->total_tiles = acc;
+        info->any_active = act;
+        info->total_surv = 0;
+        info->compact_done = 0;
+    }
+}
+
+// ------------------------------------------------------------- prefilter
+
+// FP64 test of candidate idx against the committed packing.  Returns true
+// when it is rejected.  Group mode: *g gets the single group touched (-1 none).
+__device__ bool test64(const UniDev& d, int64_t n_slots, const double* alpha, const double* beta,
+                       const double* a2, bool group, int32_t* g, int* nev) {
+    *g = -1;
+    const int T = d.T, F1 = d.F + 1;
+    if (d.dim == 1 && d.cross1d) {
+        double P[kMaxF];
+        for (int t = 0; t < T; t++) P[t] = eval64(d, alpha, beta, 1, a2[0], t);
+        *nev = T;
+        for (int64_t s = 0; s < n_slots; s++) {
+            const Pt64* q = d.pts + s * T;
+            double d0 = torus_delta(P[0] - __ldcg(&q[0].c[0]));
+            bool hit = hit1(d0, d.cell, d.inclusive);
+            for (int t = 1; t < T && !hit; t++) {
+                const double d1 = torus_delta(P[t] - __ldcg(&q[t].c[0]));
+                hit = hit1(d1, d.cell, d.inclusive) || crosses_step(d0, d1);
+                d0 = d1;
+            }
+            if (hit) {
+                if (!group) return true;
+                const int32_t gq = __ldcg(&q[0].gid);
+                if (*g == -1)
+                    *g = gq;
+                else if (*g != gq)
+                    return true;
+            }
+        }
+        return false;
+    }
+    const int64_t cpt = cells_per_t(d);
+    for (int oi = 0; oi < T; oi++) {
+        const int t = __ldg(d.order + oi);
+        double P[3];
+        for (int ax = 0; ax < d.dim; ax++) P[ax] = eval64(d, alpha + ax * F1, beta + ax * F1, 1, a2[ax], t);
+        *nev = oi + 1;
+        if (contacts64(d, t, P, group, g, cpt)) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ bool group_phase(const UniDev& d, const UniCtl& c) {
+    return d.group_mode == GROUP_UNIQUE || (d.group_mode == GROUP_SUBPATH && c.phase == 2);
+}
+
+// Thread-per-candidate FP64 generation + test.  kGrayOnly: only candidates
+// whose gray bit the mixed prefilter set (its FP64 guard-band retest).
+template <bool kGrayOnly>
+__device__ __forceinline__ void prefilter64_tiles(const UniDev* __restrict__ U, UniCtl* ctl,
+                                                  RoundInfo* info) {
+    double alpha[3 * (kMaxF + 1)], beta[3 * (kMaxF + 1)], a2[3];
+    int32_t bj[kMaxF];
+    double wj[kMaxF];
+    const int n_uni = info->n_uni, total = info->total_tiles;
+    const int lane = threadIdx.x & 31;
+    for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
+        const int u = find_uni(info->tile_off, n_uni, tile);
+        const UniDev& d = U[u];
+        const UniCtl& c = ctl[u];
+        const int off = (tile - info->tile_off[u]) * kTile + threadIdx.x;
+        const int B = c.B;
+        bool work = off < B;
+        if (kGrayOnly && work) work = (d.gray_bits[off >> 5] >> (off & 31)) & 1u;
+        bool surv = false;
+        int32_t g = -1;
+        int nev = 0;
+        if (work) {
+            const uint64_t idx = (uint64_t)(c.round_base + off);
+            const int F1 = d.F + 1;
+            if (d.rng == RNG_KNOT) {
+                gen_knot64(d, idx, alpha, beta, a2, bj, wj, 1);
+            } else {
+                for (int ax = 0; ax < d.dim; ax++)
+                    a2[ax] = gen_philox64(d, idx, ax, alpha + ax * F1, beta + ax * F1, 1);
+            }
+            surv = !test64(d, c.n_slots, alpha, beta, a2, group_phase(d, c), &g, &nev);
+        }
+        for (int o = 16; o > 0; o >>= 1) nev += __shfl_xor_sync(0xffffffffu, nev, o);
+        if (lane == 0 && nev) {
+            atomicAdd((unsigned long long*)&ctl[u].evals_fp64, (unsigned long long)nev);
+            if (!kGrayOnly) atomicAdd((unsigned long long*)&ctl[u].evals, (unsigned long long)nev);
+        }
+        if (kGrayOnly) {
+            if (work && surv) atomicOr(&d.surv_bits[off >> 5], 1u << (off & 31));
+        } else {
+            const uint32_t bits = __ballot_sync(0xffffffffu, surv);
+            if (lane == 0 && (off & ~31) < d.B_max) d.surv_bits[off >> 5] = bits;
+        }
+        if (work && d.group_mode != GROUP_NONE) d.g0[off] = g;
+    }
+}
+
+__global__ void __launch_bounds__(kTile) k_prefilter64(const UniDev* __restrict__ U, UniCtl* ctl,
+                                                       RoundInfo* info) {
+    prefilter64_tiles<false>(U, ctl, info);
+}
+
+__global__ void __launch_bounds__(kTile) k_confirm64(const UniDev* __restrict__ U, UniCtl* ctl,
+                                                     RoundInfo* info) {
+    prefilter64_tiles<true>(U, ctl, info);
+}
+
+// --------------------------------------------------------------- compact
+
+__global__ void __launch_bounds__(256) k_compact(const UniDev* __restrict__ U, UniCtl* ctl,
+                                                 RoundInfo* info) {
+    __shared__ int32_t wsum[8];
+    __shared__ int32_t s_running;
+    __shared__ bool s_last;
+    const int u = blockIdx.x;
+    const UniDev& d = U[u];
+    UniCtl& c = ctl[u];
+    const int B = c.B;
+    const int nwords = (B + 31) >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_running = 0;
+    __syncthreads();
+    for (int base = 0; base < nwords; base += 256) {
+        const int w = base + tid;
+        uint32_t bits = w < nwords ? d.surv_bits[w] : 0u;
+        if (w == nwords - 1 && (B & 31)) bits &= (1u << (B & 31)) - 1u;
+        const int cnt = __popc(bits);
+        int incl = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        int wpre = 0, tot = 0;
+        for (int k = 0; k < 8; k++) {
+            if (k < warp) wpre += wsum[k];
+            tot += wsum[k];
+        }
+        int rank = s_running + wpre + incl - cnt;
+        while (bits) {
+            const int bit = __ffs(bits) - 1;
+            bits &= bits - 1;
+            if (rank <= d.S_max) d.surv_off[rank] = w * 32 + bit;
+            rank++;
+        }
+        __syncthreads();
+        if (tid == 0) s_running += tot;
+        __syncthreads();
+    }
+    const int S_raw = s_running;
+    const int S = S_raw < d.S_max ? S_raw : d.S_max;
+    for (int r = tid; r < S; r += 256) d.ccount[r] = 0;
+    if (tid == 0) {
+        c.S_raw = S_raw;
+        c.S = S;
+        c.trunc = S;
+        __threadfence();
+        s_last = atomicAdd(&info->compact_done, 1) == info->n_uni - 1;
+    }
+    __syncthreads();
+    if (s_last && tid == 0) {
+        __threadfence();
+        int acc = 0;
+        for (int v = 0; v < info->n_uni; v++) {
+            info->surv_off[v] = acc;
+            acc += *(volatile int32_t*)&ctl[v].S;
+        }
+        info->surv_off[info->n_uni] = acc;
+        info->total_surv = acc;
+    }
+}
+
+// ------------------------------------------------------------ survivors
+
+__device__ __forceinline__ uint64_t rkey_of(int epoch, int t, int64_t lin) {
+    return ((uint64_t)(epoch & 0xFFFFFF) << 40) | ((uint64_t)t << 31) | (uint64_t)lin;
+}
+
+// Round hash slot holding `key` (claiming an empty or stale slot).
+__device__ __forceinline__ uint64_t rhash_claim(const UniDev& d, uint64_t key) {
+    const uint64_t ep = key >> 40;
+    uint64_t h = mix64(key) & d.rmask;
+    for (uint64_t probe = 0; probe <= d.rmask; probe++) {
+        uint64_t k = __ldcg(d.rkeys + h);
+        while (k != key && (k == kEmptyKey || (k >> 40) != ep)) {
+            const uint64_t prev = atomicCAS((unsigned long long*)(d.rkeys + h), k, key);
+            if (prev == k) return h;
+            k = prev;
+        }
+        if (k == key) return h;
+        h = (h + 1) & d.rmask;
+    }
+    return ~0ull;  // table full: cannot happen with rcap >= 2 * S_max * T
+}
+
+__device__ __forceinline__ int32_t rhash_head(const UniDev& d, uint64_t key) {
+    const uint64_t ep = key >> 40;
+    uint64_t h = mix64(key) & d.rmask;
+    for (uint64_t probe = 0; probe <= d.rmask; probe++) {
+        const uint64_t k = __ldcg(d.rkeys + h);
+        if (k == key) {
+            const uint64_t v = __ldcg(d.rvals + h);
+            return (v >> 32) == (ep & 0xFFFFFF) ? (int32_t)(uint32_t)v : -1;
+        }
+        if (k == kEmptyKey || (k >> 40) != ep) return -1;
+        h = (h + 1) & d.rmask;
+    }
+    return -1;
+}
+
+// One warp per survivor: FP64 regeneration (warp-parallel Philox blocks,
+// sequential normalisation sum in ascending b -- the same operations as the
+// thread-per-candidate prefilter, so identical values), trajectories at all
+// T timesteps, round-hash insert.
+__global__ void __launch_bounds__(32 * kSurvWarps) k_surv_eval(const UniDev* __restrict__ U,
+                                                                 UniCtl* ctl, RoundInfo* info) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    unsigned char* my = smem_raw + (size_t)wib * kSurvSmemPerWarp;
+    double* alpha = (double*)my;
+    double* beta = alpha + 3 * (kMaxF + 1);
+    double* a2 = beta + 3 * (kMaxF + 1);
+    double* wj = a2 + 3;
+    int32_t* bj = (int32_t*)(wj + kMaxF);
+    const int n_uni = info->n_uni, total = info->total_surv;
+    const int gwarp = blockIdx.x * kSurvWarps + wib, nwarps = gridDim.x * kSurvWarps;
+    for (int item = gwarp; item < total; item += nwarps) {
+        const int u = find_uni(info->surv_off, n_uni, item);
+        const int r = item - info->surv_off[u];
+        const UniDev& d = U[u];
+        const UniCtl& c = ctl[u];
+        const uint64_t idx = (uint64_t)(c.round_base + d.surv_off[r]);
+        const int F = d.F, F1 = F + 1, T = d.T;
+        if (d.rng == RNG_KNOT) {
+            if (lane == 0) gen_knot64(d, idx, alpha, beta, a2, bj, wj, 1);
+            __syncwarp();
+        } else {
+            for (int ax = 0; ax < d.dim; ax++) {
+                double* al = alpha + ax * F1;
+                double* bt = beta + ax * F1;
+                for (int p = lane; 2 * p <= F; p += 32) {
+                    const uint4 o = philox_block(d.seed, idx, ax, p);
+                    if (p == 0) {
+                        a2[ax] = d.pin ? 0.0 : (double)o.x * (1.0 / 2147483648.0) - 1.0;
+                        continue;
+                    }
+                    const int be = 2 * p, bo = 2 * p + 1;
+                    const double Ee = -log(((double)o.x + 0.5) * (1.0 / 4294967296.0));
+                    al[be] = (o.z & 1u) ? -Ee : Ee;
+                    bt[be] = (double)(o.z >> 1) * (1.0 / 2147483648.0) * kPi;
+                    if (bo <= F) {
+                        const double Eo = -log(((double)o.y + 0.5) * (1.0 / 4294967296.0));
+                        al[bo] = (o.w & 1u) ? -Eo : Eo;
+                    }
+                }
+                __syncwarp();
+                double sum = 0.0;
+                if (lane == 0)
+                    for (int b = 2; b <= F; b++) sum += fabs(al[b]);
+                sum = __shfl_sync(0xffffffffu, sum, 0);
+                for (int b = 2 + lane; b <= F; b += 32) {
+                    const double e = al[b];
+                    double amp = fabs(e) / sum / (double)b;
+                    if (e < 0.0) amp = -amp;
+                    if (b & 1) {
+                        al[b] = amp;
+                        bt[b] = 0.0;
+                    } else {
+                        double sf, cf;
+                        sincos(bt[b], &sf, &cf);
+                        al[b] = amp * cf;
+                        bt[b] = amp * sf;
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        const int64_t cpt = cells_per_t(d);
+        (void)cpt;
+        for (int t = lane; t < T; t += 32) {
+            Pt64 q;
+            int cc[3];
+            for (int ax = 0; ax < 3; ax++) q.c[ax] = 0.0;
+            for (int ax = 0; ax < d.dim; ax++) {
+                q.c[ax] = eval64(d, alpha + ax * F1, beta + ax * F1, 1, a2[ax], t);
+                cc[ax] = cell_of(q.c[ax], d.cell, d.gw);
+            }
+            const uint64_t key = rkey_of(c.epoch, t, lin_cell(cc, d.dim, d.gw));
+            const uint64_t h = rhash_claim(d, key);
+            int32_t nxt = -1;
+            if (h != ~0ull) {
+                const uint64_t old = atomicExch((unsigned long long*)(d.rvals + h),
+                                                ((uint64_t)(c.epoch & 0xFFFFFF) << 32) | (uint32_t)r);
+                if ((old >> 32) == (uint64_t)(c.epoch & 0xFFFFFF)) nxt = (int32_t)(uint32_t)old;
+            }
+            q.next = nxt;
+            q.gid = -1;
+            d.spos[(int64_t)r * T + t] = q;
+        }
+        __syncwarp();
+    }
+}
+
+// One warp per survivor r: the set of earlier survivors r' < r that it
+// touches (Chebyshev contact at any timestep; plus crossings in 1+1D).
+__global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U, UniCtl* ctl,
+                                                    RoundInfo* info) {
+    __shared__ int32_t s_cnt[4];
+    __shared__ int32_t s_list[4][kConflictCap];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int n_uni = info->n_uni, total = info->total_surv;
+    const int gwarp = blockIdx.x * 4 + wib, nwarps = gridDim.x * 4;
+    volatile int32_t* cnt = &s_cnt[wib];
+    volatile int32_t* lst = s_list[wib];
+    for (int item = gwarp; item < total; item += nwarps) {
+        const int u = find_uni(info->surv_off, n_uni, item);
+        const int r = item - info->surv_off[u];
+        const UniDev& d = U[u];
+        UniCtl& c = ctl[u];
+        const int T = d.T;
+        if (lane == 0) *cnt = 0;
+        __syncwarp();
+        auto add = [&](int32_t r2) {
+            const int n = *cnt < kConflictCap ? *cnt : kConflictCap;
+            for (int i = 0; i < n; i++)
+                if (lst[i] == r2) return;
+            const int pos = atomicAdd((int32_t*)cnt, 1);
+            if (pos < kConflictCap) lst[pos] = r2;
+        };
+        if (d.dim == 1 && d.cross1d) {
+            const Pt64* P = d.spos + (int64_t)r * T;
+            for (int r2 = lane; r2 < r; r2 += 32) {
+                const Pt64* Q = d.spos + (int64_t)r2 * T;
+                double d0 = torus_delta(P[0].c[0] - Q[0].c[0]);
+                bool hit = hit1(d0, d.cell, d.inclusive);
+                for (int t = 1; t < T && !hit; t++) {
+                    const double d1 = torus_delta(P[t].c[0] - Q[t].c[0]);
+                    hit = hit1(d1, d.cell, d.inclusive) || crosses_step(d0, d1);
+                    d0 = d1;
+                }
+                if (hit) add(r2);
+            }
+        } else {
+            const int nb = d.dim == 1 ? 3 : (d.dim == 2 ? 9 : 27);
+            for (int t = lane; t < T; t += 32) {
+                const Pt64 P = d.spos[(int64_t)r * T + t];
+                int c0[3];
+                for (int ax = 0; ax < d.dim; ax++) c0[ax] = cell_of(P.c[ax], d.cell, d.gw);
+                for (int k = 0; k < nb; k++) {
+                    int cc[3], rr = k;
+                    for (int ax = d.dim - 1; ax >= 0; ax--) {
+                        const int dd = rr % 3 - 1;
+                        rr /= 3;
+                        int v = c0[ax] + dd;
+                        v = v < 0 ? v + d.gw : (v >= d.gw ? v - d.gw : v);
+                        cc[ax] = v;
+                    }
+                    int32_t r2 = rhash_head(d, rkey_of(c.epoch, t, lin_cell(cc, d.dim, d.gw)));
+                    while (r2 >= 0) {
+                        const Pt64* Q = d.spos + (int64_t)r2 * T + t;
+                        if (r2 < r) {
+                            bool hit = true;
+                            for (int ax = 0; ax < d.dim && hit; ax++)
+                                hit = hit1(torus_delta(P.c[ax] - Q->c[ax]), d.cell, d.inclusive);
+                            if (hit) add(r2);
+                        }
+                        r2 = Q->next;
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        const int n = *cnt;
+        if (n > kConflictCap) {
+            if (lane == 0) atomicMin(&c.trunc, r);
+        } else {
+            for (int i = lane; i < n; i += 32) d.clist[(int64_t)r * kConflictCap + i] = lst[i];
+            if (lane == 0) d.ccount[r] = n;
+        }
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------- resolver
+
+// One warp per universe: survivors in index order; admit survivor r iff the
+// sequential-RSA rule holds against the round's earlier admissions.
+__global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, UniCtl* ctl,
+                                               RoundInfo* info) {
+    __shared__ int32_t acc_s[kSmaxCap];
+    __shared__ int32_t gid_s[kSmaxCap];
+    const int u = blockIdx.x;
+    const int lane = threadIdx.x;
+    const UniDev& d = U[u];
+    UniCtl& c = ctl[u];
+    if (c.B == 0) return;
+    const int S = c.S;
+    const int S_eff = c.trunc < S ? c.trunc : S;
+    const bool group = group_phase(d, c);
+    const bool unique_group = d.group_mode == GROUP_UNIQUE;
+    const int64_t room = d.slot_cap - c.n_slots;
+    int k = 0, stop_at = S_eff;
+    int64_t n_unique = c.n_unique, n_sub = c.n_sub;
+    bool grow = false, hit_max = false;
+    for (int r = 0; r < S_eff; r++) {
+        if (k >= room) {
+            stop_at = r;
+            grow = true;
+            break;
+        }
+        const int n = d.ccount[r];
+        const int32_t* lst = d.clist + (int64_t)r * kConflictCap;
+        bool accept;
+        int32_t gid;
+        if (!group) {
+            bool any = false;
+            for (int i = lane; i < n; i += 32) any |= acc_s[lst[i]] >= 0;
+            accept = !__any_sync(0xffffffffu, any);
+            gid = (int32_t)(c.n_slots + k);
+        } else {
+            // union of the pre-round group and the groups of admitted earlier survivors
+            int32_t mine = -1;
+            bool two = false;
+            for (int i = lane; i < n; i += 32) {
+                const int r2 = lst[i];
+                if (acc_s[r2] >= 0) {
+                    const int32_t g2 = gid_s[r2];
+                    if (mine == -1)
+                        mine = g2;
+                    else if (mine != g2)
+                        two = true;
+                }
+            }
+            const int32_t g0 = d.g0[d.surv_off[r]];
+            int32_t first = g0;
+            for (int o = 0; o < 32; o++) {
+                const int32_t v = __shfl_sync(0xffffffffu, mine, o);
+                if (first == -1) first = v;
+            }
+            two = two || (mine != -1 && mine != first);
+            two = __any_sync(0xffffffffu, two);
+            if (two) {
+                accept = false;
+                gid = -1;
+            } else if (first == -1) {
+                accept = unique_group;  // touches nothing: founds a group, or (subpath) rejected
+                gid = (int32_t)(c.n_slots + k);
+            } else {
+                accept = true;
+                gid = first;
+            }
+        }
+        if (lane == 0) {
+            acc_s[r] = accept ? k : -1;
+            gid_s[r] = accept ? gid : -1;
+        }
+        __syncwarp();
+        if (accept) {
+            k++;
+            if (!group || (unique_group && gid == (int32_t)(c.n_slots + k - 1)))
+                n_unique++;
+            else
+                n_sub++;
+            if (c.phase == 1 && c.max_n > 0 && n_unique >= c.max_n) {
+                stop_at = r + 1;
+                hit_max = true;
+                break;
+            }
+        }
+    }
+    for (int r = lane; r < S; r += 32) {
+        d.acc_rank[r] = r < stop_at ? acc_s[r] : -1;
+        d.sgid[r] = r < stop_at ? gid_s[r] : -1;
+    }
+    if (lane != 0) return;
+    int64_t next;
+    if (hit_max)
+        next = c.round_base + d.surv_off[stop_at - 1] + 1;
+    else if (stop_at < c.S_raw)
+        next = c.round_base + d.surv_off[stop_at];
+    else
+        next = c.round_base + c.B;
+    const int64_t used = next - c.round_base;
+    c.stop_at = stop_at;
+    c.n_slots_prev = c.n_slots;
+    c.n_slots += k;
+    c.n_unique = n_unique;
+    c.n_sub = n_sub;
+    c.accepted_round = k;
+    c.next_cand = next;
+    c.attempts = next;
+    c.rounds++;
+    if (grow) c.state = ST_GROW;
+    // round-size adaptation toward 64..512 survivors (braid_cuda.cu:921-924);
+    // admission results do not depend on it
+    if (c.S_raw > 512 && c.round_B > c.B_min)
+        c.round_B >>= 1;
+    else if (c.S_raw < 64 && c.round_B < c.B_cap)
+        c.round_B <<= 1;
+    // windowed accept-rate stop
+    const double thr = c.phase == 1 ? c.accept_rate : c.sub_accept_rate;
+    if (thr > 0 && c.win_target > 0 && used > 0) {
+        const int64_t bucket = c.win_target / 32 > 0 ? c.win_target / 32 : 1;
+        int last = (c.win_head + c.win_len - 1) & 63;
+        if (c.win_len == 0 || c.win_b[last] >= bucket) {
+            if (c.win_len == 64) {  // drop the oldest bucket
+                c.win_att -= c.win_b[c.win_head];
+                c.win_adm -= c.win_a[c.win_head];
+                c.win_head = (c.win_head + 1) & 63;
+                c.win_len--;
+            }
+            last = (c.win_head + c.win_len) & 63;
+            c.win_b[last] = 0;
+            c.win_a[last] = 0;
+            c.win_len++;
+        }
+        c.win_b[last] += used;
+        c.win_a[last] += k;
+        c.win_att += used;
+        c.win_adm += k;
+        while (c.win_len > 1 && c.win_att - c.win_b[c.win_head] >= c.win_target) {
+            c.win_att -= c.win_b[c.win_head];
+            c.win_adm -= c.win_a[c.win_head];
+            c.win_head = (c.win_head + 1) & 63;
+            c.win_len--;
+        }
+        const int64_t in_phase = c.phase == 1 ? next : next - c.phase1_end;
+        if (c.win_att >= c.win_target && in_phase > 1000000 &&
+            (double)c.win_adm / (double)c.win_att < thr)
+            c.phase_end = next;  // ends this phase at the next plan
+    }
+}
+
+// ---------------------------------------------------------------- commit
+
+__device__ __forceinline__ void grid_insert(const UniDev& d, UniCtl& c, int t, int64_t lin,
+                                            int64_t cpt, int32_t slot, int32_t* old_head) {
+    if (d.grid_kind == GRID_DENSE) {
+        *old_head = atomicExch(d.heads + (int64_t)t * cpt + lin, slot);
+        return;
+    }
+    const uint64_t key = ((uint64_t)t << 40) | (uint64_t)lin;
+    uint64_t h = mix64(key) & d.hmask;
+    for (uint64_t probe = 0; probe <= d.hmask; probe++) {
+        uint64_t k = __ldcg(d.hkeys + h);
+        if (k == kEmptyKey) {
+            const uint64_t prev = atomicCAS((unsigned long long*)(d.hkeys + h), kEmptyKey, key);
+            if (prev == kEmptyKey) {
+                atomicAdd((unsigned long long*)&c.hash_used, 1ull);
+                k = key;
+            } else {
+                k = prev;
+            }
+        }
+        if (k == key) {
+            *old_head = atomicExch(d.heads + h, slot);
+            return;
+        }
+        h = (h + 1) & d.hmask;
+    }
+    *old_head = -1;
+    c.err_code = 3;  // hash full (host keeps the load factor below 1/2)
+    c.state = ST_ERROR;
+}
+
+__global__ void __launch_bounds__(256) k_commit(const UniDev* __restrict__ U, UniCtl* ctl,
+                                                RoundInfo* info) {
+    const int n_uni = info->n_uni, total = info->total_surv;
+    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
+    // items: survivor-major, T per survivor; T varies per universe so walk
+    // survivors and let each thread stride over (survivor, t) within it.
+    for (int64_t w = gtid; w < (int64_t)total * kMaxF; w += nthr) {
+        const int item = (int)(w / kMaxF);
+        const int t = (int)(w % kMaxF);
+        const int u = find_uni(info->surv_off, n_uni, item);
+        const UniDev& d = U[u];
+        if (t >= d.T) continue;
+        UniCtl& c = ctl[u];
+        const int r = item - info->surv_off[u];
+        if (r >= c.stop_at) continue;
+        const int k = d.acc_rank[r];
+        if (k < 0) continue;
+        const int64_t slot = c.n_slots_prev + k;
+        Pt64 q = d.spos[(int64_t)r * d.T + t];
+        int cc[3];
+        for (int ax = 0; ax < d.dim; ax++) cc[ax] = cell_of(q.c[ax], d.cell, d.gw);
+        int32_t old;
+        grid_insert(d, c, t, lin_cell(cc, d.dim, d.gw), cells_per_t(d), (int32_t)slot, &old);
+        q.next = old;
+        q.gid = d.sgid[r];
+        d.pts[slot * d.T + t] = q;
+        Pt32 f;
+        f.c[0] = (float)q.c[0];
+        f.c[1] = (float)q.c[1];
+        f.c[2] = (float)q.c[2];
+        f.next = old;
+        d.ptf[slot * d.T + t] = f;
+        if (t == 0) d.acc_idx[slot] = c.round_base + d.surv_off[r];
+    }
+}
+
+// Rebuild the main-grid hash of universe u from its committed points (after
+// the host swapped in a larger, empty table).
+__global__ void k_rehash(const UniDev* __restrict__ U, UniCtl* ctl, int u, int64_t n_slots) {
+    const UniDev& d = U[u];
+    UniCtl& c = ctl[u];
+    const int64_t total = n_slots * d.T;
+    for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < total;
+         w += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t slot = w / d.T;
+        const int t = (int)(w % d.T);
+        Pt64* q = d.pts + slot * d.T + t;
+        int cc[3];
+        for (int ax = 0; ax < d.dim; ax++) cc[ax] = cell_of(q->c[ax], d.cell, d.gw);
+        int32_t old;
+        grid_insert(d, c, t, lin_cell(cc, d.dim, d.gw), cells_per_t(d), (int32_t)slot, &old);
+        q->next = old;
+        d.ptf[slot * d.T + t].next = old;
+    }
+}
+
+}  // namespace ug
+
+namespace ug {
+
+// Worldline parameters in term order (the --dump-params content): knot mode
+// replays the reference draw sequence (cuda/braid_knot.cu:111-166) keeping
+// each term; the Philox stream lists term j = frequency j + 2.
+__global__ void k_params(const UniDev* __restrict__ U, int u, int64_t n, double* a2o, double* ao,
+                         int32_t* bo, double* fo) {
+    const UniDev& d = U[u];
+    const int D = d.dim, nw = d.nw, F = d.F;
+    double wj[kMaxF];
+    int32_t bj[kMaxF];
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t idx = (uint64_t)d.acc_idx[s];
+        if (d.rng == RNG_KNOT) {
+            Xo r;
+            r.seed(knot_seed(d.seed, idx));
+            for (int ax = 0; ax < D; ax++) {
+                const int64_t o = (s * D + ax) * nw;
+                if ((uint32_t)nw == d.modmax) {
+                    for (int j = 0; j < nw; j++) bj[j] = j + 2;
+                    for (int j = nw - 1; j > 0; j--) {
+                        const int k = (int)r.below((uint32_t)(j + 1));
+                        const int32_t tmp = bj[j];
+                        bj[j] = bj[k];
+                        bj[k] = tmp;
+                    }
+                } else {
+                    for (int j = 0; j < nw; j++) {
+                        int bnew = 0;
+                        bool dup = true;
+                        for (int guard = 0; dup && guard < 64; guard++) {
+                            bnew = (int)r.below(d.modmax) + 2;
+                            dup = false;
+                            for (int k = 0; k < j; k++)
+                                if (bj[k] == bnew) dup = true;
+                        }
+                        bj[j] = bnew;
+                    }
+                }
+                double sum = 0.0;
+                for (int j = 0; j < nw; j++) {
+                    wj[j] = -log(1.0 - r.f64());
+                    sum += wj[j];
+                }
+                for (int j = 0; j < nw; j++) wj[j] /= sum;
+                for (int j = 0; j < nw; j++) {
+                    double amp = wj[j] / (double)bj[j];
+                    if (r.flip()) amp = -amp;
+                    ao[o + j] = amp;
+                    bo[o + j] = bj[j];
+                    fo[o + j] = (bj[j] % 2 == 0) ? r.f64() * kPi : 0.0;
+                }
+                a2o[s * D + ax] = d.pin ? 0.0 : (r.f64() * 2.0 - 1.0);
+            }
+        } else {
+            for (int ax = 0; ax < D; ax++) {
+                const int64_t o = (s * D + ax) * nw;
+                double sum = 0.0;
+                for (int p = 0; 2 * p <= F; p++) {
+                    const uint4 q = philox_block(d.seed, idx, ax, p);
+                    if (p == 0) {
+                        a2o[s * D + ax] = d.pin ? 0.0 : (double)q.x * (1.0 / 2147483648.0) - 1.0;
+                        continue;
+                    }
+                    const int be = 2 * p, bo2 = 2 * p + 1;
+                    const double Ee = -log(((double)q.x + 0.5) * (1.0 / 4294967296.0));
+                    sum += Ee;
+                    ao[o + be - 2] = (q.z & 1u) ? -Ee : Ee;
+                    fo[o + be - 2] = (double)(q.z >> 1) * (1.0 / 2147483648.0) * kPi;
+                    bo[o + be - 2] = be;
+                    if (bo2 <= F) {
+                        const double Eo = -log(((double)q.y + 0.5) * (1.0 / 4294967296.0));
+                        sum += Eo;
+                        ao[o + bo2 - 2] = (q.w & 1u) ? -Eo : Eo;
+                        fo[o + bo2 - 2] = 0.0;
+                        bo[o + bo2 - 2] = bo2;
+                    }
+                }
+                for (int j = 0; j < nw; j++) {
+                    const double e = ao[o + j];
+                    double amp = fabs(e) / sum / (double)(j + 2);
+                    ao[o + j] = e < 0.0 ? -amp : amp;
+                }
+            }
+        }
+    }
+}
+
+void launch_params(const UniDev* dU, int u, int64_t n, double* a2, double* a, int32_t* b, double* f,
+                   cudaStream_t st) {
+    const int blocks = (int)std::min<int64_t>((n + 127) / 128, 4096);
+    k_params<<<blocks, 128, 0, st>>>(dU, u, n, a2, a, b, f);
+}
+
+}  // namespace ug

@@ -1,0 +1,51 @@
+// ug_kernels.cuh -- declarations shared by the round-pipeline kernels and
+// the host runtime.
+#pragma once
+#include "ug_device.cuh"
+
+namespace ug {
+
+constexpr int kMaxUni = 1024;
+
+// Work decomposition of one round across all universes (device resident).
+struct RoundInfo {
+    int32_t n_uni;
+    int32_t total_tiles;
+    int32_t total_surv;
+    int32_t compact_done;
+    int32_t any_active;
+    int32_t mixed_ok;      // universes in the mixed prefilter this round
+    int32_t pad[2];
+    int32_t tile_off[kMaxUni + 1];
+    int32_t surv_off[kMaxUni + 1];
+};
+
+__device__ __forceinline__ int find_uni(const int32_t* off, int n, int item) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= item)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// Kernels (ug_kernels.cu)
+__global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
+__global__ void k_prefilter64(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
+__global__ void k_confirm64(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
+__global__ void k_compact(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
+__global__ void k_surv_eval(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
+__global__ void k_conflicts(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
+__global__ void k_greedy(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
+__global__ void k_commit(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
+__global__ void k_rehash(const UniDev* __restrict__ U, UniCtl* ctl, int u, int64_t n_slots);
+
+// Shared memory of k_surv_eval per warp (bytes), for F <= kMaxF.
+constexpr int kSurvWarps = 4;
+constexpr size_t kSurvSmemPerWarp = (size_t)3 * (kMaxF + 1) * 2 * sizeof(double) + 3 * sizeof(double) +
+                                    (size_t)kMaxF * (sizeof(int32_t) + sizeof(double));
+
+}  // namespace ug
