@@ -153,3 +153,17 @@ def test_group_modes(oracle):
     u = oracle.pack(m, 20000, group_mode=oracle.GROUP_UNIQUE)
     founders = np.flatnonzero(u.gid == np.arange(len(u.gid)))
     assert len(founders) == u.n_unique and u.n_sub == len(u.gid) - u.n_unique
+
+
+def test_oracle_matches_reference_gpu_binary():
+    """Accepted sets of the reference's own GPU packer (braid_knot run on a B200)."""
+    import oracle as O
+    gold = json.load(open(os.path.join(os.path.dirname(GOLD), "braid_knot_b200.json")))
+    for r in gold["runs"]:
+        m = O.Model(dim=r["dim"], T=r["T"], rng=O.RNG_KNOT, pin=r["pin"], seed=r["seed"])
+        res = O.pack(m, r["attempts"])
+        assert list(res.acc_idx) == r["idx"], r["command"]
+        for row in r["head_rows"]:
+            p = _parse(row, r["dim"], m.nw)
+            c = O.candidate(m, p["idx"])
+            assert np.array_equal(c["a"], np.array(p["a"])) and np.array_equal(c["f"], np.array(p["f"]))

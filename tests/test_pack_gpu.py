@@ -130,3 +130,17 @@ def test_batched_universes_match_single(ug, oracle):
             idx, _ = p.accepted(k)
             ref = oracle.pack(_model(oracle, u), u.attempts)
             assert np.array_equal(idx, ref.acc_idx), k
+
+
+def test_parity_reference_gpu_binary(ug):
+    """Accepted sets of the reference's own GPU packer (braid_knot on a B200, fixture)."""
+    import json
+    import os
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "braid_knot_b200.json")))
+    for r in gold["runs"]:
+        u = ug.Universe(dim=r["dim"], T=r["T"], rng=1, pin_sin1=r["pin"], seed=r["seed"],
+                        attempts=r["attempts"], round_size=8192)
+        with ug.Packer([u]) as pk:
+            pk.run()
+            idx, _ = pk.accepted(0)
+        assert list(idx) == r["idx"], r["command"]
