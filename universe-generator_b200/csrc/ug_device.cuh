@@ -82,6 +82,14 @@ struct UniDev {
     int32_t* sgid;         // [S_max]  resolved group / -1 rejected, -2 unresolved
     int32_t* acc_rank;     // [S_max]  slot offset of accepted survivors, -1 otherwise
     int64_t* acc_idx;      // [slot_cap] candidate index of each accepted slot
+    // mixed-precision (tensor-core) prefilter
+    const uint8_t* mx_bimg;  // split-BF16 sine-basis table, one UMMA image per K chunk
+    int32_t mx_ok;           // universe runs the tensor-core prefilter
+    int32_t mx_chunks;       // K chunks of 48 coefficient entries (16 frequency pairs)
+    int32_t mx_tpad;         // timesteps padded to 16 (B rows)
+    int32_t mx_nmma;         // UMMA N per pass
+    int32_t mx_npass;        // timestep passes (2 when dim * tpad > 512 TMEM columns)
+    float mx_margin;         // guard band of the FP32 Chebyshev test
 };
 
 // Mutable per-universe control block (device).

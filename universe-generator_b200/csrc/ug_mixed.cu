@@ -1,15 +1,645 @@
-// ug_mixed.cu -- mixed-precision prefilter (placeholder until the tensor-core path lands).
+// ug_mixed.cu -- tensor-core prefilter of the RSA packer (sm_100a).
+//
+// Position evaluation is a contraction: for a tile of 128 candidates and one
+// axis,  D[m, n] = sum_k A[m, k] B[n, k]  with
+//   A[m, .] = unnormalised coefficients of candidate m, three per frequency
+//             pair p: (E_2p cos f / 2p, E_2p sin f / 2p, E_2p+1 / (2p+1)),
+//             signs folded in, generated in FP32 straight into shared memory;
+//   B[n, .] = (S_2p,t, Cm_2p,t, S_2p+1,t) / sin z_t for timestep t = order[n],
+//             an FP64 host table split into BF16 hi + lo.
+// The comoving position is X = wrap(D / sum_b E_b + a2).  A is split into
+// BF16 hi + lo as well and the product runs as three tcgen05.mma passes
+// (hi*hi + hi*lo + lo*hi) accumulating in FP32 in tensor memory.  The
+// epilogue reads D with tcgen05.ld and runs the Chebyshev test against the
+// FP32 copy of the collision grid with a guard band: a contact deeper than
+// the band rejects, a separation wider than the band clears, anything in
+// between marks the candidate for the FP64 retest (k_confirm64), so every
+// decision equals the FP64 one.
+//
+// Pipeline per CTA (128 threads, one candidate per thread, persistent over
+// tiles): shared memory holds two stages of {A_hi, A_lo, B_hi, B_lo}.  All
+// threads generate stage s while the tensor core consumes stage s^1; one
+// thread issues cp.async.bulk for the B chunk (completion on an mbarrier)
+// and the MMAs (completion via tcgen05.commit on an mbarrier).  Every wait is
+// bounded; on timeout the kernel records UG_ETIMEDOUT in the control block,
+// frees its tensor memory and returns.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
 #include "ug_mixed.cuh"
 
 namespace ug {
 
-int mixed_setup(const ug_universe_cfg&, UniDev&, MixedTables&) { return UG_ENOTSUP; }
-void mixed_free(MixedTables&) {}
-int mixed_init_kernels() { return UG_OK; }
-void launch_prefilter_mixed(const UniDev*, UniCtl*, RoundInfo*, int, cudaStream_t) {}
-int mixed_error(const UniDev*, int, const UniDev&, const MixedTables&, int64_t, int64_t, double*,
-                double*, cudaStream_t) {
-    return UG_ENOTSUP;
+constexpr int kPairsPerChunk = 16;
+constexpr int kKC = 3 * kPairsPerChunk;          // 48 coefficient entries per chunk
+constexpr int kAImgBytes = kTile * kKC * 2;      // one BF16 A image (hi or lo)
+
+// ------------------------------------------------------------ PTX helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait: gives up after ~1 s of device time.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    if (mbar_try(bar, parity)) return true;
+    const uint64_t t0 = globaltimer();
+    for (uint32_t it = 0; it < (1u << 26); it++) {
+        if (mbar_try(bar, parity)) return true;
+        if ((it & 255) == 0 && globaltimer() - t0 > 1000000000ull) break;
+    }
+    return false;
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_alloc(uint32_t* holder, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(holder)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+// D[tmem] (+)= A[smem] * B[smem]^T, BF16 inputs, FP32 accumulate, K = 16.
+__device__ __forceinline__ void umma_bf16(uint32_t dtm, uint64_t ad, uint64_t bd, uint32_t idesc,
+                                          uint32_t accum) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtm),
+        "l"(ad), "l"(bd), "r"(idesc), "r"(accum)
+        : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
+    uint32_t r[8];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Shared-memory matrix descriptor, K-major, no swizzle: 8-row x 16-byte core
+// matrices; lbo = byte stride between core matrices along K, sbo = along M/N.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// Instruction descriptor: kind::f16, BF16 x BF16 -> F32, both K-major.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// ---------------------------------------------------------- generation
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// Coefficients of one K chunk (16 frequency pairs) of candidate idx, axis ax,
+// written as BF16 hi/lo rows of the canonical A images.  Returns the chunk's
+// contribution to sum_b E_b (FP64 accumulation of the FP32 variates).
+__device__ __forceinline__ double gen_chunk(const UniDev& d, uint64_t idx, int ax, int ch, bool valid,
+                                            uint8_t* a_hi, uint8_t* a_lo, int row) {
+    const int F = d.F;
+    const int P = F >> 1;
+    float v[kKC];
+    double sum = 0.0;
+#pragma unroll
+    for (int q = 0; q < kPairsPerChunk; q++) {
+        const int p = ch * kPairsPerChunk + q + 1;
+        float ae = 0.f, be = 0.f, ao = 0.f;
+        if (valid && p <= P) {
+            const uint4 o = philox_block(d.seed, idx, ax, p);
+            const float Ee = -__logf(((float)o.x + 0.5f) * 2.3283064365386963e-10f);
+            const float f = (float)(o.z >> 1) * 4.656612873077393e-10f * 3.14159265358979f;
+            float sf, cf;
+            __sincosf(f, &sf, &cf);
+            const float re = __frcp_rn((float)(2 * p));
+            const float se = (o.z & 1u) ? -Ee * re : Ee * re;
+            ae = se * cf;
+            be = se * sf;
+            sum += (double)Ee;
+            if (2 * p + 1 <= F) {
+                const float Eo = -__logf(((float)o.y + 0.5f) * 2.3283064365386963e-10f);
+                const float ro = __frcp_rn((float)(2 * p + 1));
+                ao = (o.w & 1u) ? -Eo * ro : Eo * ro;
+                sum += (double)Eo;
+            }
+        }
+        v[3 * q] = ae;
+        v[3 * q + 1] = be;
+        v[3 * q + 2] = ao;
+    }
+#pragma unroll
+    for (int g = 0; g < kKC / 8; g++) {
+        uint32_t h[4], l[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const float x0 = v[8 * g + 2 * e], x1 = v[8 * g + 2 * e + 1];
+            const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
+            h[e] = pack_bf16x2(__bfloat162float(h0), __bfloat162float(h1));
+            l[e] = pack_bf16x2(x0 - __bfloat162float(h0), x1 - __bfloat162float(h1));
+        }
+        const int off = g * (kTile * 16) + row * 16;
+        *reinterpret_cast<uint4*>(a_hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<uint4*>(a_lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
+    }
+    return sum;
+}
+
+// ------------------------------------------------- guard-band grid test
+
+// FP32 Chebyshev test of X (dim coords) at timestep t against the committed
+// packing.  Returns 1 on a certain contact; sets *gray when a pair lies in the
+// guard band.  The cell range covers every point within r + m of X.
+__device__ __forceinline__ int test32_at(const UniDev& d, int t, const float* X, float r, float m,
+                                         float inv_cell, int64_t cpt, bool* gray) {
+    int lo[3], hi[3];
+    const float band = m * inv_cell + 1e-4f;
+    for (int ax = 0; ax < d.dim; ax++) {
+        const float u = (X[ax] + 1.0f) * inv_cell;
+        const float fl = floorf(u);
+        const float fr = u - fl;
+        int c = (int)fl;
+        c = c >= d.gw ? d.gw - 1 : (c < 0 ? 0 : c);
+        lo[ax] = c - 1 - (fr < band ? 1 : 0);
+        hi[ax] = c + 1 + (fr > 1.0f - band ? 1 : 0);
+    }
+    const float rin = r - m, rout = r + m;
+    int cc[3];
+    int cnt[3] = {1, 1, 1};
+    for (int ax = 0; ax < d.dim; ax++) cnt[ax] = hi[ax] - lo[ax] + 1;
+    const int total = cnt[0] * (d.dim > 1 ? cnt[1] : 1) * (d.dim > 2 ? cnt[2] : 1);
+    for (int k = 0; k < total; k++) {
+        int rr = k;
+        for (int ax = d.dim - 1; ax >= 0; ax--) {
+            int v = lo[ax] + rr % cnt[ax];
+            rr /= cnt[ax];
+            v %= d.gw;
+            cc[ax] = v < 0 ? v + d.gw : v;
+        }
+        int32_t p = grid_head(d, t, lin_cell(cc, d.dim, d.gw), cpt);
+        while (p >= 0) {
+            const Pt32 q = d.ptf[(int64_t)p * d.T + t];
+            bool miss = false, deep = true;
+            for (int ax = 0; ax < d.dim; ax++) {
+                const float dd = fabsf(torus_deltaf(X[ax] - q.c[ax]));
+                miss |= dd > rout;
+                deep &= dd < rin;
+            }
+            if (!miss) {
+                if (deep) return 1;
+                *gray = true;
+            }
+            p = q.next;
+        }
+    }
+    return 0;
+}
+
+// --------------------------------------------------------------- kernel
+
+struct MixedLaunch {
+    uint32_t ncols;    // tensor-memory columns per CTA
+    int tpad_max;      // widest B image (rows) of the batch: sizes the B stage
+    // debug dump of X (FP32 positions) for universe u, candidates [first, first+count)
+    float* dump;
+    int u;
+    int64_t first, count;
+};
+
+__global__ void __launch_bounds__(kTile, 1) k_prefilter_mixed(const UniDev* __restrict__ U, UniCtl* ctl,
+                                                               RoundInfo* info, MixedLaunch L) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // carve: two stages of {A_hi, A_lo, B (hi then lo)}; barriers at the end
+    const int stage_bytes = 2 * kAImgBytes + L.tpad_max * kKC * 2 * 2;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * stage_bytes);
+    uint64_t* bar_b = bar;       // [2] B chunk landed
+    uint64_t* bar_m = bar + 2;   // [2] MMAs reading the stage finished
+    uint64_t* bar_d = bar + 4;   // all MMAs of the pass finished
+    uint32_t* holder = reinterpret_cast<uint32_t*>(bar + 5);
+    int* s_flag = reinterpret_cast<int*>(bar + 6);
+
+    if (warp == 0) tmem_alloc(holder, L.ncols);
+    if (tid == 0) {
+        for (int i = 0; i < 5; i++) mbar_init(&bar[i], 1);
+        fence_mbar_init();
+        *s_flag = 0;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *holder;
+
+    uint32_t ph_b[2] = {0, 0}, ph_m[2] = {0, 0}, ph_d = 0;
+    int seq = 0;
+    bool timeout = false;
+    const bool dump = L.dump != nullptr;
+    const int n_uni = dump ? 1 : info->n_uni;
+    const int total = dump ? (int)((L.count + kTile - 1) / kTile) : info->total_tiles;
+
+    for (int tile = blockIdx.x; tile < total && !timeout; tile += gridDim.x) {
+        const int u = dump ? L.u : find_uni(info->tile_off, n_uni, tile);
+        const UniDev& d = U[u];
+        const int lt = dump ? tile : tile - info->tile_off[u];
+        const int off = lt * kTile + tid;
+        int64_t base;
+        int B;
+        if (dump) {
+            base = L.first;
+            B = (int)L.count;
+        } else {
+            base = ctl[u].round_base;
+            B = ctl[u].B;
+        }
+        const bool valid = off < B;
+        const uint64_t idx = (uint64_t)(base + off);
+        if (!d.mx_ok) {  // not eligible for the tensor-core path: everything to the FP64 test
+            const uint32_t g = __ballot_sync(0xffffffffu, valid);
+            if (lane == 0 && !dump) {
+                d.surv_bits[off >> 5] = 0u;
+                d.gray_bits[off >> 5] = g;
+            }
+            continue;
+        }
+        const int dim = d.dim, T = d.T, nch = d.mx_chunks, tpad = d.mx_tpad, nm = d.mx_nmma;
+        const uint32_t bchunk = (uint32_t)tpad * kKC * 2 * 2;  // hi + lo images
+        const uint32_t idesc = idesc_bf16(128, nm);
+        const float r = (float)d.cell, mrg = d.mx_margin, inv_cell = (float)(1.0 / d.cell);
+        const int64_t cpt = cells_per_t(d);
+        float inv_sum[3] = {0.f, 0.f, 0.f}, a2f[3] = {0.f, 0.f, 0.f};
+        int state = 0;  // 0 clear so far, 1 rejected (certain contact)
+        bool gray = false;
+        int nev = 0;
+        for (int pass = 0; pass < d.mx_npass && !timeout; pass++) {
+            if (pass > 0 && __syncthreads_and(state == 1 || !valid)) break;
+            for (int ax = 0; ax < dim && !timeout; ax++) {
+                double sumE = 0.0;
+                if (pass == 0 && valid) {
+                    const uint4 o = philox_block(d.seed, idx, ax, 0);
+                    a2f[ax] = d.pin ? 0.f : (float)((double)o.x * (1.0 / 2147483648.0) - 1.0);
+                }
+                for (int ch = 0; ch < nch; ch++, seq++) {
+                    const int st = seq & 1;
+                    uint8_t* sbase = sm + st * stage_bytes;
+                    uint8_t* a_hi = sbase;
+                    uint8_t* a_lo = sbase + kAImgBytes;
+                    uint8_t* b_img = sbase + 2 * kAImgBytes;
+                    if (seq >= 2) {
+                        if (!mbar_wait(&bar_m[st], ph_m[st])) timeout = true;
+                        ph_m[st] ^= 1;
+                    }
+                    if (__syncthreads_or(timeout)) {
+                        timeout = true;
+                        break;
+                    }
+                    if (tid == 0) {
+                        mbar_expect_tx(&bar_b[st], bchunk);
+                        bulk_g2s(b_img, d.mx_bimg + (size_t)ch * bchunk, bchunk, &bar_b[st]);
+                    }
+                    sumE += gen_chunk(d, idx, ax, ch, valid, a_hi, a_lo, tid);
+                    fence_proxy_async();
+                    __syncthreads();
+                    if (tid == 0) {
+                        if (!mbar_wait(&bar_b[st], ph_b[st])) timeout = true;
+                        tc_fence_after();
+                        if (!timeout) {
+                            const uint32_t ah = smem_u32(a_hi), al = smem_u32(a_lo);
+                            const uint32_t bh = smem_u32(b_img) + (uint32_t)(pass * nm * 16);
+                            const uint32_t bl = bh + (uint32_t)tpad * kKC * 2;
+                            const uint32_t dtm = tmem + (uint32_t)(ax * nm);
+#pragma unroll
+                            for (int j = 0; j < kKC / 16; j++) {
+                                const uint64_t dah = sdesc(ah + j * 2 * (kTile * 16), kTile * 16, 128);
+                                const uint64_t dal = sdesc(al + j * 2 * (kTile * 16), kTile * 16, 128);
+                                const uint64_t dbh = sdesc(bh + j * 2 * (tpad * 16), tpad * 16, 128);
+                                const uint64_t dbl = sdesc(bl + j * 2 * (tpad * 16), tpad * 16, 128);
+                                umma_bf16(dtm, dah, dbh, idesc, (ch > 0 || j > 0) ? 1u : 0u);
+                                umma_bf16(dtm, dah, dbl, idesc, 1u);
+                                umma_bf16(dtm, dal, dbh, idesc, 1u);
+                            }
+                        }
+                        umma_commit(&bar_m[st]);
+                    }
+                    ph_b[st] ^= 1;
+                }
+                if (pass == 0) inv_sum[ax] = valid ? (float)(1.0 / sumE) : 0.f;
+            }
+            if (timeout) break;
+            if (tid == 0) umma_commit(bar_d);
+            if (!mbar_wait(bar_d, ph_d)) timeout = true;
+            ph_d ^= 1;
+            if (__syncthreads_or(timeout)) {
+                timeout = true;
+                break;
+            }
+            tc_fence_after();
+            // epilogue: columns of this pass in endpoint-first order
+            const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+            for (int c0 = 0; c0 < nm; c0 += 8) {
+                const int col0 = pass * nm + c0;
+                if (col0 >= T) break;
+                if (!dump && __all_sync(0xffffffffu, state == 1 || !valid)) break;
+                float x[3][8];
+                for (int ax = 0; ax < dim; ax++) tmem_ld8(lane_base + (uint32_t)(ax * nm + c0), x[ax]);
+                tmem_wait_ld();
+                for (int j = 0; j < 8; j++) {
+                    const int col = col0 + j;
+                    if (col >= T) break;
+                    const int t = __ldg(d.order + col);
+                    float X[3];
+                    for (int ax = 0; ax < dim; ax++) X[ax] = torus_wrapf(fmaf(x[ax][j], inv_sum[ax], a2f[ax]));
+                    if (dump) {
+                        if (valid)
+                            for (int ax = 0; ax < dim; ax++)
+                                L.dump[((size_t)off * T + t) * dim + ax] = X[ax];
+                        continue;
+                    }
+                    if (!valid || state == 1) continue;
+                    nev++;
+                    if (test32_at(d, t, X, r, mrg, inv_cell, cpt, &gray)) state = 1;
+                }
+            }
+            tc_fence_before();
+            __syncthreads();
+        }
+        if (!dump) {
+            const bool surv = valid && state == 0 && !gray && !timeout;
+            const bool gr = valid && state == 0 && (gray || timeout);
+            const uint32_t sb = __ballot_sync(0xffffffffu, surv);
+            const uint32_t gb = __ballot_sync(0xffffffffu, gr);
+            if (lane == 0) {
+                d.surv_bits[off >> 5] = sb;
+                d.gray_bits[off >> 5] = gb;
+            }
+            int ng = __popc(gb);
+            for (int o = 16; o > 0; o >>= 1) nev += __shfl_xor_sync(0xffffffffu, nev, o);
+            if (lane == 0) {
+                if (nev) atomicAdd((unsigned long long*)&ctl[u].evals, (unsigned long long)nev);
+                if (ng) {
+                    atomicAdd(&ctl[u].n_gray, ng);
+                    atomicAdd((unsigned long long*)&ctl[u].gray_total, (unsigned long long)ng);
+                }
+            }
+        }
+    }
+    if (timeout && tid == 0 && !dump) {
+        for (int v = 0; v < n_uni; v++) {
+            ctl[v].err_code = UG_ETIMEDOUT;
+            ctl[v].state = ST_ERROR;
+        }
+    }
+    // drain: the last commits of this CTA must land before tensor memory is freed
+    if (tid == 0 && seq > 0) {
+        const int s1 = (seq - 1) & 1;
+        mbar_wait(&bar_m[s1], ph_m[s1]);
+        if (seq > 1) mbar_wait(&bar_m[s1 ^ 1], ph_m[s1 ^ 1]);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) tmem_dealloc(tmem, L.ncols);
+}
+
+// FP64 positions of candidates [first, first+count) (Philox stream) for the
+// achieved-error measurement.
+__global__ void k_pos64(const UniDev* __restrict__ U, int u, int64_t first, int64_t count, double* out) {
+    const UniDev& d = U[u];
+    double alpha[3 * (kMaxF + 1)], beta[3 * (kMaxF + 1)], a2[3];
+    const int F1 = d.F + 1;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t idx = (uint64_t)(first + i);
+        for (int ax = 0; ax < d.dim; ax++) a2[ax] = gen_philox64(d, idx, ax, alpha + ax * F1, beta + ax * F1, 1);
+        for (int t = 0; t < d.T; t++)
+            for (int ax = 0; ax < d.dim; ax++)
+                out[((size_t)i * d.T + t) * d.dim + ax] = eval64(d, alpha + ax * F1, beta + ax * F1, 1, a2[ax], t);
+    }
+}
+
+// ------------------------------------------------------------------ host
+
+static int g_ncols = 32;
+static int g_tpad_max = 16;
+static size_t g_smem = 0;
+static int g_ctas_per_sm = 1;
+
+static size_t smem_bytes() { return (size_t)2 * (2 * kAImgBytes + g_tpad_max * kKC * 2 * 2) + 64; }
+
+static uint16_t bf16_bits(float x) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    return *reinterpret_cast<const uint16_t*>(&h);
+}
+static float bf16_val(uint16_t b) {
+    uint32_t u = (uint32_t)b << 16;
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+}
+
+int mixed_setup(const ug_universe_cfg& cfg, UniDev& d, MixedTables& mt) {
+    const int T = cfg.T, F = cfg.T, dim = cfg.dim;
+    d.mx_ok = (cfg.rng == UG_RNG_PHILOX && !cfg.cross1d && cfg.group_mode == UG_GROUP_NONE) ? 1 : 0;
+    const int P = F / 2;
+    const int nch = (P + kPairsPerChunk - 1) / kPairsPerChunk;
+    // B rows: timesteps padded to 16; when dim * rows exceeds the 512 tensor
+    // memory columns, two passes of exactly half the (32-padded) rows each
+    int tpad = (T + 15) / 16 * 16;
+    int nm = tpad, npass = 1;
+    if (dim * tpad > 512) {
+        tpad = (T + 31) / 32 * 32;
+        nm = tpad / 2;
+        npass = 2;
+    }
+    d.mx_chunks = nch;
+    d.mx_tpad = tpad;
+    d.mx_nmma = nm;
+    d.mx_npass = npass;
+    // guard band: split-BF16 product error 3 * 2^-16 * sum|A||B| with
+    // sum|A||B| / sum E <= 2 (|sin bz| <= b sin z, |cos bz - 1| <= b sin z for even b),
+    // FP32 accumulation of 3K products (<= 2^-23 each, relative to the same sum),
+    // FP32 generation (logf, sincosf, reciprocals: < 2e-6), stored FP32 points and
+    // the FP32 subtraction (< 4e-7); doubled for safety.
+    const int K = nch * kKC;
+    const double m = 2.0 * (3.0 * std::ldexp(1.0, -16) * 2.0 + 3.0 * K * std::ldexp(1.0, -23) * 2.0 + 2e-6) + 4e-7;
+    d.mx_margin = (float)m;
+    mt.margin = m;
+    mt.K = K;
+    mt.Tp = tpad;
+    // B images
+    std::vector<double> S((size_t)(F + 1) * T), Cm((size_t)(F + 1) * T), inv(T);
+    std::vector<int32_t> order(T);
+    {
+        std::vector<double> z(T);
+        for (int i = 0; i < T; i++) {
+            z[i] = cfg.zgrid == UG_ZGRID_REF ? (i + 1) * kPi / (T + 1) : (i + 0.5) * kPi / T;
+            inv[i] = 1.0 / sin(z[i]);
+        }
+        for (int b = 0; b <= F; b++)
+            for (int t = 0; t < T; t++) {
+                S[(size_t)b * T + t] = sin(b * z[t]);
+                Cm[(size_t)b * T + t] = cos(b * z[t]) - 1.0;
+            }
+        for (int i = 0; i < T; i++) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            return std::min(a, T - 1 - a) < std::min(b, T - 1 - b);
+        });
+    }
+    const size_t img = (size_t)tpad * kKC;  // BF16 elements per hi (or lo) image
+    std::vector<uint16_t> host((size_t)nch * 2 * img, 0);
+    for (int ch = 0; ch < nch; ch++) {
+        uint16_t* hi = host.data() + (size_t)ch * 2 * img;
+        uint16_t* lo = hi + img;
+        for (int kk = 0; kk < kKC; kk++) {
+            const int p = ch * kPairsPerChunk + kk / 3 + 1, s = kk % 3;
+            for (int n = 0; n < tpad; n++) {
+                double v = 0.0;
+                if (n < T && p <= P) {
+                    const int t = order[n];
+                    const int b = s == 2 ? 2 * p + 1 : 2 * p;
+                    if (b <= F) v = (s == 1 ? Cm[(size_t)b * T + t] : S[(size_t)b * T + t]) * inv[t];
+                }
+                const uint16_t h = bf16_bits((float)v);
+                const uint16_t l = bf16_bits((float)(v - (double)bf16_val(h)));
+                const size_t e = (size_t)(kk / 8) * (tpad * 8) + (size_t)n * 8 + (kk % 8);
+                hi[e] = h;
+                lo[e] = l;
+            }
+        }
+    }
+    void* dimg = nullptr;
+    if (cudaMalloc(&dimg, host.size() * 2) != cudaSuccess) return UG_ENOMEM;
+    if (cudaMemcpy(dimg, host.data(), host.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess) return UG_ECUDA;
+    mt.bhi = dimg;
+    d.mx_bimg = (const uint8_t*)dimg;
+    // tensor-memory columns: the widest universe decides (power of two >= 32)
+    if (tpad > g_tpad_max) g_tpad_max = tpad;
+    int cols = dim * nm;
+    int nc = 32;
+    while (nc < cols) nc <<= 1;
+    if (nc > g_ncols) g_ncols = nc;
+    return UG_OK;
+}
+
+void mixed_free(MixedTables& mt) {
+    if (mt.bhi) cudaFree(mt.bhi);
+    mt.bhi = nullptr;
+}
+
+int mixed_init_kernels() {
+    g_smem = smem_bytes();
+    // UG_SMEM_PAD=1: request (nearly) all shared memory, one CTA per SM
+    const char* pad = getenv("UG_SMEM_PAD");
+    if (pad && pad[0] == '1') g_smem = std::max<size_t>(g_smem, 220 * 1024);
+    // at most 512 / ncols CTAs per SM may hold tensor memory at once: pad the
+    // shared-memory request so that no more than that many are resident
+    const int by_tmem = 512 / g_ncols;
+    int dev = 0, smem_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    size_t req = g_smem;
+    const size_t per_cta_reserved = 1024;
+    int fit = (int)(smem_sm / (req + per_cta_reserved));
+    if (fit > by_tmem) req = smem_sm / (by_tmem + 1) - per_cta_reserved + 16;
+    g_smem = std::max(req, g_smem);
+    g_ctas_per_sm = std::max(1, std::min(by_tmem, (int)(smem_sm / (g_smem + per_cta_reserved))));
+    if (cudaFuncSetAttribute(k_prefilter_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g_smem) !=
+        cudaSuccess)
+        return UG_ECUDA;
+    return UG_OK;
+}
+
+void launch_prefilter_mixed(const UniDev* dU, UniCtl* dCtl, RoundInfo* dInfo, int nsm, cudaStream_t st) {
+    MixedLaunch L{(uint32_t)g_ncols, g_tpad_max, nullptr, 0, 0, 0};
+    k_prefilter_mixed<<<nsm * g_ctas_per_sm, kTile, g_smem, st>>>(dU, dCtl, dInfo, L);
+}
+
+int mixed_error(const UniDev* dU, int u, const UniDev& d, const MixedTables& mt, int64_t first, int64_t count,
+                double* max_err, double* margin, cudaStream_t st) {
+    if (!d.mx_ok) return UG_ENOTSUP;
+    const size_t n = (size_t)count * d.T * d.dim;
+    float* d32 = nullptr;
+    double* d64 = nullptr;
+    if (cudaMalloc(&d32, n * 4) != cudaSuccess || cudaMalloc(&d64, n * 8) != cudaSuccess) return UG_ENOMEM;
+    cudaMemsetAsync(d32, 0, n * 4, st);
+    MixedLaunch L{(uint32_t)g_ncols, g_tpad_max, d32, u, first, count};
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
+    k_prefilter_mixed<<<nsm * g_ctas_per_sm, kTile, g_smem, st>>>(dU, nullptr, nullptr, L);
+    k_pos64<<<(int)std::min<int64_t>((count + 127) / 128, 2048), 128, 0, st>>>(dU, u, first, count, d64);
+    std::vector<float> h32(n);
+    std::vector<double> h64(n);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaMemcpy(h32.data(), d32, n * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(h64.data(), d64, n * 8, cudaMemcpyDeviceToHost);
+    cudaFree(d32);
+    cudaFree(d64);
+    if (e != cudaSuccess) return UG_ECUDA;
+    double mx = 0.0;
+    for (size_t i = 0; i < n; i++) {
+        double df = fabs((double)h32[i] - h64[i]);
+        df = std::min(df, 2.0 - df);
+        mx = std::max(mx, df);
+    }
+    *max_err = mx;
+    *margin = mt.margin;
+    return UG_OK;
 }
 
 }  // namespace ug
