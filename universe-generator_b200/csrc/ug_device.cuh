@@ -64,6 +64,18 @@ struct UniDev {
     int32_t* heads;        // dense: [T * gw^dim]; hash: values [hcap]
     uint64_t* hkeys;       // hash keys [hcap]
     uint64_t hmask;        // hcap - 1
+    // occupancy bitmap: one bit per (timestep, coarse cell); a coarse cell is
+    // 2^occ_shift cells per axis.  A clear bit proves the cells empty, so
+    // empty neighbourhoods cost one L2-resident word instead of a grid probe.
+    uint32_t* occ;
+    int32_t occ_shift;
+    int32_t occ_gw;        // coarse cells per axis
+    int64_t occ_per_t;     // coarse cells per timestep
+    // second level: one bit per block of 8 (occ cells) per axis, L2-resident
+    uint32_t* occ1;
+    int32_t occ1_gw;
+    int32_t pad3;
+    int64_t occ1_per_t;
     // accepted points
     Pt64* pts;             // [slot_cap * T]
     Pt32* ptf;             // [slot_cap * T]
@@ -73,6 +85,7 @@ struct UniDev {
     uint32_t* gray_bits;   // [B_max / 32]
     int32_t* g0;           // [B_max]  group mode: single pre-round group touched (-1 none)
     int32_t* surv_off;     // [S_max]  candidate offset within the round
+    int32_t* gray_off;     // [B_max]  mixed: offsets of candidates sent to the FP64 retest
     Pt64* spos;            // [S_max * T]
     uint64_t* rkeys;       // round hash keys [rcap]: epoch<<40 | t<<31 | cell
     uint64_t* rvals;       // [rcap]: epoch<<32 | head survivor rank
@@ -380,6 +393,47 @@ __device__ __forceinline__ int64_t cells_per_t(const UniDev& U) {
     return n;
 }
 
+__device__ __forceinline__ int64_t occ_bit(const UniDev& U, int t, const int* c) {
+    int64_t lin = 0;
+    for (int ax = 0; ax < U.dim; ax++) lin = lin * U.occ_gw + (c[ax] >> U.occ_shift);
+    return (int64_t)t * U.occ_per_t + lin;
+}
+__device__ __forceinline__ bool occ_test(const UniDev& U, int t, const int* c) {
+    const int64_t b = occ_bit(U, t, c);
+    return (__ldcg(U.occ + (b >> 5)) >> (b & 31)) & 1u;
+}
+__device__ __forceinline__ int64_t occ1_bit(const UniDev& U, int t, const int* c) {
+    int64_t lin = 0;
+    for (int ax = 0; ax < U.dim; ax++) lin = lin * U.occ1_gw + (c[ax] >> (U.occ_shift + 3));
+    return (int64_t)t * U.occ1_per_t + lin;
+}
+// True when some cell of the box [lo, hi] (per axis, taken modulo gw) may hold
+// a point at timestep t: checks the second-level bits covering the box.
+__device__ __forceinline__ bool occ1_any(const UniDev& U, int t, const int* lo, const int* hi) {
+    int v[3][4], n[3] = {1, 1, 1};
+    const int sh = U.occ_shift + 3;
+    for (int ax = 0; ax < U.dim; ax++) {
+        n[ax] = 0;
+        for (int c = lo[ax]; c <= hi[ax]; c++) {
+            int w = c % U.gw;
+            w = (w < 0 ? w + U.gw : w) >> sh;
+            bool seen = false;
+            for (int k = 0; k < n[ax]; k++) seen |= v[ax][k] == w;
+            if (!seen && n[ax] < 4) v[ax][n[ax]++] = w;
+        }
+    }
+    for (int i0 = 0; i0 < n[0]; i0++)
+        for (int i1 = 0; i1 < (U.dim > 1 ? n[1] : 1); i1++)
+            for (int i2 = 0; i2 < (U.dim > 2 ? n[2] : 1); i2++) {
+                int64_t lin = v[0][i0];
+                if (U.dim > 1) lin = lin * U.occ1_gw + v[1][i1];
+                if (U.dim > 2) lin = lin * U.occ1_gw + v[2][i2];
+                const int64_t b = (int64_t)t * U.occ1_per_t + lin;
+                if ((__ldcg(U.occ1 + (b >> 5)) >> (b & 31)) & 1u) return true;
+            }
+    return false;
+}
+
 // Contacts of the point P (dim coords) at timestep t with the accepted
 // packing.  Unique mode: returns true on the first contact.  Group mode:
 // accumulates the single touched group in *g and returns true when a second
@@ -388,6 +442,14 @@ __device__ __forceinline__ bool contacts64(const UniDev& U, int t, const double*
                                            int32_t* g, int64_t cpt) {
     int c[3];
     for (int ax = 0; ax < U.dim; ax++) c[ax] = cell_of(P[ax], U.cell, U.gw);
+    {
+        int lo[3], hi[3];
+        for (int ax = 0; ax < U.dim; ax++) {
+            lo[ax] = c[ax] - 1;
+            hi[ax] = c[ax] + 1;
+        }
+        if (!occ1_any(U, t, lo, hi)) return false;
+    }
     int nb = U.dim == 1 ? 3 : (U.dim == 2 ? 9 : 27);
     for (int k = 0; k < nb; k++) {
         int cc[3], r = k;
@@ -398,6 +460,7 @@ __device__ __forceinline__ bool contacts64(const UniDev& U, int t, const double*
             v = v < 0 ? v + U.gw : (v >= U.gw ? v - U.gw : v);
             cc[ax] = v;
         }
+        if (!occ_test(U, t, cc)) continue;
         int32_t p = grid_head(U, t, lin_cell(cc, U.dim, U.gw), cpt);
         while (p >= 0) {
             const Pt64* q = U.pts + (int64_t)p * U.T + t;

@@ -44,7 +44,7 @@ static int fail(int code, const char* fmt, ...) {
 
 enum KernelId { K_PLAN, K_PRE, K_MIXED, K_CONFIRM, K_COMPACT, K_SEVAL, K_CONFL, K_GREEDY, K_COMMIT, K_NK };
 static const char* kKernelNames[12] = {"k_plan",    "k_prefilter64", "k_prefilter_mixed",
-                                       "k_confirm64", "k_compact",   "k_surv_eval",
+                                       "k_confirm64w", "k_compact",   "k_surv_eval",
                                        "k_conflicts", "k_greedy",    "k_commit",
                                        "",           "",            ""};
 
@@ -54,6 +54,7 @@ struct UniHost {
     std::vector<void*> owned;  // fixed-size allocations
     int64_t dense_bytes = 0;
     int64_t hcap = 0;
+    int64_t occ_words = 0, occ1_words = 0;
     MixedTables mt;            // tensor-core operand tables (mixed precision)
 };
 
@@ -232,6 +233,31 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
         if ((rc = alloc_hash(h, pow2_at_least(std::max<int64_t>(1 << 16, 4LL * d.S_max * T)))))
             return rc;
     }
+    // occupancy bitmap, coarsened until it is at most 256 MiB
+    {
+        int sh = 0;
+        int64_t bits;
+        for (;; sh++) {
+            const int64_t g = (d.gw + (1 << sh) - 1) >> sh;
+            int64_t per = 1;
+            for (int ax = 0; ax < c.dim; ax++) per *= g;
+            bits = (int64_t)T * per;
+            if (bits <= ((int64_t)1 << 31) || sh >= 4) {
+                d.occ_shift = sh;
+                d.occ_gw = (int32_t)g;
+                d.occ_per_t = per;
+                break;
+            }
+        }
+        h.occ_words = (bits + 31) / 32;
+        if ((rc = dalloc(h, &d.occ, (size_t)h.occ_words, 0))) return rc;
+        d.occ1_gw = (d.occ_gw + 7) >> 3;
+        int64_t per1 = 1;
+        for (int ax = 0; ax < c.dim; ax++) per1 *= d.occ1_gw;
+        d.occ1_per_t = per1;
+        h.occ1_words = ((int64_t)T * per1 + 31) / 32;
+        if ((rc = dalloc(h, &d.occ1, (size_t)h.occ1_words, 0))) return rc;
+    }
     // accepted points
     const int64_t total_budget =
         c.attempts + (c.group_mode == UG_GROUP_SUBPATH ? (c.sub_attempts ? c.sub_attempts : c.attempts) : 0);
@@ -241,6 +267,7 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
     // round buffers
     const int Bm = d.B_max, Sm = d.S_max;
     if ((rc = dalloc(h, &d.surv_bits, Bm / 32, 0)) || (rc = dalloc(h, &d.gray_bits, Bm / 32, 0)) ||
+        (rc = dalloc(h, &d.gray_off, Bm, 0)) ||
         (rc = dalloc(h, &d.g0, Bm, 0xff)) || (rc = dalloc(h, &d.surv_off, Sm + 1, 0)) ||
         (rc = dalloc(h, &d.spos, (size_t)Sm * T, 0)) || (rc = dalloc(h, &d.ccount, Sm, 0)) ||
         (rc = dalloc(h, &d.clist, (size_t)Sm * kConflictCap, 0)) ||
@@ -302,7 +329,9 @@ static int launch_round(Batch& B, bool timed) {
         launch_prefilter_mixed(B.dU, B.dCtl, B.dInfo, B.nsm, B.st);
         te(K_MIXED);
         tb(K_CONFIRM);
-        k_confirm64<<<g_pre, kTile, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+        k_gray_compact<<<B.n, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+        k_confirm64w<<<B.nsm * 4, 32 * kSurvWarps, kSurvWarps * kConfSmemPerWarp, B.st>>>(B.dU, B.dCtl,
+                                                                                           B.dInfo);
         te(K_CONFIRM);
     } else {
         tb(K_PRE);
@@ -499,7 +528,10 @@ int ug_batch_create(const ug_universe_cfg* cfgs, int32_t n, const ug_run_opts* o
                              (int)(kSurvWarps * kSurvSmemPerWarp)) != cudaSuccess)
         return bail(fail(UG_ECUDA, "smem attribute failed"));
     if (B->any_mixed && (rc = mixed_init_kernels())) return bail(rc);
-    B->kernels_per_round = B->any_mixed ? 8 : 7;
+    B->kernels_per_round = B->any_mixed ? 9 : 7;
+    if (B->any_mixed && cudaFuncSetAttribute(k_confirm64w, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)(kSurvWarps * kConfSmemPerWarp)) != cudaSuccess)
+        return bail(fail(UG_ECUDA, "smem attribute failed"));
     for (int k = 0; k < 2 * K_NK; k++) cudaEventCreate(&B->ev[k]);
     *out = B;
     return UG_OK;
@@ -554,6 +586,8 @@ int ug_batch_reset(void* h, const uint64_t* seeds) {
             CKR(cudaMemsetAsync(u.d.hkeys, 0xff, (size_t)u.hcap * sizeof(uint64_t), B->st));
             CKR(cudaMemsetAsync(u.d.heads, 0xff, (size_t)u.hcap * sizeof(int32_t), B->st));
         }
+        CKR(cudaMemsetAsync(u.d.occ, 0, (size_t)u.occ_words * sizeof(uint32_t), B->st));
+        CKR(cudaMemsetAsync(u.d.occ1, 0, (size_t)u.occ1_words * sizeof(uint32_t), B->st));
         const int32_t ep = B->hCtl[i].epoch;
         init_ctl(u.cfg, u.d, B->hCtl[i]);
         B->hCtl[i].epoch = ep;  // round-hash entries of earlier epochs stay stale

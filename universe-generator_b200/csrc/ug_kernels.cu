@@ -177,10 +177,6 @@ __global__ void __launch_bounds__(kTile) k_prefilter64(const UniDev* __restrict_
     prefilter64_tiles<false>(U, ctl, info);
 }
 
-__global__ void __launch_bounds__(kTile) k_confirm64(const UniDev* __restrict__ U, UniCtl* ctl,
-                                                     RoundInfo* info) {
-    prefilter64_tiles<true>(U, ctl, info);
-}
 
 // --------------------------------------------------------------- compact
 
@@ -286,6 +282,59 @@ __device__ __forceinline__ int32_t rhash_head(const UniDev& d, uint64_t key) {
     return -1;
 }
 
+// Warp-cooperative FP64 regeneration of candidate idx into shared memory:
+// Philox blocks are spread over the lanes, the normalisation sum runs in
+// ascending b on lane 0 -- the same operations, in the same order, as the
+// thread-per-candidate gen_philox64, so the coefficients are identical.
+__device__ __forceinline__ void warp_gen64(const UniDev& d, uint64_t idx, double* alpha, double* beta,
+                                       double* a2, int32_t* bj, double* wj, int lane) {
+    const int F = d.F, F1 = F + 1;
+    if (d.rng == RNG_KNOT) {
+        if (lane == 0) gen_knot64(d, idx, alpha, beta, a2, bj, wj, 1);
+        __syncwarp();
+    } else {
+        for (int ax = 0; ax < d.dim; ax++) {
+            double* al = alpha + ax * F1;
+            double* bt = beta + ax * F1;
+            for (int p = lane; 2 * p <= F; p += 32) {
+                const uint4 o = philox_block(d.seed, idx, ax, p);
+                if (p == 0) {
+                    a2[ax] = d.pin ? 0.0 : (double)o.x * (1.0 / 2147483648.0) - 1.0;
+                    continue;
+                }
+                const int be = 2 * p, bo = 2 * p + 1;
+                const double Ee = -log(((double)o.x + 0.5) * (1.0 / 4294967296.0));
+                al[be] = (o.z & 1u) ? -Ee : Ee;
+                bt[be] = (double)(o.z >> 1) * (1.0 / 2147483648.0) * kPi;
+                if (bo <= F) {
+                    const double Eo = -log(((double)o.y + 0.5) * (1.0 / 4294967296.0));
+                    al[bo] = (o.w & 1u) ? -Eo : Eo;
+                }
+            }
+            __syncwarp();
+            double sum = 0.0;
+            if (lane == 0)
+                for (int b = 2; b <= F; b++) sum += fabs(al[b]);
+            sum = __shfl_sync(0xffffffffu, sum, 0);
+            for (int b = 2 + lane; b <= F; b += 32) {
+                const double e = al[b];
+                double amp = fabs(e) / sum / (double)b;
+                if (e < 0.0) amp = -amp;
+                if (b & 1) {
+                    al[b] = amp;
+                    bt[b] = 0.0;
+                } else {
+                    double sf, cf;
+                    sincos(bt[b], &sf, &cf);
+                    al[b] = amp * cf;
+                    bt[b] = amp * sf;
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
 // One warp per survivor: FP64 regeneration (warp-parallel Philox blocks,
 // sequential normalisation sum in ascending b -- the same operations as the
 // thread-per-candidate prefilter, so identical values), trajectories at all
@@ -308,51 +357,8 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_surv_eval(const UniDev* __r
         const UniDev& d = U[u];
         const UniCtl& c = ctl[u];
         const uint64_t idx = (uint64_t)(c.round_base + d.surv_off[r]);
-        const int F = d.F, F1 = F + 1, T = d.T;
-        if (d.rng == RNG_KNOT) {
-            if (lane == 0) gen_knot64(d, idx, alpha, beta, a2, bj, wj, 1);
-            __syncwarp();
-        } else {
-            for (int ax = 0; ax < d.dim; ax++) {
-                double* al = alpha + ax * F1;
-                double* bt = beta + ax * F1;
-                for (int p = lane; 2 * p <= F; p += 32) {
-                    const uint4 o = philox_block(d.seed, idx, ax, p);
-                    if (p == 0) {
-                        a2[ax] = d.pin ? 0.0 : (double)o.x * (1.0 / 2147483648.0) - 1.0;
-                        continue;
-                    }
-                    const int be = 2 * p, bo = 2 * p + 1;
-                    const double Ee = -log(((double)o.x + 0.5) * (1.0 / 4294967296.0));
-                    al[be] = (o.z & 1u) ? -Ee : Ee;
-                    bt[be] = (double)(o.z >> 1) * (1.0 / 2147483648.0) * kPi;
-                    if (bo <= F) {
-                        const double Eo = -log(((double)o.y + 0.5) * (1.0 / 4294967296.0));
-                        al[bo] = (o.w & 1u) ? -Eo : Eo;
-                    }
-                }
-                __syncwarp();
-                double sum = 0.0;
-                if (lane == 0)
-                    for (int b = 2; b <= F; b++) sum += fabs(al[b]);
-                sum = __shfl_sync(0xffffffffu, sum, 0);
-                for (int b = 2 + lane; b <= F; b += 32) {
-                    const double e = al[b];
-                    double amp = fabs(e) / sum / (double)b;
-                    if (e < 0.0) amp = -amp;
-                    if (b & 1) {
-                        al[b] = amp;
-                        bt[b] = 0.0;
-                    } else {
-                        double sf, cf;
-                        sincos(bt[b], &sf, &cf);
-                        al[b] = amp * cf;
-                        bt[b] = amp * sf;
-                    }
-                }
-                __syncwarp();
-            }
-        }
+        const int F1 = d.F + 1, T = d.T;
+        warp_gen64(d, idx, alpha, beta, a2, bj, wj, lane);
         const int64_t cpt = cells_per_t(d);
         (void)cpt;
         for (int t = lane; t < T; t += 32) {
@@ -374,6 +380,153 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_surv_eval(const UniDev* __r
             q.next = nxt;
             q.gid = -1;
             d.spos[(int64_t)r * T + t] = q;
+        }
+        __syncwarp();
+    }
+}
+
+// Candidates the mixed prefilter could not decide (guard band, or universes
+// outside the tensor-core path), in index order, per universe.
+__global__ void __launch_bounds__(256) k_gray_compact(const UniDev* __restrict__ U, UniCtl* ctl,
+                                                      RoundInfo* info) {
+    __shared__ int32_t wsum[8];
+    __shared__ int32_t s_running;
+    __shared__ bool s_last;
+    const int u = blockIdx.x;
+    const UniDev& d = U[u];
+    UniCtl& c = ctl[u];
+    const int B = c.B;
+    const int nwords = (B + 31) >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_running = 0;
+    __syncthreads();
+    for (int base = 0; base < nwords; base += 256) {
+        const int w = base + tid;
+        uint32_t bits = w < nwords ? d.gray_bits[w] : 0u;
+        if (w == nwords - 1 && (B & 31)) bits &= (1u << (B & 31)) - 1u;
+        const int cnt = __popc(bits);
+        int incl = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        int wpre = 0, tot = 0;
+        for (int k = 0; k < 8; k++) {
+            if (k < warp) wpre += wsum[k];
+            tot += wsum[k];
+        }
+        int rank = s_running + wpre + incl - cnt;
+        while (bits) {
+            const int bit = __ffs(bits) - 1;
+            bits &= bits - 1;
+            d.gray_off[rank++] = w * 32 + bit;
+        }
+        __syncthreads();
+        if (tid == 0) s_running += tot;
+        __syncthreads();
+    }
+    if (tid == 0) {
+        c.n_gray = s_running;
+        __threadfence();
+        s_last = atomicAdd(&info->gray_done, 1) == info->n_uni - 1;
+    }
+    __syncthreads();
+    if (s_last && tid == 0) {
+        __threadfence();
+        int acc = 0;
+        for (int v = 0; v < info->n_uni; v++) {
+            info->gray_pref[v] = acc;
+            acc += *(volatile int32_t*)&ctl[v].n_gray;
+        }
+        info->gray_pref[info->n_uni] = acc;
+        info->total_gray = acc;
+        info->gray_done = 0;
+    }
+}
+
+// One warp per undecided candidate: FP64 regeneration and the exact test
+// against the committed packing, timesteps spread over the lanes (the FP64
+// guard-band retest of the mixed path).
+__global__ void __launch_bounds__(32 * kSurvWarps) k_confirm64w(const UniDev* __restrict__ U,
+                                                                  UniCtl* ctl, RoundInfo* info) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    unsigned char* my = smem_raw + (size_t)wib * kConfSmemPerWarp;
+    double* alpha = (double*)my;
+    double* beta = alpha + 3 * (kMaxF + 1);
+    double* a2 = beta + 3 * (kMaxF + 1);
+    double* wj = a2 + 3;
+    int32_t* bj = (int32_t*)(wj + kMaxF);
+    double* P1 = (double*)(my + kSurvSmemPerWarpBase);
+    const int n_uni = info->n_uni, total = info->total_gray;
+    const int gwarp = blockIdx.x * kSurvWarps + wib, nwarps = gridDim.x * kSurvWarps;
+    for (int item = gwarp; item < total; item += nwarps) {
+        const int u = find_uni(info->gray_pref, n_uni, item);
+        const UniDev& d = U[u];
+        UniCtl& c = ctl[u];
+        const int off = d.gray_off[item - info->gray_pref[u]];
+        const uint64_t idx = (uint64_t)(c.round_base + off);
+        const int F1 = d.F + 1, T = d.T;
+        warp_gen64(d, idx, alpha, beta, a2, bj, wj, lane);
+        const bool group = group_phase(d, c);
+        int32_t g = -1;
+        bool hitl = false;
+        int nev = 0;
+        if (d.dim == 1 && d.cross1d) {
+            for (int t = lane; t < T; t += 32) P1[t] = eval64(d, alpha, beta, 1, a2[0], t);
+            __syncwarp();
+            nev = lane == 0 ? T : 0;
+            for (int64_t s = lane; s < c.n_slots && !(hitl && !group); s += 32) {
+                const Pt64* q = d.pts + s * T;
+                double d0 = torus_delta(P1[0] - __ldcg(&q[0].c[0]));
+                bool hit = hit1(d0, d.cell, d.inclusive);
+                for (int t = 1; t < T && !hit; t++) {
+                    const double d1 = torus_delta(P1[t] - __ldcg(&q[t].c[0]));
+                    hit = hit1(d1, d.cell, d.inclusive) || crosses_step(d0, d1);
+                    d0 = d1;
+                }
+                if (hit) {
+                    if (!group) {
+                        hitl = true;
+                    } else {
+                        const int32_t gq = __ldcg(&q[0].gid);
+                        if (g == -1)
+                            g = gq;
+                        else if (g != gq)
+                            hitl = true;
+                    }
+                }
+            }
+        } else {
+            const int64_t cpt = cells_per_t(d);
+            for (int oi0 = 0; oi0 < T; oi0 += 32) {
+                const int oi = oi0 + lane;
+                if (oi < T && !hitl) {
+                    const int t = __ldg(d.order + oi);
+                    double P[3];
+                    for (int ax = 0; ax < d.dim; ax++)
+                        P[ax] = eval64(d, alpha + ax * F1, beta + ax * F1, 1, a2[ax], t);
+                    nev++;
+                    hitl = contacts64(d, t, P, group, &g, cpt);
+                }
+                if (__any_sync(0xffffffffu, hitl)) break;
+            }
+        }
+        // merge the lanes: any rejection, or (group) two distinct groups
+        bool rej = __any_sync(0xffffffffu, hitl);
+        int32_t first = -1;
+        for (int o = 0; o < 32; o++) {
+            const int32_t v = __shfl_sync(0xffffffffu, g, o);
+            if (first == -1) first = v;
+        }
+        if (group) rej = rej || __any_sync(0xffffffffu, g != -1 && g != first);
+        for (int o = 16; o > 0; o >>= 1) nev += __shfl_xor_sync(0xffffffffu, nev, o);
+        if (lane == 0) {
+            if (!rej) atomicOr(&d.surv_bits[off >> 5], 1u << (off & 31));
+            if (d.group_mode != GROUP_NONE) d.g0[off] = first;
+            if (nev) atomicAdd((unsigned long long*)&c.evals_fp64, (unsigned long long)nev);
         }
         __syncwarp();
     }
@@ -665,6 +818,12 @@ __global__ void __launch_bounds__(256) k_commit(const UniDev* __restrict__ U, Un
         for (int ax = 0; ax < d.dim; ax++) cc[ax] = cell_of(q.c[ax], d.cell, d.gw);
         int32_t old;
         grid_insert(d, c, t, lin_cell(cc, d.dim, d.gw), cells_per_t(d), (int32_t)slot, &old);
+        {
+            const int64_t b = occ_bit(d, t, cc);
+            atomicOr(d.occ + (b >> 5), 1u << (b & 31));
+            const int64_t b1 = occ1_bit(d, t, cc);
+            atomicOr(d.occ1 + (b1 >> 5), 1u << (b1 & 31));
+        }
         q.next = old;
         q.gid = d.sgid[r];
         d.pts[slot * d.T + t] = q;

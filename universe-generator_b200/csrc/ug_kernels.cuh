@@ -16,8 +16,11 @@ struct RoundInfo {
     int32_t any_active;
     int32_t mixed_ok;      // universes in the mixed prefilter this round
     int32_t pad[2];
+    int32_t total_gray;
+    int32_t gray_done;
     int32_t tile_off[kMaxUni + 1];
     int32_t surv_off[kMaxUni + 1];
+    int32_t gray_pref[kMaxUni + 1];
 };
 
 __device__ __forceinline__ int find_uni(const int32_t* off, int n, int item) {
@@ -35,7 +38,8 @@ __device__ __forceinline__ int find_uni(const int32_t* off, int n, int item) {
 // Kernels (ug_kernels.cu)
 __global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_prefilter64(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
-__global__ void k_confirm64(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
+__global__ void k_gray_compact(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
+__global__ void k_confirm64w(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_compact(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_surv_eval(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_conflicts(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
@@ -45,7 +49,10 @@ __global__ void k_rehash(const UniDev* __restrict__ U, UniCtl* ctl, int u, int64
 
 // Shared memory of k_surv_eval per warp (bytes), for F <= kMaxF.
 constexpr int kSurvWarps = 4;
-constexpr size_t kSurvSmemPerWarp = (size_t)3 * (kMaxF + 1) * 2 * sizeof(double) + 3 * sizeof(double) +
+constexpr size_t kSurvSmemPerWarpBase = (size_t)3 * (kMaxF + 1) * 2 * sizeof(double) + 3 * sizeof(double) +
                                     (size_t)kMaxF * (sizeof(int32_t) + sizeof(double));
+constexpr size_t kSurvSmemPerWarp = kSurvSmemPerWarpBase;
+// k_confirm64w adds the FP64 trajectory of a 1+1D candidate
+constexpr size_t kConfSmemPerWarp = kSurvSmemPerWarpBase + (size_t)kMaxF * sizeof(double);
 
 }  // namespace ug

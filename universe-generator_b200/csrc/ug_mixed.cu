@@ -150,18 +150,19 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
     return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-// Coefficients of one K chunk (16 frequency pairs) of candidate idx, axis ax,
-// written as BF16 hi/lo rows of the canonical A images.  Returns the chunk's
-// contribution to sum_b E_b (FP64 accumulation of the FP32 variates).
-__device__ __forceinline__ double gen_chunk(const UniDev& d, uint64_t idx, int ax, int ch, bool valid,
-                                            uint8_t* a_hi, uint8_t* a_lo, int row) {
+// Coefficients of a quarter of one K chunk (pairs 4*part .. 4*part+3 of the
+// chunk's 16) of candidate idx, axis ax, written as BF16 hi/lo into the rows
+// of the canonical A images (12 entries = three 8-byte pieces per image).
+// Returns the quarter's contribution to sum_b E_b.
+__device__ __forceinline__ double gen_quarter(const UniDev& d, uint64_t idx, int ax, int ch, int part,
+                                              bool valid, uint8_t* a_hi, uint8_t* a_lo, int row) {
     const int F = d.F;
     const int P = F >> 1;
-    float v[kKC];
+    float v[12];
     double sum = 0.0;
 #pragma unroll
-    for (int q = 0; q < kPairsPerChunk; q++) {
-        const int p = ch * kPairsPerChunk + q + 1;
+    for (int q = 0; q < 4; q++) {
+        const int p = ch * kPairsPerChunk + part * 4 + q + 1;
         float ae = 0.f, be = 0.f, ao = 0.f;
         if (valid && p <= P) {
             const uint4 o = philox_block(d.seed, idx, ax, p);
@@ -186,18 +187,19 @@ __device__ __forceinline__ double gen_chunk(const UniDev& d, uint64_t idx, int a
         v[3 * q + 2] = ao;
     }
 #pragma unroll
-    for (int g = 0; g < kKC / 8; g++) {
-        uint32_t h[4], l[4];
+    for (int g = 0; g < 3; g++) {
+        uint32_t h[2], l[2];
 #pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const float x0 = v[8 * g + 2 * e], x1 = v[8 * g + 2 * e + 1];
+        for (int e = 0; e < 2; e++) {
+            const float x0 = v[4 * g + 2 * e], x1 = v[4 * g + 2 * e + 1];
             const __nv_bfloat16 h0 = __float2bfloat16_rn(x0), h1 = __float2bfloat16_rn(x1);
             h[e] = pack_bf16x2(__bfloat162float(h0), __bfloat162float(h1));
             l[e] = pack_bf16x2(x0 - __bfloat162float(h0), x1 - __bfloat162float(h1));
         }
-        const int off = g * (kTile * 16) + row * 16;
-        *reinterpret_cast<uint4*>(a_hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<uint4*>(a_lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
+        const int ent = part * 12 + 4 * g;  // first of 4 entries, never straddles an 8-entry core row
+        const int off = (ent >> 3) * (kTile * 16) + row * 16 + (ent & 7) * 2;
+        *reinterpret_cast<uint2*>(a_hi + off) = make_uint2(h[0], h[1]);
+        *reinterpret_cast<uint2*>(a_lo + off) = make_uint2(l[0], l[1]);
     }
     return sum;
 }
@@ -233,6 +235,7 @@ __device__ __forceinline__ int test32_at(const UniDev& d, int t, const float* X,
             v %= d.gw;
             cc[ax] = v < 0 ? v + d.gw : v;
         }
+        if (!occ_test(d, t, cc)) continue;
         int32_t p = grid_head(d, t, lin_cell(cc, d.dim, d.gw), cpt);
         while (p >= 0) {
             const Pt32 q = d.ptf[(int64_t)p * d.T + t];
@@ -263,24 +266,31 @@ struct MixedLaunch {
     int64_t first, count;
 };
 
-__global__ void __launch_bounds__(kTile, 1) k_prefilter_mixed(const UniDev* __restrict__ U, UniCtl* ctl,
-                                                               RoundInfo* info, MixedLaunch L) {
+constexpr int kMxThreads = 512;  // 4 threads per candidate row
+constexpr int kMxParts = kMxThreads / kTile;
+
+__global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev* __restrict__ U, UniCtl* ctl,
+                                                                    RoundInfo* info, MixedLaunch L) {
     extern __shared__ __align__(1024) uint8_t sm[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    // carve: two stages of {A_hi, A_lo, B (hi then lo)}; barriers at the end
+    // thread (row, part): warps w and w+4k share the tensor-memory lane quarter w%4
+    const int row = (warp & 3) * 32 + lane;
+    const int part = warp >> 2;
+    // carve: two stages of {A_hi, A_lo, B (hi then lo)}; per-row state; barriers
     const int stage_bytes = 2 * kAImgBytes + L.tpad_max * kKC * 2 * 2;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + 2 * stage_bytes);
+    double* s_sum = reinterpret_cast<double*>(sm + 2 * stage_bytes);      // [kTile][kMxParts]
+    int* s_rej = reinterpret_cast<int*>(s_sum + kTile * kMxParts);       // [kTile]
+    int* s_gray = s_rej + kTile;                                          // [kTile]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(s_gray + kTile);
     uint64_t* bar_b = bar;       // [2] B chunk landed
     uint64_t* bar_m = bar + 2;   // [2] MMAs reading the stage finished
     uint64_t* bar_d = bar + 4;   // all MMAs of the pass finished
     uint32_t* holder = reinterpret_cast<uint32_t*>(bar + 5);
-    int* s_flag = reinterpret_cast<int*>(bar + 6);
 
     if (warp == 0) tmem_alloc(holder, L.ncols);
     if (tid == 0) {
         for (int i = 0; i < 5; i++) mbar_init(&bar[i], 1);
         fence_mbar_init();
-        *s_flag = 0;
     }
     tc_fence_before();
     __syncthreads();
@@ -293,12 +303,14 @@ __global__ void __launch_bounds__(kTile, 1) k_prefilter_mixed(const UniDev* __re
     const bool dump = L.dump != nullptr;
     const int n_uni = dump ? 1 : info->n_uni;
     const int total = dump ? (int)((L.count + kTile - 1) / kTile) : info->total_tiles;
+    volatile int* vrej = s_rej;
+    volatile int* vgray = s_gray;
 
     for (int tile = blockIdx.x; tile < total && !timeout; tile += gridDim.x) {
         const int u = dump ? L.u : find_uni(info->tile_off, n_uni, tile);
         const UniDev& d = U[u];
         const int lt = dump ? tile : tile - info->tile_off[u];
-        const int off = lt * kTile + tid;
+        const int off = lt * kTile + row;
         int64_t base;
         int B;
         if (dump) {
@@ -311,10 +323,12 @@ __global__ void __launch_bounds__(kTile, 1) k_prefilter_mixed(const UniDev* __re
         const bool valid = off < B;
         const uint64_t idx = (uint64_t)(base + off);
         if (!d.mx_ok) {  // not eligible for the tensor-core path: everything to the FP64 test
-            const uint32_t g = __ballot_sync(0xffffffffu, valid);
-            if (lane == 0 && !dump) {
-                d.surv_bits[off >> 5] = 0u;
-                d.gray_bits[off >> 5] = g;
+            if (part == 0) {
+                const uint32_t g = __ballot_sync(0xffffffffu, valid);
+                if (lane == 0 && !dump) {
+                    d.surv_bits[off >> 5] = 0u;
+                    d.gray_bits[off >> 5] = g;
+                }
             }
             continue;
         }
@@ -324,11 +338,13 @@ __global__ void __launch_bounds__(kTile, 1) k_prefilter_mixed(const UniDev* __re
         const float r = (float)d.cell, mrg = d.mx_margin, inv_cell = (float)(1.0 / d.cell);
         const int64_t cpt = cells_per_t(d);
         float inv_sum[3] = {0.f, 0.f, 0.f}, a2f[3] = {0.f, 0.f, 0.f};
-        int state = 0;  // 0 clear so far, 1 rejected (certain contact)
-        bool gray = false;
+        if (part == 0) {
+            s_rej[row] = valid ? 0 : 1;
+            s_gray[row] = 0;
+        }
         int nev = 0;
         for (int pass = 0; pass < d.mx_npass && !timeout; pass++) {
-            if (pass > 0 && __syncthreads_and(state == 1 || !valid)) break;
+            if (pass > 0 && __syncthreads_and(vrej[row] != 0)) break;
             for (int ax = 0; ax < dim && !timeout; ax++) {
                 double sumE = 0.0;
                 if (pass == 0 && valid) {
@@ -353,7 +369,7 @@ __global__ void __launch_bounds__(kTile, 1) k_prefilter_mixed(const UniDev* __re
                         mbar_expect_tx(&bar_b[st], bchunk);
                         bulk_g2s(b_img, d.mx_bimg + (size_t)ch * bchunk, bchunk, &bar_b[st]);
                     }
-                    sumE += gen_chunk(d, idx, ax, ch, valid, a_hi, a_lo, tid);
+                    sumE += gen_quarter(d, idx, ax, ch, part, valid, a_hi, a_lo, row);
                     fence_proxy_async();
                     __syncthreads();
                     if (tid == 0) {
@@ -379,7 +395,15 @@ __global__ void __launch_bounds__(kTile, 1) k_prefilter_mixed(const UniDev* __re
                     }
                     ph_b[st] ^= 1;
                 }
-                if (pass == 0) inv_sum[ax] = valid ? (float)(1.0 / sumE) : 0.f;
+                if (timeout) break;
+                if (pass == 0) {  // combine the four partial sums of the row in a fixed order
+                    s_sum[row * kMxParts + part] = sumE;
+                    __syncthreads();
+                    const double tot = s_sum[row * kMxParts + 0] + s_sum[row * kMxParts + 1] +
+                                       s_sum[row * kMxParts + 2] + s_sum[row * kMxParts + 3];
+                    inv_sum[ax] = valid ? (float)(1.0 / tot) : 0.f;
+                    __syncthreads();
+                }
             }
             if (timeout) break;
             if (tid == 0) umma_commit(bar_d);
@@ -390,12 +414,12 @@ __global__ void __launch_bounds__(kTile, 1) k_prefilter_mixed(const UniDev* __re
                 break;
             }
             tc_fence_after();
-            // epilogue: columns of this pass in endpoint-first order
-            const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-            for (int c0 = 0; c0 < nm; c0 += 8) {
+            // epilogue: 8-column blocks part, part+4, ... of this pass (endpoint-first order)
+            const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+            for (int c0 = part * 8; c0 < nm; c0 += 8 * kMxParts) {
                 const int col0 = pass * nm + c0;
                 if (col0 >= T) break;
-                if (!dump && __all_sync(0xffffffffu, state == 1 || !valid)) break;
+                if (!dump && __all_sync(0xffffffffu, vrej[row] != 0)) break;
                 float x[3][8];
                 for (int ax = 0; ax < dim; ax++) tmem_ld8(lane_base + (uint32_t)(ax * nm + c0), x[ax]);
                 tmem_wait_ld();
@@ -411,32 +435,33 @@ __global__ void __launch_bounds__(kTile, 1) k_prefilter_mixed(const UniDev* __re
                                 L.dump[((size_t)off * T + t) * dim + ax] = X[ax];
                         continue;
                     }
-                    if (!valid || state == 1) continue;
+                    if (vrej[row]) break;
                     nev++;
-                    if (test32_at(d, t, X, r, mrg, inv_cell, cpt, &gray)) state = 1;
+                    bool gr = false;
+                    if (test32_at(d, t, X, r, mrg, inv_cell, cpt, &gr)) vrej[row] = 1;
+                    if (gr) vgray[row] = 1;
                 }
             }
             tc_fence_before();
             __syncthreads();
         }
         if (!dump) {
-            const bool surv = valid && state == 0 && !gray && !timeout;
-            const bool gr = valid && state == 0 && (gray || timeout);
-            const uint32_t sb = __ballot_sync(0xffffffffu, surv);
-            const uint32_t gb = __ballot_sync(0xffffffffu, gr);
-            if (lane == 0) {
-                d.surv_bits[off >> 5] = sb;
-                d.gray_bits[off >> 5] = gb;
-            }
-            int ng = __popc(gb);
             for (int o = 16; o > 0; o >>= 1) nev += __shfl_xor_sync(0xffffffffu, nev, o);
-            if (lane == 0) {
-                if (nev) atomicAdd((unsigned long long*)&ctl[u].evals, (unsigned long long)nev);
-                if (ng) {
-                    atomicAdd(&ctl[u].n_gray, ng);
-                    atomicAdd((unsigned long long*)&ctl[u].gray_total, (unsigned long long)ng);
+            if (lane == 0 && nev) atomicAdd((unsigned long long*)&ctl[u].evals, (unsigned long long)nev);
+            if (part == 0) {
+                const bool rej = vrej[row] != 0, gry = vgray[row] != 0;
+                const bool surv = valid && !rej && !gry && !timeout;
+                const bool gr = valid && !rej && (gry || timeout);
+                const uint32_t sb = __ballot_sync(0xffffffffu, surv);
+                const uint32_t gb = __ballot_sync(0xffffffffu, gr);
+                if (lane == 0) {
+                    d.surv_bits[off >> 5] = sb;
+                    d.gray_bits[off >> 5] = gb;
+                    const int ng = __popc(gb);
+                    if (ng) atomicAdd((unsigned long long*)&ctl[u].gray_total, (unsigned long long)ng);
                 }
             }
+            __syncthreads();
         }
     }
     if (timeout && tid == 0 && !dump) {
@@ -480,7 +505,10 @@ static int g_tpad_max = 16;
 static size_t g_smem = 0;
 static int g_ctas_per_sm = 1;
 
-static size_t smem_bytes() { return (size_t)2 * (2 * kAImgBytes + g_tpad_max * kKC * 2 * 2) + 64; }
+static size_t smem_bytes() {
+    return (size_t)2 * (2 * kAImgBytes + g_tpad_max * kKC * 2 * 2) + (size_t)kTile * kMxParts * 8 +
+           2 * kTile * 4 + 64;
+}
 
 static uint16_t bf16_bits(float x) {
     const __nv_bfloat16 h = __float2bfloat16_rn(x);
@@ -607,7 +635,7 @@ int mixed_init_kernels() {
 
 void launch_prefilter_mixed(const UniDev* dU, UniCtl* dCtl, RoundInfo* dInfo, int nsm, cudaStream_t st) {
     MixedLaunch L{(uint32_t)g_ncols, g_tpad_max, nullptr, 0, 0, 0};
-    k_prefilter_mixed<<<nsm * g_ctas_per_sm, kTile, g_smem, st>>>(dU, dCtl, dInfo, L);
+    k_prefilter_mixed<<<nsm * g_ctas_per_sm, kMxThreads, g_smem, st>>>(dU, dCtl, dInfo, L);
 }
 
 int mixed_error(const UniDev* dU, int u, const UniDev& d, const MixedTables& mt, int64_t first, int64_t count,
@@ -621,7 +649,7 @@ int mixed_error(const UniDev* dU, int u, const UniDev& d, const MixedTables& mt,
     MixedLaunch L{(uint32_t)g_ncols, g_tpad_max, d32, u, first, count};
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
-    k_prefilter_mixed<<<nsm * g_ctas_per_sm, kTile, g_smem, st>>>(dU, nullptr, nullptr, L);
+    k_prefilter_mixed<<<nsm * g_ctas_per_sm, kMxThreads, g_smem, st>>>(dU, nullptr, nullptr, L);
     k_pos64<<<(int)std::min<int64_t>((count + 127) / 128, 2048), 128, 0, st>>>(dU, u, first, count, d64);
     std::vector<float> h32(n);
     std::vector<double> h64(n);
