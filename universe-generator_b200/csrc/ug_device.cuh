@@ -341,17 +341,27 @@ __device__ inline void gen_knot64(const UniDev& U, uint64_t idx, double* alpha, 
     }
 }
 
-// FP64 position of one axis at timestep t from canonical coefficients.
+// FP64 position of one axis at timestep t from canonical coefficients: the
+// contraction in ascending b (alpha_b S_bt, beta_b Cm_bt, alpha_b+1 S_b+1,t, ...),
+// one fused multiply-add per term.  Table loads are issued four pairs ahead.
 __device__ __forceinline__ double eval64(const UniDev& U, const double* alpha, const double* beta,
                                          int stride, double a2, int t) {
     const int T = U.T, F = U.F;
     const double* S = U.S + t;
     const double* Cm = U.Cm + t;
     double acc = 0.0;
-    for (int b = 2; b <= F; b += 2) {
+    int b = 2;
+#pragma unroll 4
+    for (; b + 1 <= F; b += 2) {
+        const double s0 = __ldg(S + (size_t)b * T), c0 = __ldg(Cm + (size_t)b * T);
+        const double s1 = __ldg(S + (size_t)(b + 1) * T);
+        acc = fma(alpha[b * stride], s0, acc);
+        acc = fma(beta[b * stride], c0, acc);
+        acc = fma(alpha[(b + 1) * stride], s1, acc);
+    }
+    if (b <= F) {  // even F: the last frequency has no odd partner
         acc = fma(alpha[b * stride], __ldg(S + (size_t)b * T), acc);
         acc = fma(beta[b * stride], __ldg(Cm + (size_t)b * T), acc);
-        if (b + 1 <= F) acc = fma(alpha[(b + 1) * stride], __ldg(S + (size_t)(b + 1) * T), acc);
     }
     return torus_wrap(fma(acc, __ldg(U.invsinz + t), a2));
 }
@@ -434,48 +444,94 @@ __device__ __forceinline__ bool occ1_any(const UniDev& U, int t, const int* lo, 
     return false;
 }
 
+// Occupancy of the cells (lo + i) mod gw, i = 0..n-1 (n <= 8), along the last
+// axis of the row whose leading coordinates are `pre` (row-major prefix of
+// the coarse bitmap index).  Bit i of the result set when cell lo + i may
+// hold a point.  One or two 32-bit words per contiguous segment.
+__device__ __forceinline__ uint32_t occ_row(const UniDev& U, int t, int64_t pre, int lo, int n) {
+    const int gw = U.gw, sh = U.occ_shift;
+    const int64_t rowbase = (int64_t)t * U.occ_per_t + pre * U.occ_gw;
+    uint32_t mask = 0;
+    int i = 0;
+    while (i < n) {
+        int c = (lo + i) % gw;
+        c = c < 0 ? c + gw : c;
+        int seg = gw - c;                 // cells until the seam
+        if (seg > n - i) seg = n - i;
+        const int b0 = c >> sh, b1 = (c + seg - 1) >> sh;
+        const int64_t bit0 = rowbase + b0;
+        const int64_t w0 = bit0 >> 5;
+        const int64_t w1 = (rowbase + b1) >> 5;
+        uint64_t bits = __ldcg(U.occ + w0);
+        if (w1 != w0) bits |= (uint64_t)__ldcg(U.occ + w1) << 32;
+        bits >>= (bit0 & 31);
+        for (int k = 0; k < seg; k++)
+            if ((bits >> (((c + k) >> sh) - b0)) & 1u) mask |= 1u << (i + k);
+        i += seg;
+    }
+    return mask;
+}
+
 // Contacts of the point P (dim coords) at timestep t with the accepted
 // packing.  Unique mode: returns true on the first contact.  Group mode:
 // accumulates the single touched group in *g and returns true when a second
 // distinct group appears.
 __device__ __forceinline__ bool contacts64(const UniDev& U, int t, const double* P, bool group,
                                            int32_t* g, int64_t cpt) {
-    int c[3];
-    for (int ax = 0; ax < U.dim; ax++) c[ax] = cell_of(P[ax], U.cell, U.gw);
-    {
-        int lo[3], hi[3];
-        for (int ax = 0; ax < U.dim; ax++) {
-            lo[ax] = c[ax] - 1;
-            hi[ax] = c[ax] + 1;
-        }
-        if (!occ1_any(U, t, lo, hi)) return false;
+    int c[3], lo[3], hi[3];
+    for (int ax = 0; ax < U.dim; ax++) {
+        c[ax] = cell_of(P[ax], U.cell, U.gw);
+        lo[ax] = c[ax] - 1;
+        hi[ax] = c[ax] + 1;
     }
-    int nb = U.dim == 1 ? 3 : (U.dim == 2 ? 9 : 27);
-    for (int k = 0; k < nb; k++) {
-        int cc[3], r = k;
-        for (int ax = U.dim - 1; ax >= 0; ax--) {
-            const int dd = r % 3 - 1;
-            r /= 3;
-            int v = c[ax] + dd;
-            v = v < 0 ? v + U.gw : (v >= U.gw ? v - U.gw : v);
-            cc[ax] = v;
-        }
-        if (!occ_test(U, t, cc)) continue;
-        int32_t p = grid_head(U, t, lin_cell(cc, U.dim, U.gw), cpt);
-        while (p >= 0) {
-            const Pt64* q = U.pts + (int64_t)p * U.T + t;
-            bool hit = true;
-            for (int ax = 0; ax < U.dim && hit; ax++)
-                hit = hit1(torus_delta(P[ax] - __ldcg(&q->c[ax])), U.cell, U.inclusive);
-            if (hit) {
-                if (!group) return true;
-                const int32_t gq = __ldcg(&q->gid);
-                if (*g == -1)
-                    *g = gq;
-                else if (*g != gq)
-                    return true;
+    if (!occ1_any(U, t, lo, hi)) return false;
+    const int D = U.dim, gw = U.gw, last = D - 1;
+    const int nrows = D == 1 ? 1 : (D == 2 ? 3 : 9);
+    uint32_t masks[9];
+#pragma unroll
+    for (int rw = 0; rw < 9; rw++) {
+        if (rw >= nrows) break;
+        int64_t pre = 0;
+        if (D >= 2) {
+            int r0 = D == 3 ? rw / 3 : rw;
+            int v0 = (c[0] + r0 - 1 + gw) % gw;
+            pre = v0 >> U.occ_shift;
+            if (D == 3) {
+                int v1 = (c[1] + rw % 3 - 1 + gw) % gw;
+                pre = pre * U.occ_gw + (v1 >> U.occ_shift);
             }
-            p = __ldcg(&q->next);
+        }
+        masks[rw] = occ_row(U, t, pre, lo[last], 3);
+    }
+    for (int rw = 0; rw < nrows; rw++) {
+        uint32_t m = masks[rw];
+        while (m) {
+            const int i = __ffs(m) - 1;
+            m &= m - 1;
+            int cc[3];
+            if (D == 3) {
+                cc[0] = (c[0] + rw / 3 - 1 + gw) % gw;
+                cc[1] = (c[1] + rw % 3 - 1 + gw) % gw;
+            } else if (D == 2) {
+                cc[0] = (c[0] + rw - 1 + gw) % gw;
+            }
+            cc[last] = (lo[last] + i + gw) % gw;
+            int32_t p = grid_head(U, t, lin_cell(cc, D, gw), cpt);
+            while (p >= 0) {
+                const Pt64* q = U.pts + (int64_t)p * U.T + t;
+                bool hit = true;
+                for (int ax = 0; ax < D && hit; ax++)
+                    hit = hit1(torus_delta(P[ax] - __ldcg(&q->c[ax])), U.cell, U.inclusive);
+                if (hit) {
+                    if (!group) return true;
+                    const int32_t gq = __ldcg(&q->gid);
+                    if (*g == -1)
+                        *g = gq;
+                    else if (*g != gq)
+                        return true;
+                }
+                p = __ldcg(&q->next);
+            }
         }
     }
     return false;

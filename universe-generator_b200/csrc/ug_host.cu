@@ -200,6 +200,7 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
     d.B_max = c.round_size ? c.round_size : 65536;
     const int T = c.T;
     d.S_max = (int)std::min<int64_t>(kSmaxCap, std::max<int64_t>(256, (1 << 18) / T));
+    if (c.dim == 1) d.S_max = 256;  // 1+1D in-round conflicts are found pairwise
     d.S_max = std::min(d.S_max, d.B_max);
     // tables
     std::vector<double> S, Cm, inv;
@@ -287,9 +288,9 @@ static void init_ctl(const ug_universe_cfg& c, const UniDev& d, UniCtl& k) {
     k.max_n = c.max_n;
     k.phase = 1;
     k.state = ST_ACTIVE;
-    k.B_min = std::min(4096, d.B_max);
+    k.B_min = std::min(1024, d.B_max);
     k.B_cap = d.B_max;
-    k.round_B = d.B_max;
+    k.round_B = std::min(4096, d.B_max);  // grows toward B_cap once survivors thin out
     k.accept_rate = c.accept_rate;
     k.sub_accept_rate = c.sub_accept_rate;
     k.win_target = c.accept_rate > 0 ? (int64_t)std::min(5e9, std::max(2e7, 30.0 / c.accept_rate)) : 0;

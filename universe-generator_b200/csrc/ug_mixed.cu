@@ -213,43 +213,74 @@ __device__ __forceinline__ int test32_at(const UniDev& d, int t, const float* X,
                                          float inv_cell, int64_t cpt, bool* gray) {
     int lo[3], hi[3];
     const float band = m * inv_cell + 1e-4f;
-    for (int ax = 0; ax < d.dim; ax++) {
+    const int D = d.dim, gw = d.gw, last = D - 1;
+    for (int ax = 0; ax < D; ax++) {
         const float u = (X[ax] + 1.0f) * inv_cell;
         const float fl = floorf(u);
         const float fr = u - fl;
         int c = (int)fl;
-        c = c >= d.gw ? d.gw - 1 : (c < 0 ? 0 : c);
+        c = c >= gw ? gw - 1 : (c < 0 ? 0 : c);
         lo[ax] = c - 1 - (fr < band ? 1 : 0);
         hi[ax] = c + 1 + (fr > 1.0f - band ? 1 : 0);
     }
+    if (!occ1_any(d, t, lo, hi)) return 0;
     const float rin = r - m, rout = r + m;
-    int cc[3];
-    int cnt[3] = {1, 1, 1};
-    for (int ax = 0; ax < d.dim; ax++) cnt[ax] = hi[ax] - lo[ax] + 1;
-    const int total = cnt[0] * (d.dim > 1 ? cnt[1] : 1) * (d.dim > 2 ? cnt[2] : 1);
-    for (int k = 0; k < total; k++) {
-        int rr = k;
-        for (int ax = d.dim - 1; ax >= 0; ax--) {
-            int v = lo[ax] + rr % cnt[ax];
-            rr /= cnt[ax];
-            v %= d.gw;
-            cc[ax] = v < 0 ? v + d.gw : v;
+    // rows over the leading axes, occupancy words along the last axis
+    const int n0 = D >= 2 ? hi[0] - lo[0] + 1 : 1;
+    const int n1 = D == 3 ? hi[1] - lo[1] + 1 : 1;
+    const int nl = hi[last] - lo[last] + 1;
+    if (n0 * n1 > 16 || nl > 8) {  // cannot happen while the band is below half a cell
+        *gray = true;
+        return 0;
+    }
+    uint32_t masks[16];
+#pragma unroll
+    for (int rw = 0; rw < 16; rw++) {
+        if (rw >= n0 * n1) break;
+        int64_t pre = 0;
+        if (D >= 2) {
+            int v0 = (lo[0] + rw / n1) % gw;
+            v0 = v0 < 0 ? v0 + gw : v0;
+            pre = v0 >> d.occ_shift;
+            if (D == 3) {
+                int v1 = (lo[1] + rw % n1) % gw;
+                v1 = v1 < 0 ? v1 + gw : v1;
+                pre = pre * d.occ_gw + (v1 >> d.occ_shift);
+            }
         }
-        if (!occ_test(d, t, cc)) continue;
-        int32_t p = grid_head(d, t, lin_cell(cc, d.dim, d.gw), cpt);
-        while (p >= 0) {
-            const Pt32 q = d.ptf[(int64_t)p * d.T + t];
-            bool miss = false, deep = true;
-            for (int ax = 0; ax < d.dim; ax++) {
-                const float dd = fabsf(torus_deltaf(X[ax] - q.c[ax]));
-                miss |= dd > rout;
-                deep &= dd < rin;
+        masks[rw] = occ_row(d, t, pre, lo[last], nl);
+    }
+    for (int rw = 0; rw < n0 * n1; rw++) {
+        uint32_t mk = masks[rw];
+        while (mk) {
+            const int i = __ffs(mk) - 1;
+            mk &= mk - 1;
+            int cc[3];
+            if (D >= 2) {
+                int v0 = (lo[0] + rw / n1) % gw;
+                cc[0] = v0 < 0 ? v0 + gw : v0;
+                if (D == 3) {
+                    int v1 = (lo[1] + rw % n1) % gw;
+                    cc[1] = v1 < 0 ? v1 + gw : v1;
+                }
             }
-            if (!miss) {
-                if (deep) return 1;
-                *gray = true;
+            int vl = (lo[last] + i) % gw;
+            cc[last] = vl < 0 ? vl + gw : vl;
+            int32_t p = grid_head(d, t, lin_cell(cc, D, gw), cpt);
+            while (p >= 0) {
+                const Pt32 q = d.ptf[(int64_t)p * d.T + t];
+                bool miss = false, deep = true;
+                for (int ax = 0; ax < D; ax++) {
+                    const float dd = fabsf(torus_deltaf(X[ax] - q.c[ax]));
+                    miss |= dd > rout;
+                    deep &= dd < rin;
+                }
+                if (!miss) {
+                    if (deep) return 1;
+                    *gray = true;
+                }
+                p = q.next;
             }
-            p = q.next;
         }
     }
     return 0;
