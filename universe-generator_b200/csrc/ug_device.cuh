@@ -17,7 +17,7 @@ constexpr double kPi = 3.14159265358979323846;
 constexpr int kMaxF = 256;        // max frequency / timesteps per universe
 constexpr int kTile = 128;        // candidates per prefilter tile
 enum : int { kConflictCap = 48 };  // earlier in-round conflicts kept per survivor
-enum : int { kSmaxCap = 4096 };    // survivors resolved per universe per round (max)
+enum : int { kSmaxCap = 8192 };    // survivors resolved per universe per round (max)
 constexpr uint32_t kEmptyKey32 = 0xffffffffu;
 constexpr uint64_t kEmptyKey = ~0ull;
 
@@ -417,124 +417,146 @@ __device__ __forceinline__ int64_t occ1_bit(const UniDev& U, int t, const int* c
     for (int ax = 0; ax < U.dim; ax++) lin = lin * U.occ1_gw + (c[ax] >> (U.occ_shift + 3));
     return (int64_t)t * U.occ1_per_t + lin;
 }
-// True when some cell of the box [lo, hi] (per axis, taken modulo gw) may hold
-// a point at timestep t: checks the second-level bits covering the box.
-__device__ __forceinline__ bool occ1_any(const UniDev& U, int t, const int* lo, const int* hi) {
-    int v[3][4], n[3] = {1, 1, 1};
-    const int sh = U.occ_shift + 3;
-    for (int ax = 0; ax < U.dim; ax++) {
-        n[ax] = 0;
-        for (int c = lo[ax]; c <= hi[ax]; c++) {
-            int w = c % U.gw;
-            w = (w < 0 ? w + U.gw : w) >> sh;
-            bool seen = false;
-            for (int k = 0; k < n[ax]; k++) seen |= v[ax][k] == w;
-            if (!seen && n[ax] < 4) v[ax][n[ax]++] = w;
-        }
+
+__device__ __forceinline__ int wrap_cell(int v, int gw) {
+    v += v < 0 ? gw : 0;
+    return v >= gw ? v - gw : v;
+}
+
+// Neighbourhood of a point: per axis up to four wrapped cell coordinates
+// (centre +-1, widened by one on a side when the point lies within the guard
+// band of that cell face).  All loops below have constant trip counts and are
+// fully unrolled; nothing divides.
+template <int D>
+struct Nbhd {
+    int v[D][4];
+    int n[D];
+    int last[D];  // wrapped coordinate of the last cell per axis
+};
+
+template <int D>
+__device__ __forceinline__ void nbhd_make(const UniDev& U, const int* c, const int* ext_lo,
+                                          const int* ext_hi, Nbhd<D>& nb) {
+#pragma unroll
+    for (int ax = 0; ax < D; ax++) {
+        const int lo = c[ax] - 1 - ext_lo[ax];
+        nb.n[ax] = 3 + ext_lo[ax] + ext_hi[ax];
+        nb.last[ax] = wrap_cell(c[ax] + 1 + ext_hi[ax], U.gw);
+#pragma unroll
+        for (int k = 0; k < 4; k++) nb.v[ax][k] = wrap_cell(lo + k, U.gw);
     }
-    for (int i0 = 0; i0 < n[0]; i0++)
-        for (int i1 = 0; i1 < (U.dim > 1 ? n[1] : 1); i1++)
-            for (int i2 = 0; i2 < (U.dim > 2 ? n[2] : 1); i2++) {
-                int64_t lin = v[0][i0];
-                if (U.dim > 1) lin = lin * U.occ1_gw + v[1][i1];
-                if (U.dim > 2) lin = lin * U.occ1_gw + v[2][i2];
-                const int64_t b = (int64_t)t * U.occ1_per_t + lin;
-                if ((__ldcg(U.occ1 + (b >> 5)) >> (b & 31)) & 1u) return true;
-            }
+}
+
+// Second-level occupancy: false proves every cell of the neighbourhood empty.
+template <int D>
+__device__ __forceinline__ bool nbhd_occ1(const UniDev& U, int t, const Nbhd<D>& nb) {
+    const int sh = U.occ_shift + 3;
+    int bl[D][2];
+#pragma unroll
+    for (int ax = 0; ax < D; ax++) {
+        bl[ax][0] = nb.v[ax][0] >> sh;
+        bl[ax][1] = nb.last[ax] >> sh;
+    }
+    const uint32_t* base = U.occ1;
+    const int64_t t0 = (int64_t)t * U.occ1_per_t;
+#pragma unroll
+    for (int i = 0; i < (1 << D); i++) {
+        int64_t lin = 0;
+        bool dup = false;
+#pragma unroll
+        for (int ax = 0; ax < D; ax++) {
+            const int pick = (i >> ax) & 1;
+            dup |= pick && bl[ax][1] == bl[ax][0];
+            lin = lin * U.occ1_gw + bl[ax][pick];
+        }
+        if (dup) continue;
+        const int64_t b = t0 + lin;
+        if ((__ldcg(base + (b >> 5)) >> (b & 31)) & 1u) return true;
+    }
     return false;
 }
 
-// Occupancy of the cells (lo + i) mod gw, i = 0..n-1 (n <= 8), along the last
-// axis of the row whose leading coordinates are `pre` (row-major prefix of
-// the coarse bitmap index).  Bit i of the result set when cell lo + i may
-// hold a point.  One or two 32-bit words per contiguous segment.
-__device__ __forceinline__ uint32_t occ_row(const UniDev& U, int t, int64_t pre, int lo, int n) {
-    const int gw = U.gw, sh = U.occ_shift;
-    const int64_t rowbase = (int64_t)t * U.occ_per_t + pre * U.occ_gw;
-    uint32_t mask = 0;
-    int i = 0;
-    while (i < n) {
-        int c = (lo + i) % gw;
-        c = c < 0 ? c + gw : c;
-        int seg = gw - c;                 // cells until the seam
-        if (seg > n - i) seg = n - i;
-        const int b0 = c >> sh, b1 = (c + seg - 1) >> sh;
-        const int64_t bit0 = rowbase + b0;
-        const int64_t w0 = bit0 >> 5;
-        const int64_t w1 = (rowbase + b1) >> 5;
-        uint64_t bits = __ldcg(U.occ + w0);
-        if (w1 != w0) bits |= (uint64_t)__ldcg(U.occ + w1) << 32;
-        bits >>= (bit0 & 31);
-        for (int k = 0; k < seg; k++)
-            if ((bits >> (((c + k) >> sh) - b0)) & 1u) mask |= 1u << (i + k);
-        i += seg;
+// Visit the chains of the occupied cells of the neighbourhood at timestep t.
+// visit(p) returns true to stop (the scan then returns true).
+template <int D, class Visit>
+__device__ __forceinline__ bool nbhd_scan(const UniDev& U, int t, const Nbhd<D>& nb, int64_t cpt,
+                                          Visit&& visit) {
+    const int gw = U.gw, sh = U.occ_shift, ogw = U.occ_gw;
+    const int64_t tb = (int64_t)t * U.occ_per_t;
+#pragma unroll
+    for (int i0 = 0; i0 < 4; i0++) {
+        if (i0 >= nb.n[0]) break;
+        const int x0 = nb.v[0][i0];
+#pragma unroll
+        for (int i1 = 0; i1 < (D > 1 ? 4 : 1); i1++) {
+            if (D > 1 && i1 >= nb.n[D > 1 ? 1 : 0]) break;
+            const int x1 = D > 1 ? nb.v[D > 1 ? 1 : 0][i1] : 0;
+#pragma unroll
+            for (int i2 = 0; i2 < (D > 2 ? 4 : 1); i2++) {
+                if (D > 2 && i2 >= nb.n[D > 2 ? 2 : 0]) break;
+                const int x2 = D > 2 ? nb.v[D > 2 ? 2 : 0][i2] : 0;
+                int64_t ob = x0 >> sh, lin = x0;
+                if (D > 1) {
+                    ob = ob * ogw + (x1 >> sh);
+                    lin = lin * gw + x1;
+                }
+                if (D > 2) {
+                    ob = ob * ogw + (x2 >> sh);
+                    lin = lin * gw + x2;
+                }
+                ob += tb;
+                if (!((__ldcg(U.occ + (ob >> 5)) >> (ob & 31)) & 1u)) continue;
+                int32_t p = grid_head(U, t, lin, cpt);
+                while (p >= 0) {
+                    int32_t nx;
+                    if (visit(p, nx)) return true;
+                    p = nx;
+                }
+            }
+        }
     }
-    return mask;
+    return false;
 }
 
-// Contacts of the point P (dim coords) at timestep t with the accepted
-// packing.  Unique mode: returns true on the first contact.  Group mode:
-// accumulates the single touched group in *g and returns true when a second
-// distinct group appears.
+// Contacts of the point P at timestep t with the accepted packing (FP64,
+// exact): the neighbourhood is the centre cell +-1 on every axis.  Unique
+// mode: true on the first contact.  Group mode: accumulates the single
+// touched group in *g and returns true when a second distinct group appears.
+template <int D>
+__device__ __forceinline__ bool contacts64_d(const UniDev& U, int t, const double* P, bool group,
+                                             int32_t* g, int64_t cpt) {
+    int c[D], z[D];
+#pragma unroll
+    for (int ax = 0; ax < D; ax++) {
+        c[ax] = cell_of(P[ax], U.cell, U.gw);
+        z[ax] = 0;
+    }
+    Nbhd<D> nb;
+    nbhd_make<D>(U, c, z, z, nb);
+    if (!nbhd_occ1<D>(U, t, nb)) return false;
+    return nbhd_scan<D>(U, t, nb, cpt, [&](int32_t p, int32_t& nx) -> bool {
+        const Pt64* q = U.pts + (int64_t)p * U.T + t;
+        nx = __ldcg(&q->next);
+        bool hit = true;
+#pragma unroll
+        for (int ax = 0; ax < D; ax++)
+            hit = hit && hit1(torus_delta(P[ax] - __ldcg(&q->c[ax])), U.cell, U.inclusive);
+        if (!hit) return false;
+        if (!group) return true;
+        const int32_t gq = __ldcg(&q->gid);
+        if (*g == -1) {
+            *g = gq;
+            return false;
+        }
+        return *g != gq;
+    });
+}
+
 __device__ __forceinline__ bool contacts64(const UniDev& U, int t, const double* P, bool group,
                                            int32_t* g, int64_t cpt) {
-    int c[3], lo[3], hi[3];
-    for (int ax = 0; ax < U.dim; ax++) {
-        c[ax] = cell_of(P[ax], U.cell, U.gw);
-        lo[ax] = c[ax] - 1;
-        hi[ax] = c[ax] + 1;
-    }
-    if (!occ1_any(U, t, lo, hi)) return false;
-    const int D = U.dim, gw = U.gw, last = D - 1;
-    const int nrows = D == 1 ? 1 : (D == 2 ? 3 : 9);
-    uint32_t masks[9];
-#pragma unroll
-    for (int rw = 0; rw < 9; rw++) {
-        if (rw >= nrows) break;
-        int64_t pre = 0;
-        if (D >= 2) {
-            int r0 = D == 3 ? rw / 3 : rw;
-            int v0 = (c[0] + r0 - 1 + gw) % gw;
-            pre = v0 >> U.occ_shift;
-            if (D == 3) {
-                int v1 = (c[1] + rw % 3 - 1 + gw) % gw;
-                pre = pre * U.occ_gw + (v1 >> U.occ_shift);
-            }
-        }
-        masks[rw] = occ_row(U, t, pre, lo[last], 3);
-    }
-    for (int rw = 0; rw < nrows; rw++) {
-        uint32_t m = masks[rw];
-        while (m) {
-            const int i = __ffs(m) - 1;
-            m &= m - 1;
-            int cc[3];
-            if (D == 3) {
-                cc[0] = (c[0] + rw / 3 - 1 + gw) % gw;
-                cc[1] = (c[1] + rw % 3 - 1 + gw) % gw;
-            } else if (D == 2) {
-                cc[0] = (c[0] + rw - 1 + gw) % gw;
-            }
-            cc[last] = (lo[last] + i + gw) % gw;
-            int32_t p = grid_head(U, t, lin_cell(cc, D, gw), cpt);
-            while (p >= 0) {
-                const Pt64* q = U.pts + (int64_t)p * U.T + t;
-                bool hit = true;
-                for (int ax = 0; ax < D && hit; ax++)
-                    hit = hit1(torus_delta(P[ax] - __ldcg(&q->c[ax])), U.cell, U.inclusive);
-                if (hit) {
-                    if (!group) return true;
-                    const int32_t gq = __ldcg(&q->gid);
-                    if (*g == -1)
-                        *g = gq;
-                    else if (*g != gq)
-                        return true;
-                }
-                p = __ldcg(&q->next);
-            }
-        }
-    }
-    return false;
+    if (U.dim == 3) return contacts64_d<3>(U, t, P, group, g, cpt);
+    if (U.dim == 2) return contacts64_d<2>(U, t, P, group, g, cpt);
+    return contacts64_d<1>(U, t, P, group, g, cpt);
 }
 
 // 1+1D crossing rule: minimum-image separation changes sign between

@@ -199,7 +199,7 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
     }
     d.B_max = c.round_size ? c.round_size : 65536;
     const int T = c.T;
-    d.S_max = (int)std::min<int64_t>(kSmaxCap, std::max<int64_t>(256, (1 << 18) / T));
+    d.S_max = (int)std::min<int64_t>(kSmaxCap, std::max<int64_t>(256, (1 << 20) / T));
     if (c.dim == 1) d.S_max = 256;  // 1+1D in-round conflicts are found pairwise
     d.S_max = std::min(d.S_max, d.B_max);
     // tables
@@ -290,7 +290,7 @@ static void init_ctl(const ug_universe_cfg& c, const UniDev& d, UniCtl& k) {
     k.state = ST_ACTIVE;
     k.B_min = std::min(1024, d.B_max);
     k.B_cap = d.B_max;
-    k.round_B = std::min(4096, d.B_max);  // grows toward B_cap once survivors thin out
+    k.round_B = std::min(std::max(4096, 2 * d.S_max), d.B_max);  // adapted every round
     k.accept_rate = c.accept_rate;
     k.sub_accept_rate = c.sub_accept_rate;
     k.win_target = c.accept_rate > 0 ? (int64_t)std::min(5e9, std::max(2e7, 30.0 / c.accept_rate)) : 0;
@@ -350,7 +350,7 @@ static int launch_round(Batch& B, bool timed) {
     k_conflicts<<<B.nsm * 8, 128, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
     te(K_CONFL);
     tb(K_GREEDY);
-    k_greedy<<<B.n, 32, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+    k_greedy<<<B.n, 32, 2 * kSmaxCap * sizeof(int32_t), B.st>>>(B.dU, B.dCtl, B.dInfo);
     te(K_GREEDY);
     tb(K_COMMIT);
     k_commit<<<B.nsm * 8, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
@@ -525,6 +525,9 @@ int ug_batch_create(const ug_universe_cfg* cfgs, int32_t n, const ug_run_opts* o
         cudaMemcpy(B->dInfo, &ri, sizeof ri, cudaMemcpyHostToDevice) != cudaSuccess)
         return bail(fail(UG_ECUDA, "control block upload failed"));
     if ((rc = push_unidev(*B))) return bail(rc);
+    if (cudaFuncSetAttribute(k_greedy, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(2 * kSmaxCap * sizeof(int32_t))) != cudaSuccess)
+        return bail(fail(UG_ECUDA, "smem attribute failed"));
     if (cudaFuncSetAttribute(k_surv_eval, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(kSurvWarps * kSurvSmemPerWarp)) != cudaSuccess)
         return bail(fail(UG_ECUDA, "smem attribute failed"));

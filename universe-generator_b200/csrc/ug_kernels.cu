@@ -618,8 +618,9 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
 // sequential-RSA rule holds against the round's earlier admissions.
 __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, UniCtl* ctl,
                                                RoundInfo* info) {
-    __shared__ int32_t acc_s[kSmaxCap];
-    __shared__ int32_t gid_s[kSmaxCap];
+    extern __shared__ int32_t greedy_smem[];
+    int32_t* acc_s = greedy_smem;
+    int32_t* gid_s = greedy_smem + kSmaxCap;
     const int u = blockIdx.x;
     const int lane = threadIdx.x;
     const UniDev& d = U[u];
@@ -722,11 +723,13 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
     c.attempts = next;
     c.rounds++;
     if (grow) c.state = ST_GROW;
-    // round-size adaptation toward 64..512 survivors (braid_cuda.cu:921-924);
-    // admission results do not depend on it
-    if (c.S_raw > 512 && c.round_B > c.B_min)
+    // round-size adaptation (the reference steers toward 64..512 survivors for
+    // its serial host admission, braid_cuda.cu:921-924; the device resolver
+    // takes up to S_max, so steer toward the survivor capacity instead).
+    // Admission results do not depend on it.
+    if (c.S_raw > d.S_max && c.round_B > c.B_min)
         c.round_B >>= 1;
-    else if (c.S_raw < 64 && c.round_B < c.B_cap)
+    else if (c.S_raw < d.S_max / 4 && c.round_B < c.B_cap)
         c.round_B <<= 1;
     // windowed accept-rate stop
     const double thr = c.phase == 1 ? c.accept_rate : c.sub_accept_rate;

@@ -209,81 +209,53 @@ __device__ __forceinline__ double gen_quarter(const UniDev& d, uint64_t idx, int
 // FP32 Chebyshev test of X (dim coords) at timestep t against the committed
 // packing.  Returns 1 on a certain contact; sets *gray when a pair lies in the
 // guard band.  The cell range covers every point within r + m of X.
-__device__ __forceinline__ int test32_at(const UniDev& d, int t, const float* X, float r, float m,
-                                         float inv_cell, int64_t cpt, bool* gray) {
-    int lo[3], hi[3];
+template <int D>
+__device__ __forceinline__ int test32_d(const UniDev& d, int t, const float* X, float r, float m,
+                                        float inv_cell, int64_t cpt, bool* gray) {
     const float band = m * inv_cell + 1e-4f;
-    const int D = d.dim, gw = d.gw, last = D - 1;
+    int c[D], elo[D], ehi[D];
+#pragma unroll
     for (int ax = 0; ax < D; ax++) {
         const float u = (X[ax] + 1.0f) * inv_cell;
         const float fl = floorf(u);
         const float fr = u - fl;
-        int c = (int)fl;
-        c = c >= gw ? gw - 1 : (c < 0 ? 0 : c);
-        lo[ax] = c - 1 - (fr < band ? 1 : 0);
-        hi[ax] = c + 1 + (fr > 1.0f - band ? 1 : 0);
+        int cc = (int)fl;
+        c[ax] = cc >= d.gw ? d.gw - 1 : (cc < 0 ? 0 : cc);
+        elo[ax] = fr < band ? 1 : 0;
+        ehi[ax] = fr > 1.0f - band ? 1 : 0;
     }
-    if (!occ1_any(d, t, lo, hi)) return 0;
+    Nbhd<D> nb;
+    nbhd_make<D>(d, c, elo, ehi, nb);
+    if (!nbhd_occ1<D>(d, t, nb)) return 0;
     const float rin = r - m, rout = r + m;
-    // rows over the leading axes, occupancy words along the last axis
-    const int n0 = D >= 2 ? hi[0] - lo[0] + 1 : 1;
-    const int n1 = D == 3 ? hi[1] - lo[1] + 1 : 1;
-    const int nl = hi[last] - lo[last] + 1;
-    if (n0 * n1 > 16 || nl > 8) {  // cannot happen while the band is below half a cell
-        *gray = true;
-        return 0;
-    }
-    uint32_t masks[16];
+    bool g = false;
+    const bool deep = nbhd_scan<D>(d, t, nb, cpt, [&](int32_t p, int32_t& nx) -> bool {
+        const Pt32 q = d.ptf[(int64_t)p * d.T + t];
+        nx = q.next;
+        bool miss = false, in = true;
 #pragma unroll
-    for (int rw = 0; rw < 16; rw++) {
-        if (rw >= n0 * n1) break;
-        int64_t pre = 0;
-        if (D >= 2) {
-            int v0 = (lo[0] + rw / n1) % gw;
-            v0 = v0 < 0 ? v0 + gw : v0;
-            pre = v0 >> d.occ_shift;
-            if (D == 3) {
-                int v1 = (lo[1] + rw % n1) % gw;
-                v1 = v1 < 0 ? v1 + gw : v1;
-                pre = pre * d.occ_gw + (v1 >> d.occ_shift);
-            }
+        for (int ax = 0; ax < D; ax++) {
+            const float dd = fabsf(torus_deltaf(X[ax] - q.c[ax]));
+            miss |= dd > rout;
+            in &= dd < rin;
         }
-        masks[rw] = occ_row(d, t, pre, lo[last], nl);
-    }
-    for (int rw = 0; rw < n0 * n1; rw++) {
-        uint32_t mk = masks[rw];
-        while (mk) {
-            const int i = __ffs(mk) - 1;
-            mk &= mk - 1;
-            int cc[3];
-            if (D >= 2) {
-                int v0 = (lo[0] + rw / n1) % gw;
-                cc[0] = v0 < 0 ? v0 + gw : v0;
-                if (D == 3) {
-                    int v1 = (lo[1] + rw % n1) % gw;
-                    cc[1] = v1 < 0 ? v1 + gw : v1;
-                }
-            }
-            int vl = (lo[last] + i) % gw;
-            cc[last] = vl < 0 ? vl + gw : vl;
-            int32_t p = grid_head(d, t, lin_cell(cc, D, gw), cpt);
-            while (p >= 0) {
-                const Pt32 q = d.ptf[(int64_t)p * d.T + t];
-                bool miss = false, deep = true;
-                for (int ax = 0; ax < D; ax++) {
-                    const float dd = fabsf(torus_deltaf(X[ax] - q.c[ax]));
-                    miss |= dd > rout;
-                    deep &= dd < rin;
-                }
-                if (!miss) {
-                    if (deep) return 1;
-                    *gray = true;
-                }
-                p = q.next;
-            }
-        }
-    }
-    return 0;
+        if (miss) return false;
+        if (in) return true;
+        g = true;
+        return false;
+    });
+    if (g) *gray = true;
+    return deep ? 1 : 0;
+}
+
+// FP32 Chebyshev test of X at timestep t against the committed packing.
+// Returns 1 on a certain contact; sets *gray when a pair lies in the guard
+// band.  The neighbourhood covers every cell within r + m of X.
+__device__ __forceinline__ int test32_at(const UniDev& d, int t, const float* X, float r, float m,
+                                         float inv_cell, int64_t cpt, bool* gray) {
+    if (d.dim == 3) return test32_d<3>(d, t, X, r, m, inv_cell, cpt, gray);
+    if (d.dim == 2) return test32_d<2>(d, t, X, r, m, inv_cell, cpt, gray);
+    return test32_d<1>(d, t, X, r, m, inv_cell, cpt, gray);
 }
 
 // --------------------------------------------------------------- kernel
