@@ -13,6 +13,28 @@
 
 namespace ug {
 
+// Index guard.  The product build compiles UG_IDX(i, n) to i.  The checked
+// build (-DUG_CHECKED) records the first out-of-range index (source line,
+// index, bound) in ug_check_record and substitutes 0, so a bad index is
+// reported instead of dereferenced.
+#ifdef UG_CHECKED
+extern __device__ unsigned long long ug_check_record[4];
+__device__ __noinline__ static int64_t ug_idx_fail(int64_t i, int64_t n, int line) {
+    if (atomicCAS(&ug_check_record[0], 0ull, (unsigned long long)line) == 0ull) {
+        ug_check_record[1] = (unsigned long long)i;
+        ug_check_record[2] = (unsigned long long)n;
+        ug_check_record[3] = 1ull;
+    }
+    return 0;
+}
+__device__ __forceinline__ int64_t ug_idx(int64_t i, int64_t n, int line) {
+    return ((uint64_t)i < (uint64_t)n) ? i : ug_idx_fail(i, n, line);
+}
+#define UG_IDX(i, n) ::ug::ug_idx((int64_t)(i), (int64_t)(n), __LINE__)
+#else
+#define UG_IDX(i, n) (i)
+#endif
+
 constexpr double kPi = 3.14159265358979323846;
 constexpr int kMaxF = 256;        // max frequency / timesteps per universe
 constexpr int kTile = 128;        // candidates per prefilter tile
@@ -103,6 +125,8 @@ struct UniDev {
     int32_t mx_nmma;         // UMMA N per pass
     int32_t mx_npass;        // timestep passes (2 when dim * tpad > 512 TMEM columns)
     float mx_margin;         // guard band of the FP32 Chebyshev test
+    // sizes (index guards of the checked build)
+    int64_t occ_words, occ1_words, dense_cells, bimg_bytes;
 };
 
 // Mutable per-universe control block (device).
@@ -385,12 +409,12 @@ __device__ __forceinline__ int64_t lin_cell(const int* c, int dim, int gw) {
 
 // Head of the chain of accepted points in cell `lin` at timestep t (-1 none).
 __device__ __forceinline__ int32_t grid_head(const UniDev& U, int t, int64_t lin, int64_t cells_per_t) {
-    if (U.grid_kind == GRID_DENSE) return __ldcg(U.heads + (int64_t)t * cells_per_t + lin);
+    if (U.grid_kind == GRID_DENSE) return __ldcg(U.heads + UG_IDX((int64_t)t * cells_per_t + lin, U.dense_cells));
     const uint64_t key = ((uint64_t)t << 40) | (uint64_t)lin;
     uint64_t h = mix64(key) & U.hmask;
     for (uint64_t probe = 0; probe <= U.hmask; probe++) {
-        const uint64_t k = __ldcg(U.hkeys + h);
-        if (k == key) return __ldcg(U.heads + h);
+        const uint64_t k = __ldcg(U.hkeys + UG_IDX(h, U.hmask + 1));
+        if (k == key) return __ldcg(U.heads + UG_IDX(h, U.hmask + 1));
         if (k == kEmptyKey) return -1;
         h = (h + 1) & U.hmask;
     }
@@ -471,7 +495,7 @@ __device__ __forceinline__ bool nbhd_occ1(const UniDev& U, int t, const Nbhd<D>&
         }
         if (dup) continue;
         const int64_t b = t0 + lin;
-        if ((__ldcg(base + (b >> 5)) >> (b & 31)) & 1u) return true;
+        if ((__ldcg(base + UG_IDX(b >> 5, U.occ1_words)) >> (b & 31)) & 1u) return true;
     }
     return false;
 }
@@ -505,7 +529,7 @@ __device__ __forceinline__ bool nbhd_scan(const UniDev& U, int t, const Nbhd<D>&
                     lin = lin * gw + x2;
                 }
                 ob += tb;
-                if (!((__ldcg(U.occ + (ob >> 5)) >> (ob & 31)) & 1u)) continue;
+                if (!((__ldcg(U.occ + UG_IDX(ob >> 5, U.occ_words)) >> (ob & 31)) & 1u)) continue;
                 int32_t p = grid_head(U, t, lin, cpt);
                 while (p >= 0) {
                     int32_t nx;
@@ -535,7 +559,7 @@ __device__ __forceinline__ bool contacts64_d(const UniDev& U, int t, const doubl
     nbhd_make<D>(U, c, z, z, nb);
     if (!nbhd_occ1<D>(U, t, nb)) return false;
     return nbhd_scan<D>(U, t, nb, cpt, [&](int32_t p, int32_t& nx) -> bool {
-        const Pt64* q = U.pts + (int64_t)p * U.T + t;
+        const Pt64* q = U.pts + UG_IDX((int64_t)p * U.T + t, U.slot_cap * U.T);
         nx = __ldcg(&q->next);
         bool hit = true;
 #pragma unroll

@@ -22,6 +22,10 @@
 
 namespace ug {
 
+#ifdef UG_CHECKED
+__device__ unsigned long long ug_check_record[4];
+#endif
+
 static thread_local std::string g_err;
 
 static int fail(int code, const char* fmt, ...) {
@@ -227,6 +231,7 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
     if (!B.opts.force_hash && dense <= (int64_t)4 << 30 && *dense_used + dense <= dense_budget) {
         d.grid_kind = GRID_DENSE;
         if ((rc = dalloc(h, &d.heads, (size_t)T * cpt, 0xff))) return rc;
+        d.dense_cells = (int64_t)T * cpt;
         h.dense_bytes = dense;
         *dense_used += dense;
     } else {
@@ -251,12 +256,14 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
             }
         }
         h.occ_words = (bits + 31) / 32;
+        d.occ_words = h.occ_words;
         if ((rc = dalloc(h, &d.occ, (size_t)h.occ_words, 0))) return rc;
         d.occ1_gw = (d.occ_gw + 7) >> 3;
         int64_t per1 = 1;
         for (int ax = 0; ax < c.dim; ax++) per1 *= d.occ1_gw;
         d.occ1_per_t = per1;
         h.occ1_words = ((int64_t)T * per1 + 31) / 32;
+        d.occ1_words = h.occ1_words;
         if ((rc = dalloc(h, &d.occ1, (size_t)h.occ1_words, 0))) return rc;
     }
     // accepted points
@@ -384,6 +391,13 @@ static int pull_ctl(Batch& B) {
     CKR(cudaMemcpyAsync(B.hCtl.data(), B.dCtl, sizeof(UniCtl) * B.n, cudaMemcpyDeviceToHost, B.st));
     B.d2h += sizeof(UniCtl) * B.n;
     CKR(cudaStreamSynchronize(B.st));
+#ifdef UG_CHECKED
+    unsigned long long rec[4] = {0, 0, 0, 0};
+    CKR(cudaMemcpyFromSymbol(rec, ug_check_record, sizeof rec));
+    if (rec[3])
+        return fail(UG_ECAP, "index guard: source line %llu index %lld bound %lld", rec[0], (long long)rec[1],
+                    (long long)rec[2]);
+#endif
     B.synced = true;
     return UG_OK;
 }

@@ -91,7 +91,7 @@ __device__ bool test64(const UniDev& d, int64_t n_slots, const double* alpha, co
         for (int t = 0; t < T; t++) P[t] = eval64(d, alpha, beta, 1, a2[0], t);
         *nev = T;
         for (int64_t s = 0; s < n_slots; s++) {
-            const Pt64* q = d.pts + s * T;
+            const Pt64* q = d.pts + UG_IDX(s * T + T - 1, d.slot_cap * T) + 1 - T;
             double d0 = torus_delta(P[0] - __ldcg(&q[0].c[0]));
             bool hit = hit1(d0, d.cell, d.inclusive);
             for (int t = 1; t < T && !hit; t++) {
@@ -166,9 +166,9 @@ __device__ __forceinline__ void prefilter64_tiles(const UniDev* __restrict__ U, 
             if (work && surv) atomicOr(&d.surv_bits[off >> 5], 1u << (off & 31));
         } else {
             const uint32_t bits = __ballot_sync(0xffffffffu, surv);
-            if (lane == 0 && (off & ~31) < d.B_max) d.surv_bits[off >> 5] = bits;
+            if (lane == 0 && (off & ~31) < d.B_max) d.surv_bits[UG_IDX(off >> 5, d.B_max / 32)] = bits;
         }
-        if (work && d.group_mode != GROUP_NONE) d.g0[off] = g;
+        if (work && d.group_mode != GROUP_NONE) d.g0[UG_IDX(off, d.B_max)] = g;
     }
 }
 
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(256) k_compact(const UniDev* __restrict__ U, U
         while (bits) {
             const int bit = __ffs(bits) - 1;
             bits &= bits - 1;
-            if (rank <= d.S_max) d.surv_off[rank] = w * 32 + bit;
+            if (rank <= d.S_max) d.surv_off[UG_IDX(rank, d.S_max + 1)] = w * 32 + bit;
             rank++;
         }
         __syncthreads();
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_surv_eval(const UniDev* __r
         const int r = item - info->surv_off[u];
         const UniDev& d = U[u];
         const UniCtl& c = ctl[u];
-        const uint64_t idx = (uint64_t)(c.round_base + d.surv_off[r]);
+        const uint64_t idx = (uint64_t)(c.round_base + d.surv_off[UG_IDX(r, d.S_max + 1)]);
         const int F1 = d.F + 1, T = d.T;
         warp_gen64(d, idx, alpha, beta, a2, bj, wj, lane);
         const int64_t cpt = cells_per_t(d);
@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_surv_eval(const UniDev* __r
             }
             q.next = nxt;
             q.gid = -1;
-            d.spos[(int64_t)r * T + t] = q;
+            d.spos[UG_IDX((int64_t)r * T + t, (int64_t)d.S_max * T)] = q;
         }
         __syncwarp();
     }
@@ -421,7 +421,8 @@ __global__ void __launch_bounds__(256) k_gray_compact(const UniDev* __restrict__
         while (bits) {
             const int bit = __ffs(bits) - 1;
             bits &= bits - 1;
-            d.gray_off[rank++] = w * 32 + bit;
+            d.gray_off[UG_IDX(rank, d.B_max)] = w * 32 + bit;
+            rank++;
         }
         __syncthreads();
         if (tid == 0) s_running += tot;
@@ -466,7 +467,7 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_confirm64w(const UniDev* __
         const int u = find_uni(info->gray_pref, n_uni, item);
         const UniDev& d = U[u];
         UniCtl& c = ctl[u];
-        const int off = d.gray_off[item - info->gray_pref[u]];
+        const int off = d.gray_off[UG_IDX(item - info->gray_pref[u], d.B_max)];
         const uint64_t idx = (uint64_t)(c.round_base + off);
         const int F1 = d.F + 1, T = d.T;
         warp_gen64(d, idx, alpha, beta, a2, bj, wj, lane);
@@ -479,7 +480,7 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_confirm64w(const UniDev* __
             __syncwarp();
             nev = lane == 0 ? T : 0;
             for (int64_t s = lane; s < c.n_slots && !(hitl && !group); s += 32) {
-                const Pt64* q = d.pts + s * T;
+                const Pt64* q = d.pts + UG_IDX(s * T + T - 1, d.slot_cap * T) + 1 - T;
                 double d0 = torus_delta(P1[0] - __ldcg(&q[0].c[0]));
                 bool hit = hit1(d0, d.cell, d.inclusive);
                 for (int t = 1; t < T && !hit; t++) {
@@ -524,8 +525,8 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_confirm64w(const UniDev* __
         if (group) rej = rej || __any_sync(0xffffffffu, g != -1 && g != first);
         for (int o = 16; o > 0; o >>= 1) nev += __shfl_xor_sync(0xffffffffu, nev, o);
         if (lane == 0) {
-            if (!rej) atomicOr(&d.surv_bits[off >> 5], 1u << (off & 31));
-            if (d.group_mode != GROUP_NONE) d.g0[off] = first;
+            if (!rej) atomicOr(&d.surv_bits[UG_IDX(off >> 5, d.B_max / 32)], 1u << (off & 31));
+            if (d.group_mode != GROUP_NONE) d.g0[UG_IDX(off, d.B_max)] = first;
             if (nev) atomicAdd((unsigned long long*)&c.evals_fp64, (unsigned long long)nev);
         }
         __syncwarp();
@@ -559,9 +560,9 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
             if (pos < kConflictCap) lst[pos] = r2;
         };
         if (d.dim == 1 && d.cross1d) {
-            const Pt64* P = d.spos + (int64_t)r * T;
+            const Pt64* P = d.spos + UG_IDX((int64_t)r * T + T - 1, (int64_t)d.S_max * T) + 1 - T;
             for (int r2 = lane; r2 < r; r2 += 32) {
-                const Pt64* Q = d.spos + (int64_t)r2 * T;
+                const Pt64* Q = d.spos + UG_IDX((int64_t)r2 * T + T - 1, (int64_t)d.S_max * T) + 1 - T;
                 double d0 = torus_delta(P[0].c[0] - Q[0].c[0]);
                 bool hit = hit1(d0, d.cell, d.inclusive);
                 for (int t = 1; t < T && !hit; t++) {
@@ -574,7 +575,7 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
         } else {
             const int nb = d.dim == 1 ? 3 : (d.dim == 2 ? 9 : 27);
             for (int t = lane; t < T; t += 32) {
-                const Pt64 P = d.spos[(int64_t)r * T + t];
+                const Pt64 P = d.spos[UG_IDX((int64_t)r * T + t, (int64_t)d.S_max * T)];
                 int c0[3];
                 for (int ax = 0; ax < d.dim; ax++) c0[ax] = cell_of(P.c[ax], d.cell, d.gw);
                 for (int k = 0; k < nb; k++) {
@@ -588,7 +589,7 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
                     }
                     int32_t r2 = rhash_head(d, rkey_of(c.epoch, t, lin_cell(cc, d.dim, d.gw)));
                     while (r2 >= 0) {
-                        const Pt64* Q = d.spos + (int64_t)r2 * T + t;
+                        const Pt64* Q = d.spos + UG_IDX((int64_t)r2 * T + t, (int64_t)d.S_max * T);
                         if (r2 < r) {
                             bool hit = true;
                             for (int ax = 0; ax < d.dim && hit; ax++)
@@ -605,8 +606,8 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
         if (n > kConflictCap) {
             if (lane == 0) atomicMin(&c.trunc, r);
         } else {
-            for (int i = lane; i < n; i += 32) d.clist[(int64_t)r * kConflictCap + i] = lst[i];
-            if (lane == 0) d.ccount[r] = n;
+            for (int i = lane; i < n; i += 32) d.clist[UG_IDX((int64_t)r * kConflictCap + i, (int64_t)d.S_max * kConflictCap)] = lst[i];
+            if (lane == 0) d.ccount[UG_IDX(r, d.S_max)] = n;
         }
         __syncwarp();
     }
@@ -640,13 +641,13 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
             grow = true;
             break;
         }
-        const int n = d.ccount[r];
-        const int32_t* lst = d.clist + (int64_t)r * kConflictCap;
+        const int n = d.ccount[UG_IDX(r, d.S_max)];
+        const int32_t* lst = d.clist + UG_IDX((int64_t)r * kConflictCap, (int64_t)d.S_max * kConflictCap);
         bool accept;
         int32_t gid;
         if (!group) {
             bool any = false;
-            for (int i = lane; i < n; i += 32) any |= acc_s[lst[i]] >= 0;
+            for (int i = lane; i < n; i += 32) any |= acc_s[UG_IDX(lst[i], kSmaxCap)] >= 0;
             accept = !__any_sync(0xffffffffu, any);
             gid = (int32_t)(c.n_slots + k);
         } else {
@@ -654,7 +655,7 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
             int32_t mine = -1;
             bool two = false;
             for (int i = lane; i < n; i += 32) {
-                const int r2 = lst[i];
+                const int r2 = (int)UG_IDX(lst[i], kSmaxCap);
                 if (acc_s[r2] >= 0) {
                     const int32_t g2 = gid_s[r2];
                     if (mine == -1)
@@ -683,8 +684,8 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
             }
         }
         if (lane == 0) {
-            acc_s[r] = accept ? k : -1;
-            gid_s[r] = accept ? gid : -1;
+            acc_s[UG_IDX(r, kSmaxCap)] = accept ? k : -1;
+            gid_s[UG_IDX(r, kSmaxCap)] = accept ? gid : -1;
         }
         __syncwarp();
         if (accept) {
@@ -701,15 +702,15 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
         }
     }
     for (int r = lane; r < S; r += 32) {
-        d.acc_rank[r] = r < stop_at ? acc_s[r] : -1;
-        d.sgid[r] = r < stop_at ? gid_s[r] : -1;
+        d.acc_rank[UG_IDX(r, d.S_max)] = r < stop_at ? acc_s[UG_IDX(r, kSmaxCap)] : -1;
+        d.sgid[UG_IDX(r, d.S_max)] = r < stop_at ? gid_s[UG_IDX(r, kSmaxCap)] : -1;
     }
     if (lane != 0) return;
     int64_t next;
     if (hit_max)
-        next = c.round_base + d.surv_off[stop_at - 1] + 1;
+        next = c.round_base + d.surv_off[UG_IDX(stop_at - 1, d.S_max + 1)] + 1;
     else if (stop_at < c.S_raw)
-        next = c.round_base + d.surv_off[stop_at];
+        next = c.round_base + d.surv_off[UG_IDX(stop_at, d.S_max + 1)];
     else
         next = c.round_base + c.B;
     const int64_t used = next - c.round_base;
@@ -770,7 +771,7 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
 __device__ __forceinline__ void grid_insert(const UniDev& d, UniCtl& c, int t, int64_t lin,
                                             int64_t cpt, int32_t slot, int32_t* old_head) {
     if (d.grid_kind == GRID_DENSE) {
-        *old_head = atomicExch(d.heads + (int64_t)t * cpt + lin, slot);
+        *old_head = atomicExch(d.heads + UG_IDX((int64_t)t * cpt + lin, d.dense_cells), slot);
         return;
     }
     const uint64_t key = ((uint64_t)t << 40) | (uint64_t)lin;
@@ -813,30 +814,30 @@ __global__ void __launch_bounds__(256) k_commit(const UniDev* __restrict__ U, Un
         UniCtl& c = ctl[u];
         const int r = item - info->surv_off[u];
         if (r >= c.stop_at) continue;
-        const int k = d.acc_rank[r];
+        const int k = d.acc_rank[UG_IDX(r, d.S_max)];
         if (k < 0) continue;
-        const int64_t slot = c.n_slots_prev + k;
-        Pt64 q = d.spos[(int64_t)r * d.T + t];
+        const int64_t slot = UG_IDX(c.n_slots_prev + k, d.slot_cap);
+        Pt64 q = d.spos[UG_IDX((int64_t)r * d.T + t, (int64_t)d.S_max * d.T)];
         int cc[3];
         for (int ax = 0; ax < d.dim; ax++) cc[ax] = cell_of(q.c[ax], d.cell, d.gw);
         int32_t old;
         grid_insert(d, c, t, lin_cell(cc, d.dim, d.gw), cells_per_t(d), (int32_t)slot, &old);
         {
             const int64_t b = occ_bit(d, t, cc);
-            atomicOr(d.occ + (b >> 5), 1u << (b & 31));
+            atomicOr(d.occ + UG_IDX(b >> 5, d.occ_words), 1u << (b & 31));
             const int64_t b1 = occ1_bit(d, t, cc);
-            atomicOr(d.occ1 + (b1 >> 5), 1u << (b1 & 31));
+            atomicOr(d.occ1 + UG_IDX(b1 >> 5, d.occ1_words), 1u << (b1 & 31));
         }
         q.next = old;
-        q.gid = d.sgid[r];
-        d.pts[slot * d.T + t] = q;
+        q.gid = d.sgid[UG_IDX(r, d.S_max)];
+        d.pts[UG_IDX(slot * d.T + t, d.slot_cap * d.T)] = q;
         Pt32 f;
         f.c[0] = (float)q.c[0];
         f.c[1] = (float)q.c[1];
         f.c[2] = (float)q.c[2];
         f.next = old;
-        d.ptf[slot * d.T + t] = f;
-        if (t == 0) d.acc_idx[slot] = c.round_base + d.surv_off[r];
+        d.ptf[UG_IDX(slot * d.T + t, d.slot_cap * d.T)] = f;
+        if (t == 0) d.acc_idx[UG_IDX(slot, d.slot_cap)] = c.round_base + d.surv_off[UG_IDX(r, d.S_max + 1)];
     }
 }
 

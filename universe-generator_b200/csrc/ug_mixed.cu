@@ -230,7 +230,7 @@ __device__ __forceinline__ int test32_d(const UniDev& d, int t, const float* X, 
     const float rin = r - m, rout = r + m;
     bool g = false;
     const bool deep = nbhd_scan<D>(d, t, nb, cpt, [&](int32_t p, int32_t& nx) -> bool {
-        const Pt32 q = d.ptf[(int64_t)p * d.T + t];
+        const Pt32 q = d.ptf[UG_IDX((int64_t)p * d.T + t, d.slot_cap * d.T)];
         nx = q.next;
         bool miss = false, in = true;
 #pragma unroll
@@ -329,8 +329,8 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
             if (part == 0) {
                 const uint32_t g = __ballot_sync(0xffffffffu, valid);
                 if (lane == 0 && !dump) {
-                    d.surv_bits[off >> 5] = 0u;
-                    d.gray_bits[off >> 5] = g;
+                    d.surv_bits[UG_IDX(off >> 5, d.B_max / 32)] = 0u;
+                    d.gray_bits[UG_IDX(off >> 5, d.B_max / 32)] = g;
                 }
             }
             continue;
@@ -370,7 +370,8 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                     }
                     if (tid == 0) {
                         mbar_expect_tx(&bar_b[st], bchunk);
-                        bulk_g2s(b_img, d.mx_bimg + (size_t)ch * bchunk, bchunk, &bar_b[st]);
+                        bulk_g2s(b_img, d.mx_bimg + UG_IDX((int64_t)ch * bchunk + bchunk - 1, d.bimg_bytes) + 1 - bchunk,
+                                 bchunk, &bar_b[st]);
                     }
                     sumE += gen_quarter(d, idx, ax, ch, part, valid, a_hi, a_lo, row);
                     fence_proxy_async();
@@ -382,7 +383,7 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                             const uint32_t ah = smem_u32(a_hi), al = smem_u32(a_lo);
                             const uint32_t bh = smem_u32(b_img) + (uint32_t)(pass * nm * 16);
                             const uint32_t bl = bh + (uint32_t)tpad * kKC * 2;
-                            const uint32_t dtm = tmem + (uint32_t)(ax * nm);
+                            const uint32_t dtm = tmem + (uint32_t)UG_IDX(ax * nm + nm - 1, L.ncols) + 1 - nm;
 #pragma unroll
                             for (int j = 0; j < kKC / 16; j++) {
                                 const uint64_t dah = sdesc(ah + j * 2 * (kTile * 16), kTile * 16, 128);
@@ -424,7 +425,8 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                 if (col0 >= T) break;
                 if (!dump && __all_sync(0xffffffffu, vrej[row] != 0)) break;
                 float x[3][8];
-                for (int ax = 0; ax < dim; ax++) tmem_ld8(lane_base + (uint32_t)(ax * nm + c0), x[ax]);
+                for (int ax = 0; ax < dim; ax++)
+                    tmem_ld8(lane_base + (uint32_t)UG_IDX(ax * nm + c0 + 7, L.ncols) - 7, x[ax]);
                 tmem_wait_ld();
                 for (int j = 0; j < 8; j++) {
                     const int col = col0 + j;
@@ -458,8 +460,8 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                 const uint32_t sb = __ballot_sync(0xffffffffu, surv);
                 const uint32_t gb = __ballot_sync(0xffffffffu, gr);
                 if (lane == 0) {
-                    d.surv_bits[off >> 5] = sb;
-                    d.gray_bits[off >> 5] = gb;
+                    d.surv_bits[UG_IDX(off >> 5, d.B_max / 32)] = sb;
+                    d.gray_bits[UG_IDX(off >> 5, d.B_max / 32)] = gb;
                     const int ng = __popc(gb);
                     if (ng) atomicAdd((unsigned long long*)&ctl[u].gray_total, (unsigned long long)ng);
                 }
@@ -599,6 +601,7 @@ int mixed_setup(const ug_universe_cfg& cfg, UniDev& d, MixedTables& mt) {
     if (cudaMemcpy(dimg, host.data(), host.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess) return UG_ECUDA;
     mt.bhi = dimg;
     d.mx_bimg = (const uint8_t*)dimg;
+    d.bimg_bytes = (int64_t)host.size() * 2;
     // tensor-memory columns: the widest universe decides (power of two >= 32)
     if (tpad > g_tpad_max) g_tpad_max = tpad;
     int cols = dim * nm;

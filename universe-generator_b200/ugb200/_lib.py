@@ -10,7 +10,8 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libug.so")
+# UG_LIB=checked selects the index-guarded diagnostic build (libug_checked.so)
+LIB_PATH = os.path.join(HERE, "libug_checked.so" if os.environ.get("UG_LIB") == "checked" else "libug.so")
 
 UG_OK, UG_EINVAL, UG_ENOMEM, UG_ECAP, UG_ECUDA, UG_ETIMEDOUT, UG_ENOTSUP = range(7)
 RNG_PHILOX, RNG_KNOT = 0, 1

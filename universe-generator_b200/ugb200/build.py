@@ -33,18 +33,24 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(p) <= t for p in deps if os.path.exists(p))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
+LIB_CHECKED = os.path.join(HERE, "libug_checked.so")
+
+
+def build(force: bool = False, verbose: bool = False, checked: bool = False) -> str:
+    """Build libug.so, or with checked=True the index-guarded libug_checked.so
+    (separate device compilation so the guard record has one definition)."""
+    lib = LIB_CHECKED if checked else LIB
+    if not force and not checked and up_to_date():
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *FLAGS, "-o", LIB + ".tmp", *sources()]
+    extra = ["-DUG_CHECKED", "-rdc=true"] if checked else []
+    cmd = [nvcc, *FLAGS, *extra, "-o", lib + ".tmp", *sources()]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True, cwd=CSRC)
-    os.replace(LIB + ".tmp", LIB)
-    return LIB
+    os.replace(lib + ".tmp", lib)
+    return lib
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
-    print(LIB)
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv, checked="--checked" in sys.argv))
