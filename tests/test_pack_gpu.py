@@ -144,3 +144,10 @@ def test_parity_reference_gpu_binary(ug):
             pk.run()
             idx, _ = pk.accepted(0)
         assert list(idx) == r["idx"], r["command"]
+
+
+def test_round_sizes_stay_within_buffers(ug, oracle):
+    """Survivor-capacity steering never grows a round past its buffers
+    (T=200: the initial round is not a power of two of the cap)."""
+    u = ug.Universe(dim=3, T=200, zgrid=1, excl=1, seed=2, attempts=120000, round_size=16384)
+    _check(ug, oracle, u)

@@ -297,7 +297,7 @@ static void init_ctl(const ug_universe_cfg& c, const UniDev& d, UniCtl& k) {
     k.state = ST_ACTIVE;
     k.B_min = std::min(1024, d.B_max);
     k.B_cap = d.B_max;
-    k.round_B = std::min(std::max(4096, 2 * d.S_max), d.B_max);  // adapted every round
+    k.round_B = std::min(std::max(4096, 2 * d.S_max), d.B_max) / kTile * kTile;  // adapted every round
     k.accept_rate = c.accept_rate;
     k.sub_accept_rate = c.sub_accept_rate;
     k.win_target = c.accept_rate > 0 ? (int64_t)std::min(5e9, std::max(2e7, 30.0 / c.accept_rate)) : 0;

@@ -52,7 +52,8 @@ __global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* inf
             }
             if (c.state == ST_ACTIVE) {
                 const int64_t left = c.phase_end - c.next_cand;
-                B = (int)(left < (int64_t)c.round_B ? left : (int64_t)c.round_B);
+                const int cap = c.round_B < d.B_max ? c.round_B : d.B_max;  // per-round buffers hold B_max
+                B = (int)(left < (int64_t)cap ? left : (int64_t)cap);
             }
         }
         c.B = B;
@@ -729,9 +730,9 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
     // takes up to S_max, so steer toward the survivor capacity instead).
     // Admission results do not depend on it.
     if (c.S_raw > d.S_max && c.round_B > c.B_min)
-        c.round_B >>= 1;
+        c.round_B = max(c.round_B >> 1, c.B_min);
     else if (c.S_raw < d.S_max / 4 && c.round_B < c.B_cap)
-        c.round_B <<= 1;
+        c.round_B = min(c.round_B << 1, c.B_cap);
     // windowed accept-rate stop
     const double thr = c.phase == 1 ? c.accept_rate : c.sub_accept_rate;
     if (thr > 0 && c.win_target > 0 && used > 0) {
