@@ -146,8 +146,9 @@ def test_parity_reference_gpu_binary(ug):
         assert list(idx) == r["idx"], r["command"]
 
 
-def test_round_sizes_stay_within_buffers(ug, oracle):
+@pytest.mark.parametrize("precision", [0, 1])
+def test_round_sizes_stay_within_buffers(ug, oracle, precision):
     """Survivor-capacity steering never grows a round past its buffers
-    (T=200: the initial round is not a power of two of the cap)."""
-    u = ug.Universe(dim=3, T=200, zgrid=1, excl=1, seed=2, attempts=120000, round_size=16384)
-    _check(ug, oracle, u)
+    (T=200: the initial round size is not a power-of-two fraction of the cap)."""
+    u = ug.Universe(dim=2, T=200, zgrid=1, excl=1, seed=2, attempts=60000, round_size=16384)
+    _check(ug, oracle, u, precision=precision)
