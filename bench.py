@@ -289,6 +289,7 @@ def main() -> int:
     e2e = {"value": e2e_c / e2e_t, "unit": "candidates/s",
            "h2d_bytes_per_step": (h2d1 - h2d0) // nrep, "d2h_bytes_per_step": (d2h1 - d2h0) // nrep}
 
+    packer.close()
     # per-kernel timing pass (events around each launch on the packer's stream)
     timer = ugb200.Packer(us, precision=prec, device=local, stream=stream.cuda_stream,
                           rounds_per_sync=8, use_graph=False, kernel_timing=True)
@@ -326,7 +327,6 @@ def main() -> int:
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(us)
         print(json.dumps(line))
-    packer.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
