@@ -409,12 +409,12 @@ __device__ __forceinline__ int64_t lin_cell(const int* c, int dim, int gw) {
 
 // Head of the chain of accepted points in cell `lin` at timestep t (-1 none).
 __device__ __forceinline__ int32_t grid_head(const UniDev& U, int t, int64_t lin, int64_t cells_per_t) {
-    if (U.grid_kind == GRID_DENSE) return __ldcg(U.heads + UG_IDX((int64_t)t * cells_per_t + lin, U.dense_cells));
+    if (U.grid_kind == GRID_DENSE) return __ldg(U.heads + UG_IDX((int64_t)t * cells_per_t + lin, U.dense_cells));
     const uint64_t key = ((uint64_t)t << 40) | (uint64_t)lin;
     uint64_t h = mix64(key) & U.hmask;
     for (uint64_t probe = 0; probe <= U.hmask; probe++) {
-        const uint64_t k = __ldcg(U.hkeys + UG_IDX(h, U.hmask + 1));
-        if (k == key) return __ldcg(U.heads + UG_IDX(h, U.hmask + 1));
+        const uint64_t k = __ldg(U.hkeys + UG_IDX(h, U.hmask + 1));
+        if (k == key) return __ldg(U.heads + UG_IDX(h, U.hmask + 1));
         if (k == kEmptyKey) return -1;
         h = (h + 1) & U.hmask;
     }
@@ -495,7 +495,7 @@ __device__ __forceinline__ bool nbhd_occ1(const UniDev& U, int t, const Nbhd<D>&
         }
         if (dup) continue;
         const int64_t b = t0 + lin;
-        if ((__ldcg(base + UG_IDX(b >> 5, U.occ1_words)) >> (b & 31)) & 1u) return true;
+        if ((__ldg(base + UG_IDX(b >> 5, U.occ1_words)) >> (b & 31)) & 1u) return true;
     }
     return false;
 }
@@ -507,29 +507,52 @@ __device__ __forceinline__ bool nbhd_scan(const UniDev& U, int t, const Nbhd<D>&
                                           Visit&& visit) {
     const int gw = U.gw, sh = U.occ_shift, ogw = U.occ_gw;
     const int64_t tb = (int64_t)t * U.occ_per_t;
+    constexpr int L = D - 1;  // the last axis runs along the bitmap words
+    const int nl = nb.n[L];
 #pragma unroll
-    for (int i0 = 0; i0 < 4; i0++) {
-        if (i0 >= nb.n[0]) break;
-        const int x0 = nb.v[0][i0];
+    for (int i0 = 0; i0 < (D > 1 ? 4 : 1); i0++) {
+        if (D > 1 && i0 >= nb.n[0]) break;
 #pragma unroll
-        for (int i1 = 0; i1 < (D > 1 ? 4 : 1); i1++) {
-            if (D > 1 && i1 >= nb.n[D > 1 ? 1 : 0]) break;
-            const int x1 = D > 1 ? nb.v[D > 1 ? 1 : 0][i1] : 0;
+        for (int i1 = 0; i1 < (D > 2 ? 4 : 1); i1++) {
+            if (D > 2 && i1 >= nb.n[D > 2 ? 1 : 0]) break;
+            int64_t orow = 0, lrow = 0;  // row prefixes: bitmap (coarse) and grid (fine)
+            if (D > 1) {
+                const int x0 = nb.v[0][i0];
+                orow = x0 >> sh;
+                lrow = x0;
+            }
+            if (D > 2) {
+                const int x1 = nb.v[D > 2 ? 1 : 0][i1];
+                orow = orow * ogw + (x1 >> sh);
+                lrow = lrow * gw + x1;
+            }
+            const int64_t obase = tb + orow * ogw;
+            // the row's cells lie in the words of its first and last cell
+            const int64_t bf = obase + (nb.v[L][0] >> sh), bl = obase + (nb.last[L] >> sh);
+            const uint32_t wf = __ldg(U.occ + UG_IDX(bf >> 5, U.occ_words));
+            const uint32_t wl = (bl >> 5) == (bf >> 5) ? wf : __ldg(U.occ + UG_IDX(bl >> 5, U.occ_words));
+            uint32_t row_bits = 0;
 #pragma unroll
-            for (int i2 = 0; i2 < (D > 2 ? 4 : 1); i2++) {
-                if (D > 2 && i2 >= nb.n[D > 2 ? 2 : 0]) break;
-                const int x2 = D > 2 ? nb.v[D > 2 ? 2 : 0][i2] : 0;
-                int64_t ob = x0 >> sh, lin = x0;
-                if (D > 1) {
-                    ob = ob * ogw + (x1 >> sh);
-                    lin = lin * gw + x1;
-                }
-                if (D > 2) {
-                    ob = ob * ogw + (x2 >> sh);
-                    lin = lin * gw + x2;
-                }
-                ob += tb;
-                if (!((__ldcg(U.occ + UG_IDX(ob >> 5, U.occ_words)) >> (ob & 31)) & 1u)) continue;
+            for (int k = 0; k < 4; k++) {
+                if (k >= nl) break;
+                const int64_t bk = obase + (nb.v[L][k] >> sh);
+                uint32_t w;
+                if ((bk >> 5) == (bf >> 5))
+                    w = wf;
+                else if ((bk >> 5) == (bl >> 5))
+                    w = wl;
+                else
+                    w = __ldg(U.occ + UG_IDX(bk >> 5, U.occ_words));
+                row_bits |= ((w >> (bk & 31)) & 1u) << k;
+            }
+            while (row_bits) {
+                const int k = __ffs(row_bits) - 1;
+                row_bits &= row_bits - 1;
+                int xl = nb.v[L][0];
+#pragma unroll
+                for (int q = 1; q < 4; q++)
+                    if (q == k) xl = nb.v[L][q];
+                const int64_t lin = D > 1 ? lrow * gw + xl : (int64_t)xl;
                 int32_t p = grid_head(U, t, lin, cpt);
                 while (p >= 0) {
                     int32_t nx;
@@ -560,14 +583,14 @@ __device__ __forceinline__ bool contacts64_d(const UniDev& U, int t, const doubl
     if (!nbhd_occ1<D>(U, t, nb)) return false;
     return nbhd_scan<D>(U, t, nb, cpt, [&](int32_t p, int32_t& nx) -> bool {
         const Pt64* q = U.pts + UG_IDX((int64_t)p * U.T + t, U.slot_cap * U.T);
-        nx = __ldcg(&q->next);
+        nx = __ldg(&q->next);
         bool hit = true;
 #pragma unroll
         for (int ax = 0; ax < D; ax++)
-            hit = hit && hit1(torus_delta(P[ax] - __ldcg(&q->c[ax])), U.cell, U.inclusive);
+            hit = hit && hit1(torus_delta(P[ax] - __ldg(&q->c[ax])), U.cell, U.inclusive);
         if (!hit) return false;
         if (!group) return true;
-        const int32_t gq = __ldcg(&q->gid);
+        const int32_t gq = __ldg(&q->gid);
         if (*g == -1) {
             *g = gq;
             return false;

@@ -230,7 +230,12 @@ __device__ __forceinline__ int test32_d(const UniDev& d, int t, const float* X, 
     const float rin = r - m, rout = r + m;
     bool g = false;
     const bool deep = nbhd_scan<D>(d, t, nb, cpt, [&](int32_t p, int32_t& nx) -> bool {
-        const Pt32 q = d.ptf[UG_IDX((int64_t)p * d.T + t, d.slot_cap * d.T)];
+        const uint4 qr = __ldg(reinterpret_cast<const uint4*>(d.ptf) + UG_IDX((int64_t)p * d.T + t, d.slot_cap * d.T));
+        Pt32 q;
+        q.c[0] = __uint_as_float(qr.x);
+        q.c[1] = __uint_as_float(qr.y);
+        q.c[2] = __uint_as_float(qr.z);
+        q.next = (int32_t)qr.w;
         nx = q.next;
         bool miss = false, in = true;
 #pragma unroll
