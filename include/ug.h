@@ -145,6 +145,20 @@ int ug_batch_positions(void* h, int32_t u, double* pos, int64_t cap_paths);
 int ug_batch_params(void* h, int32_t u, double* a2, double* a, int32_t* b, double* f,
                     int64_t cap_paths);
 
+/* The same worldline parameters as ug_batch_params, produced without
+ * allocating any device memory: the regenerated parameters are staged in a
+ * fixed 16 MiB buffer that the library image reserves on every GPU that
+ * loads it, then copied to the caller's host buffers.  No counterpart in
+ * the reference.  For callers that must not allocate device memory at the
+ * time of the call -- code running while another thread captures a CUDA
+ * graph in global mode, or a serving loop that reserved its device memory
+ * at start-up.  Dumps needing more than 16 MiB (paths x dim x (8 + 20 nw)
+ * bytes) fail with UG_ECAP.  The first call on a device looks up the
+ * buffer's device address; make it before any stream capture.  All calls
+ * share the buffer: calls whose work overlaps on the GPU race. */
+int ug_batch_params_noalloc(void* h, int32_t u, double* a2, double* a, int32_t* b, double* f,
+                            int64_t cap_paths);
+
 /* Per-kernel device times (kernel_timing = 1). */
 int ug_batch_kernel_times(void* h, ug_kernel_times* out);
 

@@ -467,6 +467,26 @@ static bool all_done(const Batch& B) {
 
 }  // namespace ug
 
+// Internal accessor for ug_noalloc.cu: what a parameter dump of universe u
+// needs, without allocating anything.
+namespace ug {
+int batch_params_view(void* h, int u, const UniDev** dU, int64_t* n, int* dim, int* nw, int* dev,
+                      cudaStream_t* st) {
+    Batch* B = (Batch*)h;
+    if (!B || u < 0 || u >= B->n) return fail(UG_EINVAL, "bad arguments");
+    int rc = pull_ctl(*B);
+    if (rc) return rc;
+    *dU = B->dU;
+    *n = B->hCtl[u].n_slots;
+    *dim = B->U[u].d.dim;
+    *nw = B->U[u].d.nw;
+    *dev = B->dev;
+    *st = B->st;
+    return UG_OK;
+}
+int set_error(int code, const char* msg) { return fail(code, "%s", msg); }
+}  // namespace ug
+
 using namespace ug;
 
 extern "C" {

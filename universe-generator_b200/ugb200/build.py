@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(os.path.dirname(HERE), "csrc")
 LIB = os.path.join(HERE, "libug.so")
-SOURCES = ["ug_host.cu", "ug_kernels.cu", "ug_mixed.cu", "ug_frames.cu"]
+SOURCES = ["ug_host.cu", "ug_kernels.cu", "ug_mixed.cu", "ug_frames.cu", "ug_noalloc.cu"]
 FLAGS = [
     "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
     "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr",
