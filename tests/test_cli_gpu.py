@@ -1,0 +1,72 @@
+"""Drop-in executables end to end on the GPU: braid_knot against the reference
+binary's own dump (fixture), braid_cuda through braidlab.engine."""
+
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(ROOT, "universe-generator_b200", "bin")
+
+
+def _run(exe, args):
+    return subprocess.run([sys.executable, os.path.join(BIN, exe), *args], capture_output=True,
+                          text=True, timeout=600)
+
+
+def test_braid_knot_executable_reproduces_reference_dump(tmp_path, oracle):
+    gold = json.load(open(os.path.join(ROOT, "tests", "golden", "braid_knot_b200.json")))
+    r0 = gold["runs"][0]
+    dump = tmp_path / "k.csv"
+    args = ["-t", str(r0["T"]), "--dim", str(r0["dim"]), "--seed", str(r0["seed"]),
+            "--attempts", str(r0["attempts"]), "--dump", str(dump)]
+    r = _run("braid_knot", args)
+    assert r.returncode == 0, r.stderr
+    assert f"done: N={len(r0['idx'])} " in r.stderr
+    rows = oracle.parse_knot_dump(dump.read_text(), r0["dim"], r0["T"] - 1)
+    assert [x["idx"] for x in rows] == r0["idx"]
+    ref_rows = oracle.parse_knot_dump("\n".join(r0["head_rows"]), r0["dim"], r0["T"] - 1)
+    for a, b in zip(rows, ref_rows):
+        assert np.array_equal(a["b"], b["b"])
+        np.testing.assert_allclose(a["a"], b["a"], rtol=1e-14)
+        np.testing.assert_allclose(a["f"], b["f"], rtol=1e-14)
+
+
+def test_braid_cuda_through_braidlab_engine(tmp_path, oracle):
+    from braidlab.config import Job
+    from braidlab.engine import binary_name, build_command, parse_done
+    from ugb200.io import load_dump
+
+    job = Job(dim=2, t=16, seed=5, accept_rate=1e-9, max_attempts=30000.0)
+    curve = tmp_path / "c.csv"
+    cmd = build_command(job, binary_name(job.dim, job.terms), str(curve))
+    dump = tmp_path / "d.csv"
+    r = _run(cmd[0], cmd[1:] + ["--dump-params", str(dump)])
+    assert r.returncode == 0, r.stderr
+    n, att = parse_done(r.stderr)
+    ref = oracle.pack(oracle.Model(dim=2, T=16, terms=2, rng=oracle.RNG_KNOT, seed=5), 30000)
+    assert (n, att) == (len(ref.acc_idx), 30000)
+    lines = curve.read_text().splitlines()
+    assert lines[0] == "attempts,n" and lines[-1] == f"30000,{n}"
+    dim, a2, a, b, f, gid = load_dump(dump)
+    assert dim == 2 and a.shape == (n, 2, 1) and gid is None
+    c = oracle.candidate(oracle.Model(dim=2, T=16, terms=2, rng=oracle.RNG_KNOT, seed=5),
+                         int(ref.acc_idx[-1]))
+    np.testing.assert_allclose(a[-1], c["a"], rtol=1e-9)  # %.10g in the dump
+
+
+def test_braid_cuda_subpaths_curve_columns(tmp_path):
+    curve = tmp_path / "c.csv"
+    r = _run("braid_cuda", ["-t", "12", "--seed", "4", "--attempts", "3000", "--terms", "12",
+                            "--subpaths", "--sub-attempts", "20000", "--curve", str(curve)])
+    assert r.returncode == 0, r.stderr
+    lines = curve.read_text().splitlines()
+    assert lines[0] == "attempts,n,nsub,filled"
+    last = [int(v) for v in lines[-1].split(",")]
+    assert last[0] == 23000 and last[2] > 0 and last[3] > 0

@@ -1,0 +1,213 @@
+"""Engine-compatible command line: a drop-in for the reference packers.
+
+    python -m ugb200.cli [--engine braid_cuda|braid_cuda3d|braid_knot] <engine flags>
+
+or the executables in universe-generator_b200/bin/ named like the reference binaries
+(braidlab.engine.binary_name).  Accepted flags follow the engines' parsers
+(cuda/braid_cuda.cu:534-584, cuda/braid_cuda3d.cu:862-913, cuda/braid_knot.cu:258-289):
+the guard no-ops ``--uniform --torus --phase`` are accepted, ``--maxfreq`` must equal T
+(braid_cuda.cu:597-603), ``--smart`` is refused, and the outputs are the engines':
+curve CSV, ``--dump-params`` / ``--dump`` CSV and the stderr ``done: N=.. in .. attempts``
+line that braidlab.engine.parse_done reads.
+
+Additions: ``--rng knot|philox`` (default knot: the reference's deterministic per-attempt
+stream, cuda/braid_knot.cu:207), ``--zgrid ref|mid``, ``--excl ref|open``,
+``--precision mixed|fp64``, ``--dim`` (braid_knot), ``--round N``.
+Every failure exits 1 with a message, like the engines.
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+from . import _lib as L
+from .io import curve_rows, write_curve, write_dump, write_knot_dump
+from .packer import Packer, Universe
+
+UNSUPPORTED = {
+    "--euclid-collision": "the L2-ball exclusion is not built (Chebyshev only)",
+    "--angle-sample": "--angle-sample is not built",
+    "--diag": "--diag probes are not built",
+    "--probe-n": "--diag probes are not built",
+    "--sub-until-fill-rate": "--sub-until-fill-rate is not built",
+    "--nu-attempts": "the second (nu) species of braid_knot is not built",
+    "--nu-div": "the second (nu) species of braid_knot is not built",
+}
+
+
+def _die(msg: str) -> int:
+    print(f"error: {msg}", file=sys.stderr)
+    return 1
+
+
+def filled_cells(pos: np.ndarray, cell: float) -> np.ndarray:
+    """Occupied (timestep, cell) buckets after each admission, in admission
+    order (the fill measure of cuda/braid_cuda.cu:865-879)."""
+    n, dim, T = pos.shape
+    gw = int(round(2.0 / cell))
+    c = np.clip(np.floor((pos + 1.0) / cell).astype(np.int64), 0, gw - 1)
+    key = np.zeros((n, T), np.int64)
+    for k in range(dim):
+        key = key * gw + c[:, k, :]
+    key = key * T + np.arange(T)[None, :]
+    seen: set[int] = set()
+    out = np.zeros(n, np.int64)
+    for r in range(n):
+        seen.update(key[r].tolist())
+        out[r] = len(seen)
+    return out
+
+
+def main(argv: list[str] | None = None, engine: str | None = None) -> int:
+    argv = list(sys.argv[1:] if argv is None else argv)
+    if engine is None:
+        engine = "braid_cuda"
+        if "--engine" in argv:
+            i = argv.index("--engine")
+            engine = argv[i + 1]
+            del argv[i:i + 2]
+    base = engine.removesuffix("_w150")
+    if base not in ("braid_cuda", "braid_cuda3d", "braid_knot"):
+        return _die(f"unknown engine {engine}")
+    knot = base == "braid_knot"
+    # engine defaults (braid_cuda.cu:514-528, braid_knot.cu:255-257)
+    T, budget = (32, 1e10) if knot else (120, 1e8)
+    seed = 1 if knot else 12345
+    dim = 3 if base == "braid_cuda3d" else 2
+    terms = 0 if knot else 2
+    curve = dump = None
+    maxfreq = 0
+    accept = sub_accept = 0.0
+    pin = subpaths = False
+    sub_budget = 0.0
+    sub_terms = 0
+    max_n = 0
+    rng, zgrid, excl, prec = L.RNG_KNOT, L.ZGRID_REF, L.EXCL_REF, L.PREC_MIXED
+    round_size = 65536
+    i = 0
+    try:
+        while i < len(argv):
+            a = argv[i]
+
+            def val():
+                nonlocal i
+                i += 1
+                if i >= len(argv):
+                    raise ValueError(f"{a} needs a value")
+                return argv[i]
+
+            if a in ("-t", "--timesteps"):
+                T = int(val())
+            elif a == "--attempts":
+                budget = float(val())
+            elif a == "--seed":
+                seed = int(val())
+            elif a in ("--uniform", "--torus", "--phase", "--sparse"):
+                pass  # accepted guards; the grid kind is chosen by size
+            elif a == "--smart":
+                return _die("--smart was removed (frequencies are drawn uniformly)")
+            elif a == "--curve":
+                curve = val()
+            elif a == "--maxfreq":
+                maxfreq = int(val())
+            elif a == "--until-accept-rate":
+                accept = float(val())
+            elif a == "--terms":
+                terms = int(val())
+            elif a == "--pin-sin1":
+                pin = True
+            elif a == "--subpaths":
+                subpaths = True
+            elif a == "--sub-attempts":
+                sub_budget = float(val())
+            elif a == "--sub-until-accept-rate":
+                sub_accept = float(val())
+            elif a == "--sub-terms":
+                sub_terms = int(val())
+            elif a == "--max-n":
+                max_n = int(val())
+            elif a in ("--dump-params", "--dump"):
+                dump = val()
+            elif a == "--dim":
+                dim = int(val())
+            elif a == "--rng":
+                rng = {"knot": L.RNG_KNOT, "philox": L.RNG_PHILOX}[val()]
+            elif a == "--zgrid":
+                zgrid = {"ref": L.ZGRID_REF, "mid": L.ZGRID_MID}[val()]
+            elif a == "--excl":
+                excl = {"ref": L.EXCL_REF, "open": L.EXCL_OPEN}[val()]
+            elif a == "--precision":
+                prec = {"mixed": L.PREC_MIXED, "fp64": L.PREC_FP64}[val()]
+            elif a == "--round":
+                round_size = int(val())
+            elif a in UNSUPPORTED:
+                return _die(UNSUPPORTED[a])
+            else:
+                return _die(f"unknown flag {a}")
+            i += 1
+    except (ValueError, KeyError) as e:
+        return _die(str(e))
+    if maxfreq not in (0, T):
+        return _die(f"--maxfreq {maxfreq}: the max frequency is T={T} (the full Nyquist band)")
+    if terms == 0:
+        terms = T
+    if terms < 2:
+        terms = 2
+    if sub_terms and sub_terms != terms:
+        return _die("--sub-terms different from --terms is not built")
+    if subpaths and dim != 2:
+        return _die("subpaths is a 2+1 engine feature")
+    u = Universe(dim=dim, T=T, terms=0 if terms == T else terms, rng=rng, zgrid=zgrid,
+                 excl=excl, pin_sin1=int(pin), group_mode=L.GROUP_SUBPATH if subpaths else 0,
+                 round_size=round_size, seed=seed, attempts=int(budget), max_n=max_n,
+                 sub_attempts=int(sub_budget), accept_rate=accept, sub_accept_rate=sub_accept)
+    kind = {2: "2+1", 3: "3+1", 1: "1+1"}[dim]
+    print(f"{kind} (torus, phase): T={T}  modmax={max(T - 1, 2)} (maxfreq={max(T - 1, 2) + 1})  "
+          f"terms={terms}  rng={'knot' if rng == L.RNG_KNOT else 'philox'}", file=sys.stderr)
+    try:
+        p = Packer([u], precision=prec)
+        p.run()
+        st = p.stats(0)
+        idx, gid = p.accepted(0)
+        params = p.params(0) if dump else None
+        pos = p.positions(0) if (subpaths and curve) else None
+        p.close()
+    except L.UgError as e:
+        return _die(str(e))
+    if knot:
+        print(f"done: N={st.n} (primary {st.n}, nu 0) in {st.attempts} attempts", file=sys.stderr)
+    else:
+        print(f"done: N={st.n_unique} in {st.phase1_end} attempts", file=sys.stderr)
+        if subpaths:
+            print(f"sub done: Nsub={st.n_sub} in {st.attempts - st.phase1_end} attempts",
+                  file=sys.stderr)
+    if curve:
+        if knot:
+            with open(curve, "w") as f:
+                f.write("attempt,n,species\n")
+                for k, ix in enumerate(idx):
+                    f.write(f"{int(ix) + 1},{k + 1},0\n")
+        else:
+            uniq = (gid == np.arange(len(gid))) if subpaths else None
+            filled = filled_cells(pos, 2.0 / T if excl == L.EXCL_REF else 1.0 / T) if subpaths else None
+            write_curve(curve, curve_rows(idx, st.attempts, n_unique_mask=uniq, filled=filled),
+                        subpaths=subpaths)
+    if dump:
+        if knot:
+            write_knot_dump(dump, dim, T, idx, params["a2"], params["a"], params["b"], params["f"])
+        else:
+            write_dump(dump, dim, params["a2"], params["a"], params["b"], params["f"],
+                       gid=gid if subpaths else None)
+        print(f"dump-params: wrote {len(idx)} worldlines to {dump}", file=sys.stderr)
+    return 0
+
+
+def entry() -> None:
+    sys.exit(main(engine=os.path.basename(sys.argv[0]) if not sys.argv[0].endswith(".py") else None))
+
+
+if __name__ == "__main__":
+    sys.exit(main())
