@@ -179,6 +179,48 @@ int ug_batch_mixed_error(void* h, int32_t u, int64_t first, int64_t count, doubl
 /* Release all device memory of the batch. */
 int ug_batch_destroy(void* h);
 
+/* ---- frames: past-light-cone images of a packing (cuda/frame_bake.cu) */
+
+/* One image of a worldline on the front (the BRF1 hit record, frame_bake.cu:31-40). */
+typedef struct ug_hit {
+    uint32_t src;  /* source path (dump row) */
+    float dx, dy;  /* offset from the pulse centre (torus image included) */
+    float chi;     /* front radius at emission */
+    float z_emit;  /* conformal time of emission */
+} ug_hit;
+
+/* frame_bake's flags (frame_bake.cu:431-470). */
+typedef struct ug_frames_cfg {
+    int32_t front;         /* 0 speed, 1 fit, 2 budget */
+    int32_t cheb;          /* 1 square (Chebyshev) metric, 0 circle; budget forces 1 */
+    int32_t n_frames;      /* instants z_obs spread over [from, to] */
+    int32_t wraps;         /* torus image cap K; -1 = ceil((chi_max + 4) / 2) */
+    double from_pi, to_pi; /* z_obs range, units of pi */
+    double zmin_pi;        /* rewind floor, units of pi */
+    double speed;          /* conformal front speed (front 0) */
+    int32_t n_obs;
+    int32_t density_bins;  /* > 0: histogram hit offsets into bins x bins per (frame, observer) */
+    const int32_t* obs_type; /* [n_obs] 0 path observer, 1 comoving point */
+    const int32_t* obs_path; /* [n_obs] path index (type 0) */
+    const double* obs_xy;    /* [n_obs][2] point (type 1) */
+} ug_frames_cfg;
+
+typedef struct ug_frames_out {
+    ug_hit* hits;        /* all hits, (frame, observer)-major, each group sorted by (chi, src) */
+    int64_t hit_cap;
+    int64_t* hit_count;  /* [n_frames][n_obs] */
+    double* frame_meta;  /* [n_frames][3]: z_obs, chi_max, K */
+    double* obs_meta;    /* [n_frames][n_obs][4]: ox, oy, beta_x, beta_y */
+    uint32_t* density;   /* [n_frames][n_obs][bins][bins] over [-chi_max, chi_max]^2, or NULL */
+    int64_t hits_total;  /* out: hits found (also when hit_cap is too small) */
+} ug_frames_out;
+
+/* Bake frames of a 2+1 packing given as dump arrays: a2 [n][2], a/b/f
+ * [n][2][nw] (the frame_bake driver, frame_bake.cu:398-635: load_dump,
+ * grid_kernel, hits_kernel, BRF1 writer; plus the density scatter). */
+int ug_frame_bake(const ug_frames_cfg* cfg, int32_t n, int32_t nw, const double* a2, const double* a,
+                  const double* b, const double* f, ug_frames_out* out);
+
 /* ---- single-universe convenience: a batch of one (the ug_pack_* surface) */
 int ug_pack_create(const ug_universe_cfg* cfg, const ug_run_opts* opts, void** out);
 int ug_pack_run(void* h);

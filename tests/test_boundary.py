@@ -150,3 +150,44 @@ def test_curve_rows_are_exact_milestones():
     ms = milestones(6000)
     assert [r[0] for r in rows] == ms + [6000]
     assert rows[0] == (1000, 4) and rows[-1] == (6000, 7)
+
+
+def test_brf1_writer_matches_reference_reader(tmp_path):
+    """A BRF1 file from ugb200.frames.write_brf1 reads back through the reference's
+    own braidlab.frames.load_frames (subprocess; the packages share a name)."""
+    from ugb200.frames import HIT_DTYPE, Baked, write_brf1
+
+    rng = np.random.default_rng(1)
+    hits = []
+    for fi in range(2):
+        row = []
+        for o in range(2):
+            h = np.zeros(5 + fi + o, HIT_DTYPE)
+            h["src"] = rng.integers(0, 9, len(h)); h["dx"] = rng.normal(size=len(h))
+            h["dy"] = rng.normal(size=len(h)); h["chi"] = rng.uniform(0, 1, len(h))
+            h["z_emit"] = rng.uniform(0.1, 1, len(h))
+            row.append(h)
+        hits.append(row)
+    bk = Baked("fit", True, 0.33, 0.0628, -1, [(0, 3, 0.0, 0.0), (1, -1, 0.1, 0.2)],
+               np.array([[1.0, 0.9, 3], [1.2, 1.1, 3]]), rng.normal(size=(2, 2, 4)), hits, None, 9)
+    p = tmp_path / "f.frames"
+    write_brf1(p, bk)
+    from braidlab.frames import load_frames
+    ours = load_frames(p)
+    assert ours.n_paths == 9 and ours.observers[1] == (1, -1, 0.1, 0.2)
+    if not os.path.isdir(os.path.join(REF, "braidlab")):
+        return
+    code = ("import sys, json; sys.path.insert(0, sys.argv[1]);"
+            "from braidlab.frames import load_frames; fs = load_frames(sys.argv[2]);"
+            "print(json.dumps([fs.n_paths, fs.front, fs.cheb, [list(o) for o in fs.observers],"
+            "[[[fr.z_obs, fr.chi_max, fr.wraps, fr.ox, fr.oy, fr.beta.tolist(), fr.hits['chi'].tolist(), fr.hits['src'].tolist()]"
+            " for fr in row] for row in fs.frames]]))")
+    r = subprocess.run([sys.executable, "-c", code, REF, str(p)], capture_output=True, text=True,
+                       check=True)
+    ref = json.loads(r.stdout)
+    assert ref[0] == 9 and ref[1] == "fit" and ref[2] is True
+    for fi, row in enumerate(ref[4]):
+        for o, fr in enumerate(row):
+            mine = ours.frames[fi][o]
+            assert fr[0] == mine.z_obs and fr[2] == mine.wraps
+            assert fr[6] == mine.hits["chi"].tolist() and fr[7] == mine.hits["src"].tolist()

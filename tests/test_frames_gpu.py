@@ -1,0 +1,96 @@
+"""frame_bake on the GPU against the reference's own Python baker (golden hits),
+plus the reference test's properties, the BRF1 round trip and the density scatter."""
+
+import io
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "frames_reference.json")
+TOL = 2e-5  # float32 hit records; positions agree to ~1e-13 in FP64
+
+
+def _arrays(text):
+    import tempfile
+
+    from ugb200.io import load_dump
+    with tempfile.NamedTemporaryFile("w", suffix=".csv", delete=False) as fh:
+        fh.write(text)
+        p = fh.name
+    dim, a2, a, b, f, _ = load_dump(p)
+    os.remove(p)
+    return a2, a, b, f
+
+
+def _bake_case(ug, c, dumps, **kw):
+    from ugb200.frames import bake
+    a2, a, b, f = _arrays(dumps[c["dump"]])
+    obs = [tuple(c["obs"])]
+    return bake(a2, a, b, f, observers=obs, from_pi=c["z_obs_pi"], to_pi=c["z_obs_pi"], frames=1,
+                zmin_pi=c["z_min_pi"], front=c["front"], metric="square" if c["cheb"] else "circle",
+                speed=c["speed"], wraps=-1 if c["wraps"] is None else c["wraps"], **kw)
+
+
+def test_hits_match_reference_baker(ug):
+    gold = json.load(open(GOLD))
+    for k, c in enumerate(gold["cases"]):
+        bk = _bake_case(ug, c, gold["dumps"])
+        got = bk.hits[0][0]
+        ref = np.array(c["hits"], dtype=float).reshape(-1, 5)
+        assert len(got) == len(ref), (k, len(got), len(ref))
+        if not len(ref):
+            continue
+        ref = ref[np.lexsort((ref[:, 0], ref[:, 3]))]
+        gg = np.stack([got["src"].astype(float), got["dx"], got["dy"], got["chi"], got["z_emit"]], 1)
+        gg = gg[np.lexsort((gg[:, 0], gg[:, 3]))]
+        assert np.array_equal(gg[:, 0], ref[:, 0]), k
+        np.testing.assert_allclose(gg[:, 1:], ref[:, 1:], atol=TOL, rtol=0)
+
+
+def test_reference_properties_on_packed_dump(ug):
+    """Hits sit on the front, emit times lie in the rewind window (tests/test_frames.py:34-45)."""
+    gold = json.load(open(GOLD))
+    a2, a, b, f = _arrays(gold["dumps"]["packed"])
+    from ugb200.frames import bake
+    for front in ("fit", "budget", "speed"):
+        bk = bake(a2, a, b, f, observers=[("path", 0), ("point", 0.2, -0.1)], from_pi=0.3,
+                  to_pi=0.7, frames=3, zmin_pi=0.02, front=front)
+        for fi in range(3):
+            z_obs = bk.frame_meta[fi, 0]
+            for o in range(2):
+                h = bk.hits[fi][o]
+                assert len(h) > 0
+                assert np.all(h["src"] < len(a2))
+                assert np.all(h["z_emit"] <= z_obs + 1e-5) and np.all(h["z_emit"] >= 0.02 * math.pi - 1e-5)
+                r = np.maximum(np.abs(h["dx"]), np.abs(h["dy"]))
+                np.testing.assert_allclose(r, h["chi"], atol=1e-5)
+
+
+def test_brf1_round_trip_and_density(ug, tmp_path):
+    from braidlab.frames import load_frames
+    from ugb200.frames import bake, write_brf1
+    gold = json.load(open(GOLD))
+    a2, a, b, f = _arrays(gold["dumps"]["packed"])
+    bins = 64
+    bk = bake(a2, a, b, f, observers=[("path", 2)], from_pi=0.3, to_pi=0.7, frames=4,
+              zmin_pi=0.02, front="fit", density_bins=bins)
+    p = tmp_path / "x.frames"
+    write_brf1(p, bk)
+    fs = load_frames(p)
+    assert fs.n_paths == len(a2) and fs.front == "fit" and len(fs.frames) == 4
+    for fi in range(4):
+        fr = fs.frames[fi][0]
+        assert np.array_equal(fr.hits, np.sort(bk.hits[fi][0], order=["chi", "src"]))
+        chi_max = bk.frame_meta[fi, 1]
+        h = bk.hits[fi][0]
+        cx = np.floor((h["dx"].astype(np.float32) + np.float32(chi_max)) * np.float32(bins / (2 * chi_max)))
+        cy = np.floor((h["dy"].astype(np.float32) + np.float32(chi_max)) * np.float32(bins / (2 * chi_max)))
+        ok = (cx >= 0) & (cy >= 0) & (cx < bins) & (cy < bins)
+        ref = np.zeros((bins, bins), np.uint32)
+        np.add.at(ref, (cy[ok].astype(int), cx[ok].astype(int)), 1)
+        assert np.array_equal(bk.density[fi, 0], ref)

@@ -1,0 +1,85 @@
+"""Reader of baked .frames files (reference braidlab/frames.py:88-144).
+
+The BRF1 layout (cuda/frame_bake.cu:29-38):
+  header : b"BRF1", u32 n_paths, u32 n_observers, u32 n_instants, u32 front,
+           u32 cheb, f64 speed, f64 z_min, i32 wraps
+  observers: u32 type, i32 path_idx, f64 px, f64 py
+  per instant: f64 z_obs, f64 chi_max, i32 K, then per observer
+           f64 ox, f64 oy, f64 beta_x, f64 beta_y, u64 n_hits, n_hits x
+           (u32 src, f32 dx, f32 dy, f32 chi, f32 z_emit)
+"""
+
+from __future__ import annotations
+
+import struct
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+BETA_CAP = 0.995
+FRAME_GRID = 420
+FRAME_BISECT = 24
+BUDGET_GRID_CAP = 4000
+HIT_DTYPE = np.dtype([("src", "<u4"), ("dx", "<f4"), ("dy", "<f4"), ("chi", "<f4"),
+                      ("z_emit", "<f4")])
+_FRONTS = ("speed", "fit", "budget")
+
+
+@dataclass(frozen=True)
+class ObserverFrame:
+    z_obs: float
+    chi_max: float
+    wraps: int
+    ox: float
+    oy: float
+    beta: np.ndarray
+    hits: np.ndarray
+
+    @property
+    def redshift(self) -> np.ndarray:
+        """Cosmological 1+Z per hit: sin(z_obs) / sin(z_emit)."""
+        return np.sin(self.z_obs) / np.sin(self.hits["z_emit"].astype(np.float64))
+
+
+@dataclass(frozen=True)
+class FrameSet:
+    n_paths: int
+    front: str
+    cheb: bool
+    speed: float
+    z_min: float
+    observers: list
+    frames: list
+
+
+def load_frames(path: str | Path) -> FrameSet:
+    """Read a .frames file; hits of each frame sorted by (chi, src)."""
+    raw = Path(path).read_bytes()
+    if raw[:4] != b"BRF1":
+        raise ValueError(f"{path}: not a BRF1 frames file")
+    n_paths, n_obs, n_inst, front, cheb = struct.unpack_from("<5I", raw, 4)
+    speed, z_min = struct.unpack_from("<2d", raw, 24)
+    off = 44
+    observers = []
+    for _ in range(n_obs):
+        typ, pidx = struct.unpack_from("<Ii", raw, off)
+        px, py = struct.unpack_from("<2d", raw, off + 8)
+        observers.append((typ, pidx, px, py))
+        off += 24
+    frames = []
+    for _ in range(n_inst):
+        z_obs, chi_max = struct.unpack_from("<2d", raw, off)
+        (k,) = struct.unpack_from("<i", raw, off + 16)
+        off += 20
+        row = []
+        for _o in range(n_obs):
+            ox, oy, bx, by = struct.unpack_from("<4d", raw, off)
+            (nh,) = struct.unpack_from("<Q", raw, off + 32)
+            off += 40
+            hits = np.frombuffer(raw, dtype=HIT_DTYPE, count=nh, offset=off)
+            off += nh * HIT_DTYPE.itemsize
+            row.append(ObserverFrame(z_obs, chi_max, k, ox, oy, np.array([bx, by]),
+                                     np.sort(hits, order=["chi", "src"])))
+        frames.append(row)
+    return FrameSet(n_paths, _FRONTS[front], bool(cheb), speed, z_min, observers, frames)

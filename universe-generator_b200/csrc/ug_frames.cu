@@ -1,0 +1,404 @@
+// ug_frames.cu -- past-light-cone frame baking of a packed universe (2+1).
+//
+// For each instant z_obs and observer, the pulse centre is frozen at the
+// observer's comoving position and the universe is rewound while a front
+// expands (cuda/frame_bake.cu:1-40): front "speed" (conformal, speed c),
+// "fit" (c = -1/eta(z_min)) or "budget" (wiggle-budget reach).  Every torus
+// image (2nx, 2ny), |n| <= K, of every worldline is walked along the rewind
+// grid for sign changes of dist(pos + shift - centre) - chi_front and each
+// crossing is refined by 24 bisection steps with fresh evaluations
+// (frame_bake.cu:281-371).  Hits are (src, dx, dy, chi, z_emit); optionally
+// they are histogrammed into a bins x bins uint32 density grid per frame over
+// [-chi_max, chi_max]^2 (no reference counterpart; the reference draws
+// scatter plots, plots/render_frames.py:47-110).
+//
+// Evaluation: X(z) = [a2 sin z + sum_j a_j (sin(b_j z + f_j) - sin f_j)] / sin z
+// (frame_bake.cu:201-212).  Full-band dumps evaluate sum_j a_j sin(b_j z + f_j)
+// as Im P(e^{iz}) with P(w) = sum_b (a_b e^{i f_b}) w^b by complex Horner --
+// one sincos per evaluation instead of one per term; few-term dumps sum the
+// terms directly.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ug.h"
+
+namespace ug {
+
+int set_error(int code, const char* msg);
+
+namespace {
+
+constexpr int kGridRows = 420;     // rewind grid (frame_bake.cu:71)
+constexpr int kBisect = 24;        // bisection steps (frame_bake.cu:72)
+constexpr int kBudgetCap = 4000;   // budget rewind-grid cap (frame_bake.cu:73)
+constexpr double kPiF = 3.14159265358979323846;
+
+struct FPaths {
+    int n, nw, bmax;
+    int horner;            // 1: complex Horner over b = 0..bmax; 0: per-term sums
+    const double* a2;      // [n][2]
+    const double* s0;      // [n][2]  sum_j a_j sin f_j
+    const double* a;       // [n][2][nw]
+    const double* b;       // [n][2][nw]
+    const double* f;       // [n][2][nw]
+    const double2* coef;   // [n][2][bmax+1] a_b e^{i f_b} (Horner form)
+};
+
+struct FFront {
+    int budget, cheb, M, bMax;
+    double spd, zObs, etaObs, chiMax;
+};
+
+__host__ __device__ inline double wiggle_direct(const double* a, const double* b, const double* f, int nw,
+                                                double z) {
+    double s = 0.0;
+    for (int j = 0; j < nw; j++) s += a[j] * sin(b[j] * z + f[j]);
+    return s;
+}
+
+__device__ inline double wiggle_horner(const double2* c, int bmax, double z) {
+    double sz, cz;
+    sincos(z, &sz, &cz);
+    double pr = c[bmax].x, pi = c[bmax].y;
+    for (int k = bmax - 1; k >= 0; k--) {
+        const double nr = fma(pr, cz, fma(-pi, sz, c[k].x));
+        const double ni = fma(pr, sz, fma(pi, cz, c[k].y));
+        pr = nr;
+        pi = ni;
+    }
+    return pi;
+}
+
+__device__ inline void comov(const FPaths& P, int p, double z, double* X, double* Y) {
+    const double s = sin(z);
+    double w[2];
+    for (int ax = 0; ax < 2; ax++) {
+        const size_t o = ((size_t)p * 2 + ax);
+        w[ax] = P.horner ? wiggle_horner(P.coef + o * (P.bmax + 1), P.bmax, z)
+                         : wiggle_direct(P.a + o * P.nw, P.b + o * P.nw, P.f + o * P.nw, P.nw, z);
+    }
+    *X = (P.a2[(size_t)p * 2] * s + w[0] - P.s0[(size_t)p * 2]) / s;
+    *Y = (P.a2[(size_t)p * 2 + 1] * s + w[1] - P.s0[(size_t)p * 2 + 1]) / s;
+}
+
+// Wiggle-budget reach of the front (frame_bake.cu:236-251).
+__host__ __device__ inline double reach_of(double z, double zObs, int bMax) {
+    const double s = sin(z), sObs = sin(zObs);
+    double best = 0.0;
+    for (int b = 2; b <= bMax; b++) {
+        const double da = (cos(b * z) - 1.0) / (b * s) - (cos(b * zObs) - 1.0) / (b * sObs);
+        const double db = sin(b * z) / (b * s) - sin(b * zObs) / (b * sObs);
+        const double d = (b % 2 == 0) ? sqrt(da * da + db * db) : fabs(db);
+        best = d > best ? d : best;
+    }
+    return best;
+}
+
+__device__ inline double metric(double dx, double dy, int cheb) {
+    return cheb ? fmax(fabs(dx), fabs(dy)) : sqrt(dx * dx + dy * dy);
+}
+
+__global__ void k_fb_grid(FPaths P, int M, const double* zg, double* px, double* py) {
+    const int64_t total = (int64_t)P.n * (M + 1);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int p = (int)(i / (M + 1)), r = (int)(i % (M + 1));
+        comov(P, p, zg[r], &px[i], &py[i]);
+    }
+}
+
+// One thread per (path, torus image): the crossing finder.
+__global__ void k_fb_hits(FPaths P, FFront F, double ox, double oy, int K, int obsIdx, const double* zg,
+                          const double* chig, const double* px, const double* py, ug_hit* hits,
+                          unsigned long long* count, unsigned long long cap) {
+    const int side = 2 * K + 1;
+    const int64_t total = (int64_t)P.n * side * side;
+    for (int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; tid < total;
+         tid += (int64_t)gridDim.x * blockDim.x) {
+        const int p = (int)(tid / (side * side));
+        const int sh = (int)(tid % (side * side));
+        const int nx = sh % side - K, ny = sh / side - K;
+        const double bx = 2.0 * nx - ox, by = 2.0 * ny - oy;
+        // rows the front cannot reach for this image (comoving coords stay within +-2)
+        const double dmin = fmax(0.0, 2.0 * fmax(fabs((double)nx), fabs((double)ny)) - 4.0);
+        if (dmin >= F.chiMax) continue;
+        const int i0 = F.budget ? 1 : max(1, (int)ceil(dmin * F.M / F.chiMax));
+        if (i0 > F.M) continue;
+        const int64_t row = (int64_t)p * (F.M + 1);
+        double prev = metric(px[row + i0 - 1] + bx, py[row + i0 - 1] + by, F.cheb) - chig[i0 - 1];
+        // the observer sits on the front at chi = 0: keep its own image inside
+        if (p == obsIdx && nx == 0 && ny == 0 && i0 == 1 && fabs(prev) < 1e-9)
+            prev = -1e-12;
+        else if (prev == 0.0)
+            prev = 1e-12;
+        for (int i = i0; i <= F.M; i++) {
+            const double g = metric(px[row + i] + bx, py[row + i] + by, F.cheb) - chig[i];
+            if ((prev < 0.0) != (g < 0.0)) {
+                const bool inside = prev < 0.0;
+                double chi, zEmit, qx, qy;
+                if (F.budget) {
+                    double lo = zg[i - 1], hi = zg[i];
+                    for (int it = 0; it < kBisect; it++) {
+                        const double mid = (lo + hi) / 2.0;
+                        comov(P, p, mid, &qx, &qy);
+                        const double gm = metric(qx + bx, qy + by, F.cheb) - reach_of(mid, F.zObs, F.bMax);
+                        if ((gm < 0.0) == inside)
+                            lo = mid;
+                        else
+                            hi = mid;
+                    }
+                    zEmit = (lo + hi) / 2.0;
+                    chi = reach_of(zEmit, F.zObs, F.bMax);
+                } else {
+                    double lo = chig[i - 1], hi = chig[i];
+                    for (int it = 0; it < kBisect; it++) {
+                        const double mid = (lo + hi) / 2.0;
+                        comov(P, p, 2.0 * atan(exp(F.etaObs - mid / F.spd)), &qx, &qy);
+                        const double gm = metric(qx + bx, qy + by, F.cheb) - mid;
+                        if ((gm < 0.0) == inside)
+                            lo = mid;
+                        else
+                            hi = mid;
+                    }
+                    chi = (lo + hi) / 2.0;
+                    zEmit = 2.0 * atan(exp(F.etaObs - chi / F.spd));
+                }
+                comov(P, p, zEmit, &qx, &qy);
+                const unsigned long long slot = atomicAdd(count, 1ull);
+                if (slot < cap) {
+                    ug_hit h;
+                    h.src = (uint32_t)p;
+                    h.dx = (float)(qx + bx);
+                    h.dy = (float)(qy + by);
+                    h.chi = (float)chi;
+                    h.z_emit = (float)zEmit;
+                    hits[slot] = h;
+                }
+            }
+            prev = g;
+        }
+    }
+}
+
+// Density scatter: hit offsets binned over [-chi_max, chi_max]^2.
+__global__ void k_fb_density(const ug_hit* hits, int64_t n, double chiMax, int bins, uint32_t* grid) {
+    const float inv = (float)(bins / (2.0 * chiMax));
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const ug_hit h = hits[i];
+        int cx = (int)floorf((h.dx + (float)chiMax) * inv);
+        int cy = (int)floorf((h.dy + (float)chiMax) * inv);
+        if (cx < 0 || cy < 0 || cx >= bins || cy >= bins) continue;
+        atomicAdd(&grid[(size_t)cy * bins + cx], 1u);
+    }
+}
+
+double h_eta(double z) { return log(tan(z / 2.0)); }
+
+// Host comoving position and velocity of a path (frame_bake.cu:201-228).
+void h_comov(const std::vector<double>& a2, const std::vector<double>& a, const std::vector<double>& b,
+             const std::vector<double>& f, int nw, int p, double z, double* X, double* Y, double* VX,
+             double* VY) {
+    const double s = sin(z), c = cos(z);
+    double xx[2], dd[2];
+    for (int ax = 0; ax < 2; ax++) {
+        xx[ax] = a2[(size_t)p * 2 + ax] * s;
+        dd[ax] = a2[(size_t)p * 2 + ax] * c;
+        for (int j = 0; j < nw; j++) {
+            const size_t o = ((size_t)p * 2 + ax) * nw + j;
+            xx[ax] += a[o] * (sin(b[o] * z + f[o]) - sin(f[o]));
+            dd[ax] += a[o] * b[o] * cos(b[o] * z + f[o]);
+        }
+    }
+    *X = xx[0] / s;
+    *Y = xx[1] / s;
+    *VX = (dd[0] * s - xx[0] * c) / (s * s);
+    *VY = (dd[1] * s - xx[1] * c) / (s * s);
+}
+
+struct DevBuf {
+    std::vector<void*> p;
+    ~DevBuf() {
+        for (void* q : p) cudaFree(q);
+    }
+    template <class T>
+    T* get(size_t n) {
+        void* q = nullptr;
+        if (cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return nullptr;
+        p.push_back(q);
+        return (T*)q;
+    }
+};
+
+}  // namespace
+}  // namespace ug
+
+using namespace ug;
+
+extern "C" int ug_frame_bake(const ug_frames_cfg* cfg, int32_t n, int32_t nw, const double* a2,
+                             const double* a, const double* b, const double* f, ug_frames_out* out) {
+    if (!cfg || !out || n < 1 || nw < 1 || !a2 || !a || !b || !f)
+        return set_error(UG_EINVAL, "frame_bake: bad arguments");
+    if (cfg->front < 0 || cfg->front > 2) return set_error(UG_EINVAL, "--front must be speed|fit|budget");
+    if (cfg->n_frames < 1 || cfg->n_obs < 1) return set_error(UG_EINVAL, "need >= 1 frame and observer");
+    for (int o = 0; o < cfg->n_obs; o++)
+        if (cfg->obs_type[o] == 0 && (cfg->obs_path[o] < 0 || cfg->obs_path[o] >= n))
+            return set_error(UG_EINVAL, "observer path out of range");
+    std::vector<double> A2(a2, a2 + (size_t)n * 2), A(a, a + (size_t)n * 2 * nw), Bv(b, b + (size_t)n * 2 * nw),
+        Fv(f, f + (size_t)n * 2 * nw);
+    int bMax = 2;
+    for (double x : Bv) bMax = std::max(bMax, (int)x);
+    // Horner when the band is dense enough that one polynomial beats nw sines
+    const int horner = (bMax <= 4 * nw) ? 1 : 0;
+    std::vector<double> s0((size_t)n * 2, 0.0);
+    std::vector<double2> coef;
+    if (horner) coef.assign((size_t)n * 2 * (bMax + 1), make_double2(0.0, 0.0));
+    for (int p = 0; p < n; p++)
+        for (int ax = 0; ax < 2; ax++)
+            for (int j = 0; j < nw; j++) {
+                const size_t o = ((size_t)p * 2 + ax) * nw + j;
+                s0[(size_t)p * 2 + ax] += A[o] * sin(Fv[o]);
+                if (horner) {
+                    double2& c = coef[((size_t)p * 2 + ax) * (bMax + 1) + (int)Bv[o]];
+                    c.x += A[o] * cos(Fv[o]);
+                    c.y += A[o] * sin(Fv[o]);
+                }
+            }
+    DevBuf buf;
+    double* dA2 = buf.get<double>(A2.size());
+    double* dS0 = buf.get<double>(s0.size());
+    double* dA = buf.get<double>(A.size());
+    double* dB = buf.get<double>(Bv.size());
+    double* dF = buf.get<double>(Fv.size());
+    double2* dC = buf.get<double2>(std::max<size_t>(coef.size(), 1));
+    const int Mmax = std::min(kBudgetCap, std::max(kGridRows, 2 * bMax));
+    double* dZg = buf.get<double>(Mmax + 1);
+    double* dChig = buf.get<double>(Mmax + 1);
+    double* dPx = buf.get<double>((size_t)n * (Mmax + 1));
+    double* dPy = buf.get<double>((size_t)n * (Mmax + 1));
+    const bool want_density = cfg->density_bins > 0 && out->density;
+    const size_t bins2 = want_density ? (size_t)cfg->density_bins * cfg->density_bins : 0;
+    uint32_t* dDen = want_density ? buf.get<uint32_t>(bins2) : nullptr;
+    const unsigned long long hitCap = 1ull << 24;  // per (frame, observer) launch, frame_bake.cu:515
+    ug_hit* dHits = buf.get<ug_hit>(hitCap);
+    unsigned long long* dCount = buf.get<unsigned long long>(1);
+    if (!dA2 || !dS0 || !dA || !dB || !dF || !dC || !dZg || !dChig || !dPx || !dPy || !dHits || !dCount ||
+        (want_density && !dDen))
+        return set_error(UG_ENOMEM, "frame_bake: device allocation failed");
+    cudaMemcpy(dA2, A2.data(), A2.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(dS0, s0.data(), s0.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(dA, A.data(), A.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(dB, Bv.data(), Bv.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(dF, Fv.data(), Fv.size() * 8, cudaMemcpyHostToDevice);
+    if (horner) cudaMemcpy(dC, coef.data(), coef.size() * sizeof(double2), cudaMemcpyHostToDevice);
+    FPaths P{n, nw, bMax, horner, dA2, dS0, dA, dB, dF, dC};
+    const double zMin = std::max(2e-3, cfg->zmin_pi * kPiF);
+    int64_t written = 0;
+    out->hits_total = 0;
+    std::vector<ug_hit> hh;
+    for (int fi = 0; fi < cfg->n_frames; fi++) {
+        const double frac = cfg->n_frames == 1 ? 0.0 : (double)fi / (cfg->n_frames - 1);
+        const double zObs = std::min((cfg->from_pi + (cfg->to_pi - cfg->from_pi) * frac) * kPiF, kPiF - 1e-3);
+        if (zMin >= zObs) return set_error(UG_EINVAL, "rewind floor >= z_obs");
+        FFront F{};
+        F.budget = cfg->front == 2;
+        F.cheb = F.budget || cfg->cheb;
+        F.zObs = zObs;
+        F.etaObs = h_eta(zObs);
+        F.spd = cfg->front == 0 ? std::max(1e-3, cfg->speed) : -1.0 / h_eta(zMin);
+        F.bMax = bMax;
+        F.M = F.budget ? std::min(kBudgetCap, std::max(kGridRows, 2 * bMax)) : kGridRows;
+        std::vector<double> zg(F.M + 1), chig(F.M + 1);
+        if (F.budget) {
+            F.chiMax = 0.0;
+            for (int i = 0; i <= F.M; i++) {
+                zg[i] = zObs - (zObs - zMin) * i / F.M;
+                chig[i] = reach_of(zg[i], zObs, bMax);
+                F.chiMax = std::max(F.chiMax, chig[i]);
+            }
+        } else {
+            F.chiMax = F.spd * (F.etaObs - h_eta(zMin));
+            for (int i = 0; i <= F.M; i++) {
+                chig[i] = F.chiMax * i / F.M;
+                zg[i] = 2.0 * atan(exp(F.etaObs - chig[i] / F.spd));
+            }
+        }
+        const int K = cfg->wraps >= 0 ? cfg->wraps : (int)ceil((F.chiMax + 4.0) / 2.0);
+        if (out->frame_meta) {
+            out->frame_meta[fi * 3 + 0] = zObs;
+            out->frame_meta[fi * 3 + 1] = F.chiMax;
+            out->frame_meta[fi * 3 + 2] = K;
+        }
+        cudaMemcpy(dZg, zg.data(), (F.M + 1) * 8, cudaMemcpyHostToDevice);
+        cudaMemcpy(dChig, chig.data(), (F.M + 1) * 8, cudaMemcpyHostToDevice);
+        {
+            const int64_t tot = (int64_t)n * (F.M + 1);
+            k_fb_grid<<<(int)std::min<int64_t>((tot + 255) / 256, 65536), 256>>>(P, F.M, dZg, dPx, dPy);
+        }
+        for (int o = 0; o < cfg->n_obs; o++) {
+            double ox, oy, bxv = 0.0, byv = 0.0;
+            if (cfg->obs_type[o] == 0) {
+                double vx, vy;
+                h_comov(A2, A, Bv, Fv, nw, cfg->obs_path[o], zObs, &ox, &oy, &vx, &vy);
+                bxv = sin(zObs) * vx / F.spd;
+                byv = sin(zObs) * vy / F.spd;
+            } else {
+                ox = cfg->obs_xy[2 * o];
+                oy = cfg->obs_xy[2 * o + 1];
+            }
+            if (out->obs_meta) {
+                double* m = out->obs_meta + ((size_t)fi * cfg->n_obs + o) * 4;
+                m[0] = ox;
+                m[1] = oy;
+                m[2] = bxv;
+                m[3] = byv;
+            }
+            cudaMemset(dCount, 0, 8);
+            const int side = 2 * K + 1;
+            const int64_t tot = (int64_t)n * side * side;
+            k_fb_hits<<<(int)std::min<int64_t>((tot + 127) / 128, 1 << 20), 128>>>(
+                P, F, ox, oy, K, cfg->obs_type[o] == 0 ? cfg->obs_path[o] : -1, dZg, dChig, dPx, dPy, dHits,
+                dCount, hitCap);
+            unsigned long long nh = 0;
+            cudaError_t e = cudaMemcpy(&nh, dCount, 8, cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) {
+                std::string m = std::string("frame_bake: ") + cudaGetErrorString(e);
+                return set_error(UG_ECUDA, m.c_str());
+            }
+            if (nh > hitCap) return set_error(UG_ECAP, "frame_bake: hit cap overflow (lower the wraps)");
+            if (want_density) {
+                cudaMemset(dDen, 0, bins2 * 4);
+                if (nh)
+                    k_fb_density<<<(int)std::min<unsigned long long>((nh + 255) / 256, 65536), 256>>>(
+                        dHits, (int64_t)nh, F.chiMax, cfg->density_bins, dDen);
+                cudaMemcpy(out->density + ((size_t)fi * cfg->n_obs + o) * bins2, dDen, bins2 * 4,
+                           cudaMemcpyDeviceToHost);
+            }
+            if (out->hit_count) out->hit_count[(size_t)fi * cfg->n_obs + o] = (int64_t)nh;
+            out->hits_total += (int64_t)nh;
+            if (out->hits && written + (int64_t)nh <= out->hit_cap) {
+                hh.resize(nh);
+                if (nh) cudaMemcpy(hh.data(), dHits, nh * sizeof(ug_hit), cudaMemcpyDeviceToHost);
+                // device append order is scheduling-dependent: sort by (chi, src)
+                std::sort(hh.begin(), hh.end(), [](const ug_hit& x, const ug_hit& y) {
+                    return x.chi < y.chi || (x.chi == y.chi && x.src < y.src);
+                });
+                if (nh) memcpy(out->hits + written, hh.data(), nh * sizeof(ug_hit));
+                written += (int64_t)nh;
+            }
+        }
+    }
+    const cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        std::string m = std::string("frame_bake: ") + cudaGetErrorString(e);
+        return set_error(UG_ECUDA, m.c_str());
+    }
+    if (out->hits && out->hits_total > out->hit_cap) return set_error(UG_ECAP, "frame_bake: hit buffer too small");
+    return UG_OK;
+}

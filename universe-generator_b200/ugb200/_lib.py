@@ -26,6 +26,7 @@ EXPORTS = (
     "ug_batch_params_noalloc",
     "ug_batch_kernel_times", "ug_batch_reset_times", "ug_batch_counters", "ug_batch_mixed_error",
     "ug_batch_destroy", "ug_pack_create", "ug_pack_run", "ug_pack_stats", "ug_pack_destroy",
+    "ug_frame_bake",
 )
 
 
@@ -97,6 +98,7 @@ def load():
     L.ug_batch_mixed_error.argtypes = [vp, i32, i64, i64, C.POINTER(C.c_double),
                                        C.POINTER(C.c_double)]
     L.ug_batch_destroy.argtypes = [vp]
+    L.ug_frame_bake.argtypes = [vp, i32, i32, vp, vp, vp, vp, vp]
     for name in EXPORTS:
         f = getattr(L, name)
         if f.restype is None or name != "ug_last_error":
