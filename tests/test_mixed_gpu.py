@@ -53,3 +53,17 @@ def test_mixed_batch_with_fp64_only_universes(ug, oracle):
             idx, _ = p.accepted(k)
             ref = oracle.pack(_model(oracle, u), u.attempts)
             assert np.array_equal(idx, ref.acc_idx), k
+
+
+@pytest.mark.parametrize("T,seed", [(16, 3), (40, 8), (101, 2)])
+def test_mixed_1d_crossing_rule(ug, oracle, T, seed):
+    """1+1D with the crossing rule through the tensor-core path (guard-banded FP32
+    contact and sign-change test, FP64 retest of the undecided)."""
+    u = ug.Universe(dim=1, T=T, zgrid=1, excl=1, cross1d=1, seed=seed, attempts=30000, round_size=4096)
+    ref = oracle.pack(_model(oracle, u), u.attempts)
+    with ug.Packer([u], precision=ug.PREC_MIXED) as p:
+        p.run()
+        a, _ = p.accepted(0)
+        st = p.stats(0)
+    assert np.array_equal(a, ref.acc_idx)
+    assert st.gray < u.attempts // 10  # most candidates decided in FP32

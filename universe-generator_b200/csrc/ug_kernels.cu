@@ -360,14 +360,18 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_surv_eval(const UniDev* __r
         const uint64_t idx = (uint64_t)(c.round_base + d.surv_off[UG_IDX(r, d.S_max + 1)]);
         const int F1 = d.F + 1, T = d.T;
         warp_gen64(d, idx, alpha, beta, a2, bj, wj, lane);
-        const int64_t cpt = cells_per_t(d);
-        (void)cpt;
-        for (int t = lane; t < T; t += 32) {
+        for (int t0 = lane; t0 < T; t0 += 4 * 32) {
+          double X4[3][4];
+          for (int ax = 0; ax < d.dim; ax++)
+              eval64_multi<4>(d, alpha + ax * F1, beta + ax * F1, a2[ax], t0, 32, X4[ax]);
+          for (int k = 0; k < 4; k++) {
+            const int t = t0 + 32 * k;
+            if (t >= T) break;
             Pt64 q;
             int cc[3];
             for (int ax = 0; ax < 3; ax++) q.c[ax] = 0.0;
             for (int ax = 0; ax < d.dim; ax++) {
-                q.c[ax] = eval64(d, alpha + ax * F1, beta + ax * F1, 1, a2[ax], t);
+                q.c[ax] = X4[ax][k];
                 cc[ax] = cell_of(q.c[ax], d.cell, d.gw);
             }
             const uint64_t key = rkey_of(c.epoch, t, lin_cell(cc, d.dim, d.gw));
@@ -381,6 +385,7 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_surv_eval(const UniDev* __r
             q.next = nxt;
             q.gid = -1;
             d.spos[UG_IDX((int64_t)r * T + t, (int64_t)d.S_max * T)] = q;
+          }
         }
         __syncwarp();
     }

@@ -423,6 +423,61 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                 break;
             }
             tc_fence_after();
+            if (dim == 1 && d.cross1d && !dump) {
+                // 1+1D with the crossing rule: stage the FP32 trajectory (natural
+                // timestep order; the stages are free once the MMAs are done), then
+                // test every accepted path at every timestep.
+                float* xs = reinterpret_cast<float*>(sm);
+                const int pitch = T + 1;
+                const uint32_t lb = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+                for (int c0 = part * 8; c0 < nm; c0 += 8 * kMxParts) {
+                    float x8[8];
+                    tmem_ld8(lb + (uint32_t)UG_IDX(c0 + 7, L.ncols) - 7, x8);
+                    tmem_wait_ld();
+                    for (int j = 0; j < 8; j++)
+                        if (c0 + j < T) xs[row * pitch + c0 + j] = torus_wrapf(fmaf(x8[j], inv_sum[0], a2f[0]));
+                }
+                tc_fence_before();
+                __syncthreads();
+                const int64_t ns = ctl[u].n_slots;
+                const float rin = r - mrg, rout = r + mrg;
+                for (int64_t sl = part; sl < ns; sl += kMxParts) {
+                    if (vrej[row]) break;
+                    const Pt32* q = d.ptf + UG_IDX(sl * T + T - 1, d.slot_cap * T) + 1 - T;
+                    bool hit = false, g = false;
+                    float d0 = torus_deltaf(xs[row * pitch] - __ldg(&q[0].c[0]));
+                    float a0 = fabsf(d0);
+                    hit = a0 < rin;
+                    g = !hit && a0 <= rout;
+                    for (int t = 1; t < T && !hit; t++) {
+                        const float d1 = torus_deltaf(xs[row * pitch + t] - __ldg(&q[t].c[0]));
+                        const float a1 = fabsf(d1);
+                        if (a1 < rin) {
+                            hit = true;
+                            break;
+                        }
+                        g = g || a1 <= rout;
+                        // crossing: certain when both signs are certain and the sum is clear of 1
+                        const bool flip = (d0 < 0.f) != (d1 < 0.f);
+                        const bool signs_sure = a0 > mrg && a1 > mrg;
+                        const float sum = a0 + a1;
+                        if (flip && signs_sure && sum < 1.f - 2.f * mrg) {
+                            hit = true;
+                            break;
+                        }
+                        if ((!signs_sure && sum < 1.f + 2.f * mrg) ||
+                            (flip && sum >= 1.f - 2.f * mrg && sum <= 1.f + 2.f * mrg))
+                            g = true;
+                        d0 = d1;
+                        a0 = a1;
+                    }
+                    nev += T;
+                    if (hit) vrej[row] = 1;
+                    else if (g) vgray[row] = 1;
+                }
+                __syncthreads();
+                continue;  // single pass for dim 1
+            }
             // epilogue: 8-column blocks part, part+4, ... of this pass (endpoint-first order)
             const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
             for (int c0 = part * 8; c0 < nm; c0 += 8 * kMxParts) {
@@ -533,7 +588,8 @@ static float bf16_val(uint16_t b) {
 
 int mixed_setup(const ug_universe_cfg& cfg, UniDev& d, MixedTables& mt) {
     const int T = cfg.T, F = cfg.T, dim = cfg.dim;
-    d.mx_ok = (cfg.rng == UG_RNG_PHILOX && !cfg.cross1d && cfg.group_mode == UG_GROUP_NONE) ? 1 : 0;
+    d.mx_ok = (cfg.rng == UG_RNG_PHILOX && cfg.group_mode == UG_GROUP_NONE) ? 1 : 0;
+    const bool natural = cfg.dim == 1 && cfg.cross1d;  // the crossing test walks t in order
     const int P = F / 2;
     const int nch = (P + kPairsPerChunk - 1) / kPairsPerChunk;
     // B rows: timesteps padded to 16; when dim * rows exceeds the 512 tensor
@@ -575,9 +631,10 @@ int mixed_setup(const ug_universe_cfg& cfg, UniDev& d, MixedTables& mt) {
                 Cm[(size_t)b * T + t] = cos(b * z[t]) - 1.0;
             }
         for (int i = 0; i < T; i++) order[i] = i;
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-            return std::min(a, T - 1 - a) < std::min(b, T - 1 - b);
-        });
+        if (!natural)
+            std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+                return std::min(a, T - 1 - a) < std::min(b, T - 1 - b);
+            });
     }
     const size_t img = (size_t)tpad * kKC;  // BF16 elements per hi (or lo) image
     std::vector<uint16_t> host((size_t)nch * 2 * img, 0);
