@@ -390,46 +390,6 @@ __device__ __forceinline__ double eval64(const UniDev& U, const double* alpha, c
     return torus_wrap(fma(acc, __ldg(U.invsinz + t), a2));
 }
 
-// eval64 for NT timesteps t0, t0+step, ... at once: NT independent
-// accumulation chains, each in the same order as eval64 (identical values).
-// Timesteps >= T are skipped (their outputs are left untouched).
-template <int NT>
-__device__ __forceinline__ void eval64_multi(const UniDev& U, const double* alpha, const double* beta, double a2,
-                                             int t0, int step, double* out) {
-    const int T = U.T, F = U.F;
-    double acc[NT];
-    int tt[NT];
-#pragma unroll
-    for (int k = 0; k < NT; k++) {
-        acc[k] = 0.0;
-        tt[k] = min(t0 + k * step, T - 1);
-    }
-    int b = 2;
-    for (; b + 1 <= F; b += 2) {
-        const double al0 = alpha[b], be0 = beta[b], al1 = alpha[b + 1];
-        const double* S0 = U.S + (size_t)b * T;
-        const double* C0 = U.Cm + (size_t)b * T;
-        const double* S1 = U.S + (size_t)(b + 1) * T;
-#pragma unroll
-        for (int k = 0; k < NT; k++) {
-            acc[k] = fma(al0, __ldg(S0 + tt[k]), acc[k]);
-            acc[k] = fma(be0, __ldg(C0 + tt[k]), acc[k]);
-            acc[k] = fma(al1, __ldg(S1 + tt[k]), acc[k]);
-        }
-    }
-    if (b <= F) {
-        const double al0 = alpha[b], be0 = beta[b];
-#pragma unroll
-        for (int k = 0; k < NT; k++) {
-            acc[k] = fma(al0, __ldg(U.S + (size_t)b * T + tt[k]), acc[k]);
-            acc[k] = fma(be0, __ldg(U.Cm + (size_t)b * T + tt[k]), acc[k]);
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < NT; k++)
-        if (t0 + k * step < T) out[k] = torus_wrap(fma(acc[k], __ldg(U.invsinz + tt[k]), a2));
-}
-
 // ------------------------------------------------------------ grid access
 
 __device__ __forceinline__ uint64_t mix64(uint64_t k) {

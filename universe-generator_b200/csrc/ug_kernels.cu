@@ -360,31 +360,13 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_surv_eval(const UniDev* __r
         const uint64_t idx = (uint64_t)(c.round_base + d.surv_off[UG_IDX(r, d.S_max + 1)]);
         const int F1 = d.F + 1, T = d.T;
         warp_gen64(d, idx, alpha, beta, a2, bj, wj, lane);
-        // timesteps per lane per pass: as many independent chains as the lane has
-        // timesteps, up to four (T <= 32: one chain, no duplicated work)
-        const int nt = T <= 32 ? 1 : (T <= 64 ? 2 : (T <= 96 ? 3 : 4));
-        for (int t0 = lane; t0 < T; t0 += nt * 32) {
-          double X4[3][4];
-          for (int ax = 0; ax < d.dim; ax++) {
-              const double* al = alpha + ax * F1;
-              const double* bt = beta + ax * F1;
-              if (nt == 1)
-                  eval64_multi<1>(d, al, bt, a2[ax], t0, 32, X4[ax]);
-              else if (nt == 2)
-                  eval64_multi<2>(d, al, bt, a2[ax], t0, 32, X4[ax]);
-              else if (nt == 3)
-                  eval64_multi<3>(d, al, bt, a2[ax], t0, 32, X4[ax]);
-              else
-                  eval64_multi<4>(d, al, bt, a2[ax], t0, 32, X4[ax]);
-          }
-          for (int k = 0; k < nt; k++) {
-            const int t = t0 + 32 * k;
-            if (t >= T) break;
+        for (int t = lane; t < T; t += 32) {
+          {
             Pt64 q;
             int cc[3];
             for (int ax = 0; ax < 3; ax++) q.c[ax] = 0.0;
             for (int ax = 0; ax < d.dim; ax++) {
-                q.c[ax] = X4[ax][k];
+                q.c[ax] = eval64(d, alpha + ax * F1, beta + ax * F1, 1, a2[ax], t);
                 cc[ax] = cell_of(q.c[ax], d.cell, d.gw);
             }
             const uint64_t key = rkey_of(c.epoch, t, lin_cell(cc, d.dim, d.gw));
