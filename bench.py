@@ -271,6 +271,10 @@ def main() -> int:
         times.append(e0.elapsed_time(e1))
         cands += sum(packer.stats(k).attempts for k in range(len(us)))
     launches = packer.counters()[0] - launches0
+    # accepted sets of the last timed job, for the FP64 single-universe comparison
+    sample = list(range(0, len(us), 8)) if len(us) > 1 else [0]
+    last_seeds = seeds(args.warmup + args.steps - 1)
+    acc_batched = {k: packer.accepted(k)[0] for k in sample}
     if sampler:
         sampler.terminate()
         sampler.wait()
@@ -321,6 +325,29 @@ def main() -> int:
                 "launches": pk_n, "avg_launch_ms": pk_ms / max(pk_n, 1),
                 "evals": evals, "kernel_share": {k: v[0] for k, v in kt.items()}}
 
+    # the plain FP64 single-universe form on the same B200 and the same seeds: one
+    # universe per packer, thread-per-candidate FP64 prefilter (the metric's denominator)
+    f_ms, f_c, same = 0.0, 0, True
+    for k in sample:
+        u = us[k]
+        uu = ugb200.Universe(**{**u.__dict__, "seed": last_seeds[k]})
+        with ugb200.Packer([uu], precision=ugb200.PREC_FP64, device=local, stream=stream.cuda_stream,
+                           rounds_per_sync=8, use_graph=True) as p1:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            p1.run()
+            e1.record(stream)
+            e1.synchronize()
+            f_ms += e0.elapsed_time(e1)
+            f_c += p1.stats(0).attempts
+            same = same and np.array_equal(p1.accepted(0)[0], acc_batched[k])
+    fp64_plain = {"value": f_c / (f_ms / 1000.0), "unit": "candidates/s",
+                  "sample": f"{len(sample)} of the workload's universes (every 8th), each run alone "
+                            f"in FP64 with the seeds of the last timed job, {f_c} candidates",
+                  "same_accepted_set": bool(same)}
+    fp64_plain["mixed_batched_speedup"] = value / fp64_plain["value"]
+
     if rank == 0:
         line = {"metric": "candidates tested/s", "value": value, "unit": "candidates/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -333,7 +360,7 @@ def main() -> int:
                            "l2": "flushed between steps (256 MiB write)",
                            "parallelism": f"replicas x{world}"},
                 "e2e": e2e, "gpu_launches": launches,
-                "roofline": roofline,
+                "roofline": roofline, "fp64_plain_single_universe": fp64_plain,
                 "clocks": clocks_summary(clk_path)}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(us)
