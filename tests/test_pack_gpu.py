@@ -152,3 +152,19 @@ def test_round_sizes_stay_within_buffers(ug, oracle, precision):
     (T=200: the initial round size is not a power-of-two fraction of the cap)."""
     u = ug.Universe(dim=2, T=200, zgrid=1, excl=1, seed=2, attempts=60000, round_size=16384)
     _check(ug, oracle, u, precision=precision)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("excl,T", [(0, 9), (0, 17), (0, 25), (1, 13), (1, 21)])
+def test_seam_blocks_when_cells_are_not_a_multiple_of_eight(ug, oracle, precision, excl, T):
+    """Neighbourhoods that wrap across the seam where the last occupancy block is
+    short (gw = 9, 17, 25, 26, 42 cells): every block of the range must be checked."""
+    for dim in (1, 2, 3):
+        for seed in range(3):
+            u = ug.Universe(dim=dim, T=T, zgrid=excl, excl=excl, seed=1000 * dim + seed,
+                            attempts=6000, round_size=1024)
+            ref = oracle.pack(_model(oracle, u), u.attempts)
+            with ug.Packer([u], precision=precision) as p:
+                p.run()
+                idx, _ = p.accepted(0)
+            assert np.array_equal(idx, ref.acc_idx), (dim, seed)

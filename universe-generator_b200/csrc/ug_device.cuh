@@ -472,30 +472,51 @@ __device__ __forceinline__ void nbhd_make(const UniDev& U, const int* c, const i
 }
 
 // Second-level occupancy: false proves every cell of the neighbourhood empty.
+// Per axis the range is up to four consecutive cells modulo gw, so its blocks
+// form at most three runs (one wrap); every distinct block is checked.
 template <int D>
 __device__ __forceinline__ bool nbhd_occ1(const UniDev& U, int t, const Nbhd<D>& nb) {
     const int sh = U.occ_shift + 3;
-    int bl[D][2];
+    int bl[D][3], nbk[D];
 #pragma unroll
     for (int ax = 0; ax < D; ax++) {
         bl[ax][0] = nb.v[ax][0] >> sh;
-        bl[ax][1] = nb.last[ax] >> sh;
+        bl[ax][1] = bl[ax][0];
+        bl[ax][2] = bl[ax][0];
+        int cnt = 1;
+#pragma unroll
+        for (int k = 1; k < 4; k++) {
+            if (k >= nb.n[ax]) break;
+            const int bk = nb.v[ax][k] >> sh;
+            const int prev = cnt == 1 ? bl[ax][0] : (cnt == 2 ? bl[ax][1] : bl[ax][2]);
+            if (bk != prev && cnt < 3) {
+                if (cnt == 1)
+                    bl[ax][1] = bk;
+                else
+                    bl[ax][2] = bk;
+                cnt++;
+            }
+        }
+        nbk[ax] = cnt;
     }
     const uint32_t* base = U.occ1;
     const int64_t t0 = (int64_t)t * U.occ1_per_t;
 #pragma unroll
-    for (int i = 0; i < (1 << D); i++) {
-        int64_t lin = 0;
-        bool dup = false;
+    for (int i0 = 0; i0 < 3; i0++) {
+        if (i0 >= nbk[0]) break;
 #pragma unroll
-        for (int ax = 0; ax < D; ax++) {
-            const int pick = (i >> ax) & 1;
-            dup |= pick && bl[ax][1] == bl[ax][0];
-            lin = lin * U.occ1_gw + bl[ax][pick];
+        for (int i1 = 0; i1 < (D > 1 ? 3 : 1); i1++) {
+            if (D > 1 && i1 >= nbk[D > 1 ? 1 : 0]) break;
+#pragma unroll
+            for (int i2 = 0; i2 < (D > 2 ? 3 : 1); i2++) {
+                if (D > 2 && i2 >= nbk[D > 2 ? 2 : 0]) break;
+                int64_t lin = bl[0][i0];
+                if (D > 1) lin = lin * U.occ1_gw + bl[D > 1 ? 1 : 0][i1];
+                if (D > 2) lin = lin * U.occ1_gw + bl[D > 2 ? 2 : 0][i2];
+                const int64_t b = t0 + lin;
+                if ((__ldg(base + UG_IDX(b >> 5, U.occ1_words)) >> (b & 31)) & 1u) return true;
+            }
         }
-        if (dup) continue;
-        const int64_t b = t0 + lin;
-        if ((__ldg(base + UG_IDX(b >> 5, U.occ1_words)) >> (b & 31)) & 1u) return true;
     }
     return false;
 }
