@@ -239,8 +239,10 @@ def main() -> int:
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     total_cands = sum(u.attempts for u in us)
 
+    base_seeds = [u.seed for u in us]  # reset() writes the new seeds into the universes
+
     def seeds(step):
-        return [(u.seed + 7919 * (step + 1)) & (2**64 - 1) for u in us]
+        return [(s0 + 7919 * (step + 1)) & (2**64 - 1) for s0 in base_seeds]
 
     # warm-up
     for w in range(args.warmup):
