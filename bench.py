@@ -200,6 +200,12 @@ def main() -> int:
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="run one untimed packing job of the workload and exit (for ncu captures)")
+    ap.add_argument("--stride", type=int, default=1,
+                    help="--profile-case: every stride-th universe of the workload")
+    ap.add_argument("--max-rounds", type=int, default=0,
+                    help="--profile-case: stop after this many rounds (0: run to the stop rule)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -222,9 +228,17 @@ def main() -> int:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     prec = ugb200.PREC_MIXED if args.precision == "mixed" else ugb200.PREC_FP64
+    # weak scaling: every rank packs the full universe list with its own seeds
     us, cfg = workloads(args.workload, ugb200, 1000 * rank)
-    if len(us) > 1 and world > 1:  # shard universes across ranks (weak: each rank the full list)
-        pass
+    if args.profile_case:
+        sub = us[::max(1, args.stride)]
+        with ugb200.Packer(sub, precision=prec, device=local, use_graph=False) as p:
+            p.run(max_rounds=args.max_rounds)
+            st = [p.stats(k) for k in range(len(sub))]
+        print(json.dumps({"profile_case": args.workload, "universes": len(sub),
+                          "candidates": sum(s.attempts for s in st),
+                          "evals": sum(s.evals for s in st), "rounds": max(s.rounds for s in st)}))
+        return 0
     stream = torch.cuda.Stream()
     try:
         packer = ugb200.Packer(us, precision=prec, device=local, stream=stream.cuda_stream,
