@@ -125,6 +125,13 @@ struct UniDev {
     int32_t mx_nmma;         // UMMA N per pass
     int32_t mx_npass;        // timestep passes (2 when dim * tpad > 512 TMEM columns)
     float mx_margin;         // guard band of the FP32 Chebyshev test
+    // survivor trajectories as an FP64 product coef[K x Rpad]^T * KT[K x Tpad]:
+    // term k runs over (b = 2..F: sin term, then the cos term of even b) -- the
+    // accumulation order of eval64, so both give the same bits
+    const double* KT;        // [K * Tpad] S_b / Cm_b rows in term order, zero padded
+    double* coef;            // [K * Rpad] alpha_b / beta_b of row (survivor r, axis) = r * dim + ax
+    double* a2row;           // [Rpad]
+    int32_t K, Tpad, Rpad, pad4;
     // sizes (index guards of the checked build)
     int64_t occ_words, occ1_words, dense_cells, bimg_bytes;
 };

@@ -46,11 +46,14 @@ static int fail(int code, const char* fmt, ...) {
                         __FILE__, __LINE__, #x, cudaGetErrorString(e_));                      \
     } while (0)
 
-enum KernelId { K_PLAN, K_PRE, K_MIXED, K_CONFIRM, K_COMPACT, K_SEVAL, K_CONFL, K_GREEDY, K_COMMIT, K_NK };
-static const char* kKernelNames[12] = {"k_plan",    "k_prefilter64", "k_prefilter_mixed",
-                                       "k_confirm64w", "k_compact",   "k_surv_eval",
-                                       "k_conflicts", "k_greedy",    "k_commit",
-                                       "",           "",            ""};
+enum KernelId {
+    K_PLAN, K_PRE, K_MIXED, K_CONFIRM, K_COMPACT, K_SGEN, K_CONFL, K_GREEDY, K_COMMIT, K_SGEMM, K_SHASH,
+    K_NK
+};
+static const char* kKernelNames[12] = {"k_plan",      "k_prefilter64", "k_prefilter_mixed",
+                                       "k_confirm64w", "k_compact",     "k_surv_gen",
+                                       "k_conflicts", "k_greedy",      "k_commit",
+                                       "k_surv_gemm", "k_surv_hash",   ""};
 
 struct UniHost {
     ug_universe_cfg cfg;
@@ -224,6 +227,28 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
     d.Cm = dC;
     d.invsinz = dI;
     d.order = dO;
+    // term-ordered table of the survivor product (row kseq_s(b): sin(b z),
+    // row kseq_s(b) + 1 for even b: cos(b z) - 1), timesteps padded to 32
+    {
+        const int F = d.F;
+        d.K = kseq_len(F);
+        d.Tpad = (T + 31) / 32 * 32;
+        d.Rpad = (d.S_max * c.dim + 31) / 32 * 32;
+        std::vector<double> kt((size_t)d.K * d.Tpad, 0.0);
+        for (int b = 2; b <= F; b++) {
+            const int k = kseq_s(b);
+            for (int t = 0; t < T; t++) {
+                kt[(size_t)k * d.Tpad + t] = S[(size_t)b * T + t];
+                if (!(b & 1)) kt[(size_t)(k + 1) * d.Tpad + t] = Cm[(size_t)b * T + t];
+            }
+        }
+        double* dK;
+        if ((rc = dalloc(h, &dK, kt.size())) || (rc = dalloc(h, &d.coef, (size_t)d.K * d.Rpad, 0)) ||
+            (rc = dalloc(h, &d.a2row, (size_t)d.Rpad, 0)))
+            return rc;
+        CKR(cudaMemcpy(dK, kt.data(), kt.size() * 8, cudaMemcpyHostToDevice));
+        d.KT = dK;
+    }
     // grid
     int64_t cpt = 1;
     for (int ax = 0; ax < c.dim; ax++) cpt *= d.gw;
@@ -349,10 +374,16 @@ static int launch_round(Batch& B, bool timed) {
     tb(K_COMPACT);
     k_compact<<<B.n, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
     te(K_COMPACT);
-    tb(K_SEVAL);
-    k_surv_eval<<<B.nsm * 4, 32 * kSurvWarps, kSurvWarps * kSurvSmemPerWarp, B.st>>>(B.dU, B.dCtl,
-                                                                                      B.dInfo);
-    te(K_SEVAL);
+    tb(K_SGEN);
+    k_surv_gen<<<B.nsm * 4, 32 * kSurvWarps, kSurvWarps * kSurvSmemPerWarp, B.st>>>(B.dU, B.dCtl,
+                                                                                     B.dInfo);
+    te(K_SGEN);
+    tb(K_SGEMM);
+    k_surv_gemm<<<B.nsm * 4, 128, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+    te(K_SGEMM);
+    tb(K_SHASH);
+    k_surv_hash<<<B.nsm * 8, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+    te(K_SHASH);
     tb(K_CONFL);
     k_conflicts<<<B.nsm * 8, 128, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
     te(K_CONFL);
@@ -562,7 +593,7 @@ int ug_batch_create(const ug_universe_cfg* cfgs, int32_t n, const ug_run_opts* o
     if (cudaFuncSetAttribute(k_greedy, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(2 * kSmaxCap * sizeof(int32_t))) != cudaSuccess)
         return bail(fail(UG_ECUDA, "smem attribute failed"));
-    if (cudaFuncSetAttribute(k_surv_eval, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(k_surv_gen, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(kSurvWarps * kSurvSmemPerWarp)) != cudaSuccess)
         return bail(fail(UG_ECUDA, "smem attribute failed"));
     if (B->any_mixed && (rc = mixed_init_kernels())) return bail(rc);

@@ -5,7 +5,9 @@
 //   k_prefilter64  FP64 test of every candidate against the committed packing
 //                  (or k_prefilter_mixed + k_confirm64, ug_mixed.cu)
 //   k_compact      survivors in candidate-index order (deterministic)
-//   k_surv_eval    FP64 trajectories of the survivors + round hash insert
+//   k_surv_gen     FP64 coefficients of the survivors (term-ordered rows)
+//   k_surv_gemm    their FP64 trajectories as a register-tiled product
+//   k_surv_hash    round hash insert of every survivor timestep
 //   k_conflicts    each survivor's contacts with EARLIER survivors of the round
 //   k_greedy       in-order resolution: survivor i is admitted iff it touches
 //                  no admitted earlier survivor (group rules in group modes)
@@ -235,13 +237,22 @@ __global__ void __launch_bounds__(256) k_compact(const UniDev* __restrict__ U, U
     __syncthreads();
     if (s_last && tid == 0) {
         __threadfence();
-        int acc = 0;
+        int acc = 0, sev = 0, spt = 0;
         for (int v = 0; v < info->n_uni; v++) {
+            const int Sv = *(volatile int32_t*)&ctl[v].S;
             info->surv_off[v] = acc;
-            acc += *(volatile int32_t*)&ctl[v].S;
+            info->sev_off[v] = sev;
+            info->spt_off[v] = spt;
+            acc += Sv;
+            sev += ((Sv * U[v].dim + 31) >> 5) * ((U[v].T + 31) >> 5);
+            spt += Sv * U[v].T;
         }
         info->surv_off[info->n_uni] = acc;
+        info->sev_off[info->n_uni] = sev;
+        info->spt_off[info->n_uni] = spt;
         info->total_surv = acc;
+        info->total_sev = sev;
+        info->total_spt = spt;
     }
 }
 
@@ -336,12 +347,14 @@ __device__ __forceinline__ void warp_gen64(const UniDev& d, uint64_t idx, double
     }
 }
 
-// One warp per survivor: FP64 regeneration (warp-parallel Philox blocks,
-// sequential normalisation sum in ascending b -- the same operations as the
-// thread-per-candidate prefilter, so identical values), trajectories at all
-// T timesteps, round-hash insert.
-__global__ void __launch_bounds__(32 * kSurvWarps) k_surv_eval(const UniDev* __restrict__ U,
-                                                                 UniCtl* ctl, RoundInfo* info) {
+// Survivor trajectories in three steps.
+//
+// k_surv_gen: one warp per survivor regenerates its FP64 coefficients
+// (warp-parallel Philox blocks, sequential normalisation sum in ascending b --
+// the same operations as the thread-per-candidate prefilter, so identical
+// values) and stores them as rows r * dim + ax of the term-ordered matrix coef.
+__global__ void __launch_bounds__(32 * kSurvWarps) k_surv_gen(const UniDev* __restrict__ U,
+                                                                UniCtl* ctl, RoundInfo* info) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     unsigned char* my = smem_raw + (size_t)wib * kSurvSmemPerWarp;
@@ -358,31 +371,117 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_surv_eval(const UniDev* __r
         const UniDev& d = U[u];
         const UniCtl& c = ctl[u];
         const uint64_t idx = (uint64_t)(c.round_base + d.surv_off[UG_IDX(r, d.S_max + 1)]);
-        const int F1 = d.F + 1, T = d.T;
+        const int F = d.F, F1 = F + 1, R = d.Rpad;
+        [[maybe_unused]] const int64_t ncoef = (int64_t)d.K * R;
         warp_gen64(d, idx, alpha, beta, a2, bj, wj, lane);
-        for (int t = lane; t < T; t += 32) {
-          {
-            Pt64 q;
-            int cc[3];
-            for (int ax = 0; ax < 3; ax++) q.c[ax] = 0.0;
-            for (int ax = 0; ax < d.dim; ax++) {
-                q.c[ax] = eval64(d, alpha + ax * F1, beta + ax * F1, 1, a2[ax], t);
-                cc[ax] = cell_of(q.c[ax], d.cell, d.gw);
+        for (int ax = 0; ax < d.dim; ax++) {
+            const int row = r * d.dim + ax;
+            const double* al = alpha + ax * F1;
+            const double* bt = beta + ax * F1;
+            for (int b = 2 + lane; b <= F; b += 32) {
+                const int64_t k = kseq_s(b);
+                d.coef[UG_IDX(k * R + row, ncoef)] = al[b];
+                if (!(b & 1)) d.coef[UG_IDX((k + 1) * R + row, ncoef)] = bt[b];
             }
-            const uint64_t key = rkey_of(c.epoch, t, lin_cell(cc, d.dim, d.gw));
-            const uint64_t h = rhash_claim(d, key);
-            int32_t nxt = -1;
-            if (h != ~0ull) {
-                const uint64_t old = atomicExch((unsigned long long*)(d.rvals + h),
-                                                ((uint64_t)(c.epoch & 0xFFFFFF) << 32) | (uint32_t)r);
-                if ((old >> 32) == (uint64_t)(c.epoch & 0xFFFFFF)) nxt = (int32_t)(uint32_t)old;
-            }
-            q.next = nxt;
-            q.gid = -1;
-            d.spos[UG_IDX((int64_t)r * T + t, (int64_t)d.S_max * T)] = q;
-          }
+            if (lane == 0) d.a2row[UG_IDX(row, R)] = a2[ax];
         }
         __syncwarp();
+    }
+}
+
+// k_surv_gemm: X[row][t] = wrap(a2 + invsinz_t * sum_k coef[k][row] KT[k][t]),
+// one warp per 32-row x 32-timestep tile.  Lane (rg, tg) owns rows
+// row0 + 0..3 and timesteps t0 + 8 jj + {0,1}; every (row, t) is a single FMA
+// chain in ascending k, i.e. eval64's operations in eval64's order.
+__global__ void __launch_bounds__(128) k_surv_gemm(const UniDev* __restrict__ U, UniCtl* ctl,
+                                                   RoundInfo* info) {
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+    const int n_uni = info->n_uni, total = info->total_sev;
+    const int rg = lane >> 2, tg = lane & 3;
+    for (int item = gwarp; item < total; item += nwarps) {
+        const int u = find_uni(info->sev_off, n_uni, item);
+        const int local = item - info->sev_off[u];
+        const UniDev& d = U[u];
+        const int T = d.T, dim = d.dim, K = d.K, R = d.Rpad, TP = d.Tpad;
+        const int ntb = (T + 31) >> 5;
+        const int rb = local / ntb, tb = local - rb * ntb;
+        const int row0 = rb * 32 + rg * 4;
+        const int t0 = tb * 32 + 2 * tg;
+        const double* A = d.coef + row0;
+        const double* Bt = d.KT + t0;
+        double acc[4][8];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 8; j++) acc[i][j] = 0.0;
+#pragma unroll 2
+        for (int k = 0; k < K; k++) {
+            const double2 a01 = __ldg((const double2*)(A + (size_t)k * R));
+            const double2 a23 = __ldg((const double2*)(A + (size_t)k * R + 2));
+            const double av[4] = {a01.x, a01.y, a23.x, a23.y};
+            double bv[8];
+#pragma unroll
+            for (int jj = 0; jj < 4; jj++) {
+                const double2 b2 = __ldg((const double2*)(Bt + (size_t)k * TP + 8 * jj));
+                bv[2 * jj] = b2.x;
+                bv[2 * jj + 1] = b2.y;
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 8; j++) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+        }
+        const int nrows = ctl[u].S * dim;
+        [[maybe_unused]] const int64_t nspos = (int64_t)d.S_max * T;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int row = row0 + i;
+            if (row >= nrows) continue;
+            const int r = row / dim, ax = row - r * dim;
+            const double a2 = d.a2row[UG_IDX(row, R)];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int t = t0 + 8 * (j >> 1) + (j & 1);
+                if (t < T)
+                    d.spos[UG_IDX((int64_t)r * T + t, nspos)].c[ax] =
+                        torus_wrap(fma(acc[i][j], __ldg(d.invsinz + t), a2));
+            }
+        }
+    }
+}
+
+// Round hash block of a cell: 2 cells per axis, so the 3 neighbour cells of
+// a point span at most 2 blocks per axis (3 at the seam of an odd gw).
+__device__ __forceinline__ int rblock_gw(const UniDev& d) { return (d.gw + 1) >> 1; }
+
+// k_surv_hash: one thread per survivor timestep inserts the point into the
+// round hash (key: epoch, t, block).
+__global__ void __launch_bounds__(256) k_surv_hash(const UniDev* __restrict__ U, UniCtl* ctl,
+                                                   RoundInfo* info) {
+    const int n_uni = info->n_uni, total = info->total_spt;
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < total; w += gridDim.x * blockDim.x) {
+        const int u = find_uni(info->spt_off, n_uni, w);
+        const UniDev& d = U[u];
+        const UniCtl& c = ctl[u];
+        const int T = d.T;
+        const int local = w - info->spt_off[u];
+        const int r = local / T, t = local - r * T;
+        Pt64* q = d.spos + UG_IDX((int64_t)r * T + t, (int64_t)d.S_max * T);
+        int bc[3];
+        for (int ax = 0; ax < d.dim; ax++) bc[ax] = cell_of(q->c[ax], d.cell, d.gw) >> 1;
+        for (int ax = d.dim; ax < 3; ax++) q->c[ax] = 0.0;
+        const uint64_t key = rkey_of(c.epoch, t, lin_cell(bc, d.dim, rblock_gw(d)));
+        const uint64_t h = rhash_claim(d, key);
+        int32_t nxt = -1;
+        if (h != ~0ull) {
+            const uint64_t old = atomicExch((unsigned long long*)(d.rvals + h),
+                                            ((uint64_t)(c.epoch & 0xFFFFFF) << 32) | (uint32_t)r);
+            if ((old >> 32) == (uint64_t)(c.epoch & 0xFFFFFF)) nxt = (int32_t)(uint32_t)old;
+        }
+        q->next = nxt;
+        q->gid = -1;
     }
 }
 
@@ -574,32 +673,42 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
                 if (hit) add(r2);
             }
         } else {
-            const int nb = d.dim == 1 ? 3 : (d.dim == 2 ? 9 : 27);
+            const int gw = d.gw, gwb = rblock_gw(d);
             for (int t = lane; t < T; t += 32) {
                 const Pt64 P = d.spos[UG_IDX((int64_t)r * T + t, (int64_t)d.S_max * T)];
-                int c0[3];
-                for (int ax = 0; ax < d.dim; ax++) c0[ax] = cell_of(P.c[ax], d.cell, d.gw);
-                for (int k = 0; k < nb; k++) {
-                    int cc[3], rr = k;
-                    for (int ax = d.dim - 1; ax >= 0; ax--) {
-                        const int dd = rr % 3 - 1;
-                        rr /= 3;
-                        int v = c0[ax] + dd;
-                        v = v < 0 ? v + d.gw : (v >= d.gw ? v - d.gw : v);
-                        cc[ax] = v;
-                    }
-                    int32_t r2 = rhash_head(d, rkey_of(c.epoch, t, lin_cell(cc, d.dim, d.gw)));
-                    while (r2 >= 0) {
-                        const Pt64* Q = d.spos + UG_IDX((int64_t)r2 * T + t, (int64_t)d.S_max * T);
-                        if (r2 < r) {
-                            bool hit = true;
-                            for (int ax = 0; ax < d.dim && hit; ax++)
-                                hit = hit1(torus_delta(P.c[ax] - Q->c[ax]), d.cell, d.inclusive);
-                            if (hit) add(r2);
-                        }
-                        r2 = Q->next;
-                    }
+                // distinct round-hash blocks of the 3 neighbour cells per axis
+                int bl[3][3], nbk[3];
+                for (int ax = 0; ax < 3; ax++) {
+                    nbk[ax] = 1;
+                    bl[ax][0] = bl[ax][1] = bl[ax][2] = 0;
                 }
+                for (int ax = 0; ax < d.dim; ax++) {
+                    const int c0 = cell_of(P.c[ax], d.cell, gw);
+                    const int v0 = (c0 == 0 ? gw - 1 : c0 - 1) >> 1;
+                    const int v1 = c0 >> 1;
+                    const int v2 = (c0 == gw - 1 ? 0 : c0 + 1) >> 1;
+                    int n = 0;
+                    bl[ax][n++] = v0;
+                    if (v1 != v0) bl[ax][n++] = v1;
+                    if (v2 != v0 && v2 != v1) bl[ax][n++] = v2;
+                    nbk[ax] = n;
+                }
+                for (int i0 = 0; i0 < nbk[0]; i0++)
+                    for (int i1 = 0; i1 < nbk[1]; i1++)
+                        for (int i2 = 0; i2 < nbk[2]; i2++) {
+                            const int bc[3] = {bl[0][i0], bl[1][i1], bl[2][i2]};
+                            int32_t r2 = rhash_head(d, rkey_of(c.epoch, t, lin_cell(bc, d.dim, gwb)));
+                            while (r2 >= 0) {
+                                const Pt64* Q = d.spos + UG_IDX((int64_t)r2 * T + t, (int64_t)d.S_max * T);
+                                if (r2 < r) {
+                                    bool hit = true;
+                                    for (int ax = 0; ax < d.dim && hit; ax++)
+                                        hit = hit1(torus_delta(P.c[ax] - Q->c[ax]), d.cell, d.inclusive);
+                                    if (hit) add(r2);
+                                }
+                                r2 = Q->next;
+                            }
+                        }
             }
         }
         __syncwarp();
@@ -801,19 +910,14 @@ __device__ __forceinline__ void grid_insert(const UniDev& d, UniCtl& c, int t, i
 
 __global__ void __launch_bounds__(256) k_commit(const UniDev* __restrict__ U, UniCtl* ctl,
                                                 RoundInfo* info) {
-    const int n_uni = info->n_uni, total = info->total_surv;
-    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
-    // items: survivor-major, T per survivor; T varies per universe so walk
-    // survivors and let each thread stride over (survivor, t) within it.
-    for (int64_t w = gtid; w < (int64_t)total * kMaxF; w += nthr) {
-        const int item = (int)(w / kMaxF);
-        const int t = (int)(w % kMaxF);
-        const int u = find_uni(info->surv_off, n_uni, item);
+    const int n_uni = info->n_uni, total = info->total_spt;
+    // items: (survivor, timestep) pairs, survivor-major per universe
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < total; w += gridDim.x * blockDim.x) {
+        const int u = find_uni(info->spt_off, n_uni, w);
         const UniDev& d = U[u];
-        if (t >= d.T) continue;
         UniCtl& c = ctl[u];
-        const int r = item - info->surv_off[u];
+        const int local = w - info->spt_off[u];
+        const int r = local / d.T, t = local - r * d.T;
         if (r >= c.stop_at) continue;
         const int k = d.acc_rank[UG_IDX(r, d.S_max)];
         if (k < 0) continue;

@@ -18,10 +18,19 @@ struct RoundInfo {
     int32_t pad[2];
     int32_t total_gray;
     int32_t gray_done;
+    int32_t total_sev;     // k_surv_gemm warp tiles (32 rows x 32 timesteps)
+    int32_t total_spt;     // survivor timesteps (k_surv_hash / k_commit items)
     int32_t tile_off[kMaxUni + 1];
     int32_t surv_off[kMaxUni + 1];
     int32_t gray_pref[kMaxUni + 1];
+    int32_t sev_off[kMaxUni + 1];
+    int32_t spt_off[kMaxUni + 1];
 };
+
+// Term k of the survivor product: sin term of frequency b at k = kseq_s(b),
+// its cos term (even b) at kseq_s(b) + 1.
+__host__ __device__ __forceinline__ int kseq_s(int b) { return (b - 2) + ((b - 1) >> 1); }
+__host__ __device__ __forceinline__ int kseq_len(int F) { return kseq_s(F) + 1 + ((F & 1) ? 0 : 1); }
 
 __device__ __forceinline__ int find_uni(const int32_t* off, int n, int item) {
     int lo = 0, hi = n - 1;
@@ -41,13 +50,15 @@ __global__ void k_prefilter64(const UniDev* __restrict__ U, UniCtl* ctl, RoundIn
 __global__ void k_gray_compact(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_confirm64w(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_compact(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
-__global__ void k_surv_eval(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
+__global__ void k_surv_gen(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
+__global__ void k_surv_gemm(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
+__global__ void k_surv_hash(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_conflicts(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_greedy(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_commit(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_rehash(const UniDev* __restrict__ U, UniCtl* ctl, int u, int64_t n_slots);
 
-// Shared memory of k_surv_eval per warp (bytes), for F <= kMaxF.
+// Shared memory of k_surv_gen per warp (bytes), for F <= kMaxF.
 constexpr int kSurvWarps = 4;
 constexpr size_t kSurvSmemPerWarpBase = (size_t)3 * (kMaxF + 1) * 2 * sizeof(double) + 3 * sizeof(double) +
                                     (size_t)kMaxF * (sizeof(int32_t) + sizeof(double));
