@@ -87,7 +87,7 @@ struct Batch {
     bool any_mixed = false;
     int64_t launches = 0;  // kernels issued (graph replays count every node)
     int64_t h2d = 0, d2h = 0;  // bytes copied between host and device
-    int kernels_per_round = 7;
+    int kernels_per_round = 9;
 };
 
 static int64_t pow2_at_least(int64_t v) {
@@ -264,7 +264,8 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
         if ((rc = alloc_hash(h, pow2_at_least(std::max<int64_t>(1 << 16, 4LL * d.S_max * T)))))
             return rc;
     }
-    // occupancy bitmap, coarsened until it is at most 256 MiB
+    // occupancy bitmap, coarsened until it is at most 512 MiB (T <= 256 in 3D
+    // keeps 2 cells per coarse cell per axis or finer)
     {
         int sh = 0;
         int64_t bits;
@@ -273,7 +274,7 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
             int64_t per = 1;
             for (int ax = 0; ax < c.dim; ax++) per *= g;
             bits = (int64_t)T * per;
-            if (bits <= ((int64_t)1 << 31) || sh >= 4) {
+            if (bits <= ((int64_t)1 << 32) || sh >= 4) {
                 d.occ_shift = sh;
                 d.occ_gw = (int32_t)g;
                 d.occ_per_t = per;
@@ -597,7 +598,7 @@ int ug_batch_create(const ug_universe_cfg* cfgs, int32_t n, const ug_run_opts* o
                              (int)(kSurvWarps * kSurvSmemPerWarp)) != cudaSuccess)
         return bail(fail(UG_ECUDA, "smem attribute failed"));
     if (B->any_mixed && (rc = mixed_init_kernels())) return bail(rc);
-    B->kernels_per_round = B->any_mixed ? 9 : 7;
+    B->kernels_per_round = B->any_mixed ? 11 : 9;
     if (B->any_mixed && cudaFuncSetAttribute(k_confirm64w, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)(kSurvWarps * kConfSmemPerWarp)) != cudaSuccess)
         return bail(fail(UG_ECUDA, "smem attribute failed"));

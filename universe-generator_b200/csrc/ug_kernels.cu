@@ -878,8 +878,11 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
 
 // ---------------------------------------------------------------- commit
 
+// Appends slot to the chain of cell lin at timestep t; *old_head gets the
+// previous head.  *new_key is set when the insert claimed a new hash key (the
+// caller counts them into UniCtl::hash_used).
 __device__ __forceinline__ void grid_insert(const UniDev& d, UniCtl& c, int t, int64_t lin,
-                                            int64_t cpt, int32_t slot, int32_t* old_head) {
+                                            int64_t cpt, int32_t slot, int32_t* old_head, bool* new_key) {
     if (d.grid_kind == GRID_DENSE) {
         *old_head = atomicExch(d.heads + UG_IDX((int64_t)t * cpt + lin, d.dense_cells), slot);
         return;
@@ -891,7 +894,7 @@ __device__ __forceinline__ void grid_insert(const UniDev& d, UniCtl& c, int t, i
         if (k == kEmptyKey) {
             const uint64_t prev = atomicCAS((unsigned long long*)(d.hkeys + h), kEmptyKey, key);
             if (prev == kEmptyKey) {
-                atomicAdd((unsigned long long*)&c.hash_used, 1ull);
+                *new_key = true;
                 k = key;
             } else {
                 k = prev;
@@ -908,41 +911,60 @@ __device__ __forceinline__ void grid_insert(const UniDev& d, UniCtl& c, int t, i
     c.state = ST_ERROR;
 }
 
+// Sets a bit of an occupancy bitmap; bits are only ever set during a run, so
+// a bit read as set needs no atomic.
+__device__ __forceinline__ void occ_set(uint32_t* words, int64_t bit, int64_t nwords) {
+    uint32_t* w = words + UG_IDX(bit >> 5, nwords);
+    const uint32_t m = 1u << (bit & 31);
+    if (!(__ldcg(w) & m)) atomicOr(w, m);
+}
+
 __global__ void __launch_bounds__(256) k_commit(const UniDev* __restrict__ U, UniCtl* ctl,
                                                 RoundInfo* info) {
     const int n_uni = info->n_uni, total = info->total_spt;
-    // items: (survivor, timestep) pairs, survivor-major per universe
-    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < total; w += gridDim.x * blockDim.x) {
-        const int u = find_uni(info->spt_off, n_uni, w);
-        const UniDev& d = U[u];
-        UniCtl& c = ctl[u];
-        const int local = w - info->spt_off[u];
-        const int r = local / d.T, t = local - r * d.T;
-        if (r >= c.stop_at) continue;
-        const int k = d.acc_rank[UG_IDX(r, d.S_max)];
-        if (k < 0) continue;
-        const int64_t slot = UG_IDX(c.n_slots_prev + k, d.slot_cap);
-        Pt64 q = d.spos[UG_IDX((int64_t)r * d.T + t, (int64_t)d.S_max * d.T)];
-        int cc[3];
-        for (int ax = 0; ax < d.dim; ax++) cc[ax] = cell_of(q.c[ax], d.cell, d.gw);
-        int32_t old;
-        grid_insert(d, c, t, lin_cell(cc, d.dim, d.gw), cells_per_t(d), (int32_t)slot, &old);
-        {
-            const int64_t b = occ_bit(d, t, cc);
-            atomicOr(d.occ + UG_IDX(b >> 5, d.occ_words), 1u << (b & 31));
-            const int64_t b1 = occ1_bit(d, t, cc);
-            atomicOr(d.occ1 + UG_IDX(b1 >> 5, d.occ1_words), 1u << (b1 & 31));
+    const int lane = threadIdx.x & 31;
+    // items: (survivor, timestep) pairs, survivor-major per universe; the trip
+    // count is uniform over the block so the warp-level counting below converges
+    for (int w0 = blockIdx.x * blockDim.x; w0 < total; w0 += gridDim.x * blockDim.x) {
+        const int w = w0 + threadIdx.x;
+        int u = -1;
+        bool new_key = false;
+        if (w < total) {
+            u = find_uni(info->spt_off, n_uni, w);
+            const UniDev& d = U[u];
+            UniCtl& c = ctl[u];
+            const int local = w - info->spt_off[u];
+            const int r = local / d.T, t = local - r * d.T;
+            const int k = r < c.stop_at ? d.acc_rank[UG_IDX(r, d.S_max)] : -1;
+            if (k >= 0) {
+                const int64_t slot = UG_IDX(c.n_slots_prev + k, d.slot_cap);
+                Pt64 q = d.spos[UG_IDX((int64_t)r * d.T + t, (int64_t)d.S_max * d.T)];
+                int cc[3];
+                for (int ax = 0; ax < d.dim; ax++) cc[ax] = cell_of(q.c[ax], d.cell, d.gw);
+                int32_t old;
+                grid_insert(d, c, t, lin_cell(cc, d.dim, d.gw), cells_per_t(d), (int32_t)slot, &old, &new_key);
+                occ_set(d.occ, occ_bit(d, t, cc), d.occ_words);
+                occ_set(d.occ1, occ1_bit(d, t, cc), d.occ1_words);
+                q.next = old;
+                q.gid = d.sgid[UG_IDX(r, d.S_max)];
+                d.pts[UG_IDX(slot * d.T + t, d.slot_cap * d.T)] = q;
+                Pt32 f;
+                f.c[0] = (float)q.c[0];
+                f.c[1] = (float)q.c[1];
+                f.c[2] = (float)q.c[2];
+                f.next = old;
+                d.ptf[UG_IDX(slot * d.T + t, d.slot_cap * d.T)] = f;
+                if (t == 0)
+                    d.acc_idx[UG_IDX(slot, d.slot_cap)] = c.round_base + d.surv_off[UG_IDX(r, d.S_max + 1)];
+            }
         }
-        q.next = old;
-        q.gid = d.sgid[UG_IDX(r, d.S_max)];
-        d.pts[UG_IDX(slot * d.T + t, d.slot_cap * d.T)] = q;
-        Pt32 f;
-        f.c[0] = (float)q.c[0];
-        f.c[1] = (float)q.c[1];
-        f.c[2] = (float)q.c[2];
-        f.next = old;
-        d.ptf[UG_IDX(slot * d.T + t, d.slot_cap * d.T)] = f;
-        if (t == 0) d.acc_idx[UG_IDX(slot, d.slot_cap)] = c.round_base + d.surv_off[UG_IDX(r, d.S_max + 1)];
+        // new hash keys: one atomic per (warp, universe) instead of one per key
+        const uint32_t nk = __ballot_sync(0xffffffffu, new_key);
+        if (nk) {
+            const uint32_t mine = nk & __match_any_sync(0xffffffffu, u);
+            if (new_key && lane == __ffs(mine) - 1)
+                atomicAdd((unsigned long long*)&ctl[u].hash_used, (unsigned long long)__popc(mine));
+        }
     }
 }
 
@@ -960,7 +982,9 @@ __global__ void k_rehash(const UniDev* __restrict__ U, UniCtl* ctl, int u, int64
         int cc[3];
         for (int ax = 0; ax < d.dim; ax++) cc[ax] = cell_of(q->c[ax], d.cell, d.gw);
         int32_t old;
-        grid_insert(d, c, t, lin_cell(cc, d.dim, d.gw), cells_per_t(d), (int32_t)slot, &old);
+        bool new_key = false;
+        grid_insert(d, c, t, lin_cell(cc, d.dim, d.gw), cells_per_t(d), (int32_t)slot, &old, &new_key);
+        if (new_key) atomicAdd((unsigned long long*)&c.hash_used, 1ull);
         q->next = old;
         d.ptf[slot * d.T + t].next = old;
     }
