@@ -349,6 +349,8 @@ def main() -> int:
         uu = ugb200.Universe(**{**u.__dict__, "seed": last_seeds[k]})
         with ugb200.Packer([uu], precision=ugb200.PREC_FP64, device=local, stream=stream.cuda_stream,
                            rounds_per_sync=8, use_graph=True) as p1:
+            p1.run()  # warm-up: builds the CUDA graph of the rounds, as the batched warm-up does
+            p1.reset([last_seeds[k]])
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)

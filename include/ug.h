@@ -172,9 +172,11 @@ int ug_batch_reset_times(void* h);
 /* Maximum |X_mixed - X_fp64| of the tensor-core evaluation over the first
  * `count` candidates of universe u (all timesteps and axes): the achieved
  * position error of the mixed-precision prefilter against FP64.  Also
- * returns the guard margin the prefilter applies. */
+ * returns the widest guard band the prefilter applies (`margin`) and the
+ * largest ratio of the error to the guard band of its own (candidate,
+ * timestep) (`max_ratio`, below 1 whenever every decision is exact). */
 int ug_batch_mixed_error(void* h, int32_t u, int64_t first, int64_t count, double* max_err,
-                         double* margin);
+                         double* margin, double* max_ratio);
 
 /* Release all device memory of the batch. */
 int ug_batch_destroy(void* h);

@@ -17,14 +17,18 @@ def _model(O, u):
 def test_mixed_position_error_within_guard(ug, dim, T, zg, ex):
     u = ug.Universe(dim=dim, T=T, zgrid=zg, excl=ex, seed=3, attempts=1000, round_size=1024)
     with ug.Packer([u], precision=ug.PREC_MIXED) as p:
-        err, margin = p.mixed_error(0, 0, 2048)
-    print(f"dim={dim} T={T}: max |X_mixed - X_fp64| = {err:.3e}, guard {margin:.3e}")
+        err, margin, ratio = p.mixed_error(0, 0, 2048)
+    print(f"dim={dim} T={T}: max |X_mixed - X_fp64| = {err:.3e}, widest guard {margin:.3e}, "
+          f"max error / own guard {ratio:.3e}")
     assert err < margin / 2
+    # the guard band of every (candidate, timestep) is twice its rigorous error bound
+    assert ratio < 0.5
 
 
 @pytest.mark.parametrize("dim,T,zg,ex,att", [(2, 16, 0, 0, 30000), (2, 32, 1, 1, 60000),
                                              (3, 24, 1, 1, 40000), (2, 64, 1, 1, 100000),
-                                             (3, 200, 1, 1, 8000), (2, 23, 0, 1, 30000)])
+                                             (3, 200, 1, 1, 8000), (2, 23, 0, 1, 30000),
+                                             (3, 240, 1, 1, 6000), (2, 250, 1, 1, 40000)])
 def test_mixed_accepted_set_equals_oracle_and_fp64(ug, oracle, dim, T, zg, ex, att):
     u = ug.Universe(dim=dim, T=T, zgrid=zg, excl=ex, seed=11 + T, attempts=att, round_size=4096)
     ref = oracle.pack(_model(oracle, u), att)

@@ -125,6 +125,10 @@ struct UniDev {
     int32_t mx_nmma;         // UMMA N per pass
     int32_t mx_npass;        // timestep passes (2 when dim * tpad > 512 TMEM columns)
     float mx_margin;         // guard band of the FP32 Chebyshev test
+    // per-(candidate, timestep) guard band: 2 mx_mc1 * bound + mx_mc0, where
+    // bound = min(2, 2 invsinz_t rho) >= sum_k |A_k B_kt| / sum E and
+    // rho = sum_b (E_b / b) / sum E of the candidate (largest over its axes)
+    float mx_mc1, mx_mc0;
     // survivor trajectories as an FP64 product coef[K x Rpad]^T * KT[K x Tpad]:
     // term k runs over (b = 2..F: sin term, then the cos term of even b) -- the
     // accumulation order of eval64, so both give the same bits

@@ -792,11 +792,12 @@ int ug_batch_reset_times(void* h) {
     return UG_OK;
 }
 
-int ug_batch_mixed_error(void* h, int32_t u, int64_t first, int64_t count, double* max_err, double* margin) {
+int ug_batch_mixed_error(void* h, int32_t u, int64_t first, int64_t count, double* max_err, double* margin,
+                         double* max_ratio) {
     Batch* B = (Batch*)h;
     if (!B || u < 0 || u >= B->n) return fail(UG_EINVAL, "bad arguments");
     if (B->opts.precision != UG_PREC_MIXED) return fail(UG_ENOTSUP, "batch is not mixed precision");
-    return mixed_error(B->dU, u, B->U[u].d, B->U[u].mt, first, count, max_err, margin, B->st);
+    return mixed_error(B->dU, u, B->U[u].d, B->U[u].mt, first, count, max_err, margin, max_ratio, B->st);
 }
 
 int ug_batch_destroy(void* h) {

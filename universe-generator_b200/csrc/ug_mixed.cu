@@ -155,11 +155,12 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
 // of the canonical A images (12 entries = three 8-byte pieces per image).
 // Returns the quarter's contribution to sum_b E_b.
 __device__ __forceinline__ double gen_quarter(const UniDev& d, uint64_t idx, int ax, int ch, int part,
-                                              bool valid, uint8_t* a_hi, uint8_t* a_lo, int row) {
+                                              bool valid, uint8_t* a_hi, uint8_t* a_lo, int row,
+                                              double* sum_eb) {
     const int F = d.F;
     const int P = F >> 1;
     float v[12];
-    double sum = 0.0;
+    double sum = 0.0, seb = 0.0;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         const int p = ch * kPairsPerChunk + part * 4 + q + 1;
@@ -175,11 +176,13 @@ __device__ __forceinline__ double gen_quarter(const UniDev& d, uint64_t idx, int
             ae = se * cf;
             be = se * sf;
             sum += (double)Ee;
+            seb += (double)Ee / (double)(2 * p);
             if (2 * p + 1 <= F) {
                 const float Eo = -__logf(((float)o.y + 0.5f) * 2.3283064365386963e-10f);
                 const float ro = __frcp_rn((float)(2 * p + 1));
                 ao = (o.w & 1u) ? -Eo * ro : Eo * ro;
                 sum += (double)Eo;
+                seb += (double)Eo / (double)(2 * p + 1);
             }
         }
         v[3 * q] = ae;
@@ -201,6 +204,7 @@ __device__ __forceinline__ double gen_quarter(const UniDev& d, uint64_t idx, int
         *reinterpret_cast<uint2*>(a_hi + off) = make_uint2(h[0], h[1]);
         *reinterpret_cast<uint2*>(a_lo + off) = make_uint2(l[0], l[1]);
     }
+    *sum_eb += seb;
     return sum;
 }
 
@@ -268,8 +272,10 @@ __device__ __forceinline__ int test32_at(const UniDev& d, int t, const float* X,
 struct MixedLaunch {
     uint32_t ncols;    // tensor-memory columns per CTA
     int tpad_max;      // widest B image (rows) of the batch: sizes the B stage
-    // debug dump of X (FP32 positions) for universe u, candidates [first, first+count)
+    // debug dump of X (FP32 positions) for universe u, candidates [first, first+count),
+    // and of the guard band of each (candidate, timestep)
     float* dump;
+    float* dump_m;
     int u;
     int64_t first, count;
 };
@@ -286,8 +292,8 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
     const int part = warp >> 2;
     // carve: two stages of {A_hi, A_lo, B (hi then lo)}; per-row state; barriers
     const int stage_bytes = 2 * kAImgBytes + L.tpad_max * kKC * 2 * 2;
-    double* s_sum = reinterpret_cast<double*>(sm + 2 * stage_bytes);      // [kTile][kMxParts]
-    int* s_rej = reinterpret_cast<int*>(s_sum + kTile * kMxParts);       // [kTile]
+    double* s_sum = reinterpret_cast<double*>(sm + 2 * stage_bytes);      // [kTile][kMxParts][2]
+    int* s_rej = reinterpret_cast<int*>(s_sum + kTile * kMxParts * 2);   // [kTile]
     int* s_gray = s_rej + kTile;                                          // [kTile]
     uint64_t* bar = reinterpret_cast<uint64_t*>(s_gray + kTile);
     uint64_t* bar_b = bar;       // [2] B chunk landed
@@ -346,6 +352,7 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
         const float r = (float)d.cell, mrg = d.mx_margin, inv_cell = (float)(1.0 / d.cell);
         const int64_t cpt = cells_per_t(d);
         float inv_sum[3] = {0.f, 0.f, 0.f}, a2f[3] = {0.f, 0.f, 0.f};
+        float rho = 0.f;  // largest sum_b (E_b / b) / sum E over the axes
         if (part == 0) {
             s_rej[row] = valid ? 0 : 1;
             s_gray[row] = 0;
@@ -354,7 +361,7 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
         for (int pass = 0; pass < d.mx_npass && !timeout; pass++) {
             if (pass > 0 && __syncthreads_and(vrej[row] != 0)) break;
             for (int ax = 0; ax < dim && !timeout; ax++) {
-                double sumE = 0.0;
+                double sumE = 0.0, sumEb = 0.0;
                 if (pass == 0 && valid) {
                     const uint4 o = philox_block(d.seed, idx, ax, 0);
                     a2f[ax] = d.pin ? 0.f : (float)((double)o.x * (1.0 / 2147483648.0) - 1.0);
@@ -378,7 +385,7 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                         bulk_g2s(b_img, d.mx_bimg + UG_IDX((int64_t)ch * bchunk + bchunk - 1, d.bimg_bytes) + 1 - bchunk,
                                  bchunk, &bar_b[st]);
                     }
-                    sumE += gen_quarter(d, idx, ax, ch, part, valid, a_hi, a_lo, row);
+                    sumE += gen_quarter(d, idx, ax, ch, part, valid, a_hi, a_lo, row, &sumEb);
                     fence_proxy_async();
                     __syncthreads();
                     if (tid == 0) {
@@ -406,11 +413,14 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                 }
                 if (timeout) break;
                 if (pass == 0) {  // combine the four partial sums of the row in a fixed order
-                    s_sum[row * kMxParts + part] = sumE;
+                    double* ss = s_sum + row * kMxParts * 2;
+                    ss[2 * part] = sumE;
+                    ss[2 * part + 1] = sumEb;
                     __syncthreads();
-                    const double tot = s_sum[row * kMxParts + 0] + s_sum[row * kMxParts + 1] +
-                                       s_sum[row * kMxParts + 2] + s_sum[row * kMxParts + 3];
+                    const double tot = ss[0] + ss[2] + ss[4] + ss[6];
+                    const double teb = ss[1] + ss[3] + ss[5] + ss[7];
                     inv_sum[ax] = valid ? (float)(1.0 / tot) : 0.f;
+                    if (valid) rho = fmaxf(rho, (float)(teb / tot));
                     __syncthreads();
                 }
             }
@@ -494,16 +504,21 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                     const int t = __ldg(d.order + col);
                     float X[3];
                     for (int ax = 0; ax < dim; ax++) X[ax] = torus_wrapf(fmaf(x[ax][j], inv_sum[ax], a2f[ax]));
+                    // guard band of this timestep (1% over the bound: FP32 evaluation of it)
+                    const float bnd = fminf(2.f, 2.f * (float)__ldg(d.invsinz + t) * rho);
+                    const float mt = (2.f * d.mx_mc1 * bnd + d.mx_mc0) * 1.01f;
                     if (dump) {
-                        if (valid)
+                        if (valid) {
                             for (int ax = 0; ax < dim; ax++)
                                 L.dump[((size_t)off * T + t) * dim + ax] = X[ax];
+                            L.dump_m[(size_t)off * T + t] = mt;
+                        }
                         continue;
                     }
                     if (vrej[row]) break;
                     nev++;
                     bool gr = false;
-                    if (test32_at(d, t, X, r, mrg, inv_cell, cpt, &gr)) vrej[row] = 1;
+                    if (test32_at(d, t, X, r, mt, inv_cell, cpt, &gr)) vrej[row] = 1;
                     if (gr) vgray[row] = 1;
                 }
             }
@@ -571,7 +586,7 @@ static size_t g_smem = 0;
 static int g_ctas_per_sm = 1;
 
 static size_t smem_bytes() {
-    return (size_t)2 * (2 * kAImgBytes + g_tpad_max * kKC * 2 * 2) + (size_t)kTile * kMxParts * 8 +
+    return (size_t)2 * (2 * kAImgBytes + g_tpad_max * kKC * 2 * 2) + (size_t)kTile * kMxParts * 16 +
            2 * kTile * 4 + 64;
 }
 
@@ -610,9 +625,18 @@ int mixed_setup(const ug_universe_cfg& cfg, UniDev& d, MixedTables& mt) {
     // FP32 accumulation of 3K products (<= 2^-23 each, relative to the same sum),
     // FP32 generation (logf, sincosf, reciprocals: < 2e-6), stored FP32 points and
     // the FP32 subtraction (< 4e-7); doubled for safety.
+    // The bound 2 on sum|A||B| / sum E tightens per candidate and timestep to
+    // min(2, 2 rho / sin z_t): the pair terms of frequency b are at most
+    // (E_b / b) * 2 / sin z_t (Cauchy-Schwarz over (cos f, sin f) with
+    // |sin x|^2 + |cos x - 1|^2 <= 4), so their sum is at most
+    // (2 / sin z_t) sum_b E_b / b = (2 / sin z_t) rho sum E.
     const int K = nch * kKC;
-    const double m = 2.0 * (3.0 * std::ldexp(1.0, -16) * 2.0 + 3.0 * K * std::ldexp(1.0, -23) * 2.0 + 2e-6) + 4e-7;
+    const double mc1 = 3.0 * std::ldexp(1.0, -16) + 3.0 * K * std::ldexp(1.0, -23);
+    const double mc0 = 2.0 * 2e-6 + 4e-7;
+    const double m = 2.0 * mc1 * 2.0 + mc0;
     d.mx_margin = (float)m;
+    d.mx_mc1 = (float)mc1;
+    d.mx_mc0 = (float)mc0;
     mt.margin = m;
     mt.K = K;
     mt.Tp = tpad;
@@ -702,39 +726,51 @@ int mixed_init_kernels() {
 }
 
 void launch_prefilter_mixed(const UniDev* dU, UniCtl* dCtl, RoundInfo* dInfo, int nsm, cudaStream_t st) {
-    MixedLaunch L{(uint32_t)g_ncols, g_tpad_max, nullptr, 0, 0, 0};
+    MixedLaunch L{(uint32_t)g_ncols, g_tpad_max, nullptr, nullptr, 0, 0, 0};
     k_prefilter_mixed<<<nsm * g_ctas_per_sm, kMxThreads, g_smem, st>>>(dU, dCtl, dInfo, L);
 }
 
 int mixed_error(const UniDev* dU, int u, const UniDev& d, const MixedTables& mt, int64_t first, int64_t count,
-                double* max_err, double* margin, cudaStream_t st) {
+                double* max_err, double* margin, double* max_ratio, cudaStream_t st) {
     if (!d.mx_ok) return UG_ENOTSUP;
-    const size_t n = (size_t)count * d.T * d.dim;
-    float* d32 = nullptr;
+    const size_t nm = (size_t)count * d.T;
+    const size_t n = nm * d.dim;
+    float *d32 = nullptr, *dm = nullptr;
     double* d64 = nullptr;
-    if (cudaMalloc(&d32, n * 4) != cudaSuccess || cudaMalloc(&d64, n * 8) != cudaSuccess) return UG_ENOMEM;
+    if (cudaMalloc(&d32, n * 4) != cudaSuccess || cudaMalloc(&dm, nm * 4) != cudaSuccess ||
+        cudaMalloc(&d64, n * 8) != cudaSuccess) {
+        cudaFree(d32);
+        cudaFree(dm);
+        return UG_ENOMEM;
+    }
     cudaMemsetAsync(d32, 0, n * 4, st);
-    MixedLaunch L{(uint32_t)g_ncols, g_tpad_max, d32, u, first, count};
+    cudaMemsetAsync(dm, 0, nm * 4, st);
+    MixedLaunch L{(uint32_t)g_ncols, g_tpad_max, d32, dm, u, first, count};
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
     k_prefilter_mixed<<<nsm * g_ctas_per_sm, kMxThreads, g_smem, st>>>(dU, nullptr, nullptr, L);
     k_pos64<<<(int)std::min<int64_t>((count + 127) / 128, 2048), 128, 0, st>>>(dU, u, first, count, d64);
-    std::vector<float> h32(n);
+    std::vector<float> h32(n), hm(nm);
     std::vector<double> h64(n);
     cudaError_t e = cudaStreamSynchronize(st);
     if (e == cudaSuccess) e = cudaMemcpy(h32.data(), d32, n * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(hm.data(), dm, nm * 4, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(h64.data(), d64, n * 8, cudaMemcpyDeviceToHost);
     cudaFree(d32);
+    cudaFree(dm);
     cudaFree(d64);
     if (e != cudaSuccess) return UG_ECUDA;
-    double mx = 0.0;
+    double mx = 0.0, ratio = 0.0;
     for (size_t i = 0; i < n; i++) {
         double df = fabs((double)h32[i] - h64[i]);
         df = std::min(df, 2.0 - df);
         mx = std::max(mx, df);
+        const double band = (double)hm[i / d.dim];
+        ratio = std::max(ratio, band > 0.0 ? df / band : INFINITY);
     }
     *max_err = mx;
     *margin = mt.margin;
+    *max_ratio = ratio;
     return UG_OK;
 }
 

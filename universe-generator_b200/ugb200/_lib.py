@@ -96,7 +96,7 @@ def load():
     L.ug_batch_reset_times.argtypes = [vp]
     L.ug_batch_counters.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]
     L.ug_batch_mixed_error.argtypes = [vp, i32, i64, i64, C.POINTER(C.c_double),
-                                       C.POINTER(C.c_double)]
+                                       C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.ug_batch_destroy.argtypes = [vp]
     L.ug_frame_bake.argtypes = [vp, i32, i32, vp, vp, vp, vp, vp]
     for name in EXPORTS:

@@ -164,11 +164,14 @@ class Packer:
     def reset_times(self) -> None:
         L.check(L.load().ug_batch_reset_times(self._h))
 
-    def mixed_error(self, u: int = 0, first: int = 0, count: int = 4096) -> tuple[float, float]:
+    def mixed_error(self, u: int = 0, first: int = 0, count: int = 4096) -> tuple[float, float, float]:
+        """(max |X_mixed - X_fp64|, widest guard band, max error / own guard band)."""
         e = C.c_double()
         m = C.c_double()
-        L.check(L.load().ug_batch_mixed_error(self._h, u, first, count, C.byref(e), C.byref(m)))
-        return e.value, m.value
+        q = C.c_double()
+        L.check(L.load().ug_batch_mixed_error(self._h, u, first, count, C.byref(e), C.byref(m),
+                                              C.byref(q)))
+        return e.value, m.value, q.value
 
     def close(self) -> None:
         if self._h:
