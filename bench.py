@@ -206,6 +206,8 @@ def main() -> int:
                     help="--profile-case: every stride-th universe of the workload")
     ap.add_argument("--max-rounds", type=int, default=0,
                     help="--profile-case: stop after this many rounds (0: run to the stop rule)")
+    ap.add_argument("--universe", type=int, default=-1,
+                    help="--profile-case: only this universe of the workload")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -231,7 +233,7 @@ def main() -> int:
     # weak scaling: every rank packs the full universe list with its own seeds
     us, cfg = workloads(args.workload, ugb200, 1000 * rank)
     if args.profile_case:
-        sub = us[::max(1, args.stride)]
+        sub = [us[args.universe]] if args.universe >= 0 else us[::max(1, args.stride)]
         with ugb200.Packer(sub, precision=prec, device=local, use_graph=False) as p:
             p.run(max_rounds=args.max_rounds)
             st = [p.stats(k) for k in range(len(sub))]

@@ -323,7 +323,14 @@ static void init_ctl(const ug_universe_cfg& c, const UniDev& d, UniCtl& k) {
     k.state = ST_ACTIVE;
     k.B_min = std::min(1024, d.B_max);
     k.B_cap = d.B_max;
-    k.round_B = std::min(std::max(4096, 2 * d.S_max), d.B_max) / kTile * kTile;  // adapted every round
+    // first round: at most half a timestep's cells (a small torus jams after few
+    // paths, and a round far above that only piles up in-round conflicts);
+    // adapted every round after that
+    int64_t cpt = 1;
+    for (int ax = 0; ax < c.dim; ax++) cpt *= d.gw;
+    int64_t b0 = std::max(4096, 2 * d.S_max);
+    if (cpt / 2 < b0) b0 = std::max<int64_t>(1024, cpt / 2);
+    k.round_B = (int)std::min<int64_t>(b0, d.B_max) / kTile * kTile;
     k.accept_rate = c.accept_rate;
     k.sub_accept_rate = c.sub_accept_rate;
     k.win_target = c.accept_rate > 0 ? (int64_t)std::min(5e9, std::max(2e7, 30.0 / c.accept_rate)) : 0;

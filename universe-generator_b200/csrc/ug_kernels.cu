@@ -78,6 +78,7 @@ __global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* inf
         info->any_active = act;
         info->total_surv = 0;
         info->compact_done = 0;
+        info->tile_next = 0;
     }
 }
 
@@ -650,6 +651,8 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
         const UniDev& d = U[u];
         UniCtl& c = ctl[u];
         const int T = d.T;
+        // survivors past a truncation point are re-proposed next round: skip them
+        if (r > *(volatile const int32_t*)&c.trunc) continue;
         if (lane == 0) *cnt = 0;
         __syncwarp();
         auto add = [&](int32_t r2) {

@@ -18,6 +18,8 @@ struct RoundInfo {
     int32_t pad[2];
     int32_t total_gray;
     int32_t gray_done;
+    int32_t tile_next;     // mixed prefilter: tiles handed out beyond the first gridDim.x
+    int32_t pad_ti;
     int32_t total_sev;     // k_surv_gemm warp tiles (32 rows x 32 timesteps)
     int32_t total_spt;     // survivor timesteps (k_surv_hash / k_commit items)
     int32_t tile_off[kMaxUni + 1];

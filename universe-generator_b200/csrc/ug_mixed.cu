@@ -145,6 +145,10 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
 
 // ---------------------------------------------------------- generation
 
+// 1/b rounded to nearest FP32 (the value __frcp_rn gives), b = 0 .. kMaxF + 1;
+// the frequency of a generation step is warp-uniform, so reads broadcast.
+__constant__ float c_rcp[kMaxF + 2];
+
 __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
     const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
     return *reinterpret_cast<const uint32_t*>(&v);
@@ -171,18 +175,19 @@ __device__ __forceinline__ double gen_quarter(const UniDev& d, uint64_t idx, int
             const float f = (float)(o.z >> 1) * 4.656612873077393e-10f * 3.14159265358979f;
             float sf, cf;
             __sincosf(f, &sf, &cf);
-            const float re = __frcp_rn((float)(2 * p));
-            const float se = (o.z & 1u) ? -Ee * re : Ee * re;
+            const float re = c_rcp[2 * p];
+            const float we = Ee * re;
+            const float se = (o.z & 1u) ? -we : we;
             ae = se * cf;
             be = se * sf;
             sum += (double)Ee;
-            seb += (double)Ee / (double)(2 * p);
+            seb += (double)we;  // FP32 rounding of E_b / b is covered by the 1% slack of the band
             if (2 * p + 1 <= F) {
                 const float Eo = -__logf(((float)o.y + 0.5f) * 2.3283064365386963e-10f);
-                const float ro = __frcp_rn((float)(2 * p + 1));
-                ao = (o.w & 1u) ? -Eo * ro : Eo * ro;
+                const float wo = Eo * c_rcp[2 * p + 1];
+                ao = (o.w & 1u) ? -wo : wo;
                 sum += (double)Eo;
-                seb += (double)Eo / (double)(2 * p + 1);
+                seb += (double)wo;
             }
         }
         v[3 * q] = ae;
@@ -320,7 +325,18 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
     volatile int* vrej = s_rej;
     volatile int* vgray = s_gray;
 
-    for (int tile = blockIdx.x; tile < total && !timeout; tile += gridDim.x) {
+    // tiles: the first gridDim.x statically, the rest handed out one at a time
+    // (tile costs differ by orders of magnitude across universes)
+    __shared__ int s_next;
+    auto next_tile = [&](int cur) -> int {
+        if (dump) return cur + (int)gridDim.x;
+        if (tid == 0) s_next = (int)gridDim.x + atomicAdd(&info->tile_next, 1);
+        __syncthreads();
+        const int nt = s_next;
+        __syncthreads();
+        return nt;
+    };
+    for (int tile = blockIdx.x; tile < total && !timeout; tile = next_tile(tile)) {
         const int u = dump ? L.u : find_uni(info->tile_off, n_uni, tile);
         const UniDev& d = U[u];
         const int lt = dump ? tile : tile - info->tile_off[u];
@@ -372,8 +388,8 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                     uint8_t* a_hi = sbase;
                     uint8_t* a_lo = sbase + kAImgBytes;
                     uint8_t* b_img = sbase + 2 * kAImgBytes;
-                    if (seq >= 2) {
-                        if (!mbar_wait(&bar_m[st], ph_m[st])) timeout = true;
+                    if (seq >= 2) {  // one thread polls; the CTA barrier releases the rest
+                        if (tid == 0 && !mbar_wait(&bar_m[st], ph_m[st])) timeout = true;
                         ph_m[st] ^= 1;
                     }
                     if (__syncthreads_or(timeout)) {
@@ -425,8 +441,10 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                 }
             }
             if (timeout) break;
-            if (tid == 0) umma_commit(bar_d);
-            if (!mbar_wait(bar_d, ph_d)) timeout = true;
+            if (tid == 0) {
+                umma_commit(bar_d);
+                if (!mbar_wait(bar_d, ph_d)) timeout = true;
+            }
             ph_d ^= 1;
             if (__syncthreads_or(timeout)) {
                 timeout = true;
@@ -703,6 +721,12 @@ void mixed_free(MixedTables& mt) {
 }
 
 int mixed_init_kernels() {
+    {
+        float rcp[kMaxF + 2];
+        rcp[0] = 0.f;
+        for (int b = 1; b < kMaxF + 2; b++) rcp[b] = (float)(1.0 / (double)b);
+        if (cudaMemcpyToSymbol(c_rcp, rcp, sizeof rcp) != cudaSuccess) return UG_ECUDA;
+    }
     g_smem = smem_bytes();
     // UG_SMEM_PAD=1: request (nearly) all shared memory, one CTA per SM
     const char* pad = getenv("UG_SMEM_PAD");
