@@ -31,6 +31,9 @@ for _p in (ROOT, PKG):
 import numpy as np  # noqa: E402
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# DRAM bytes (read + write) per k_prefilter_mixed launch over one complete job of the
+# workload, from the 1-pass ncu capture in profiles/k_prefilter_mixed_c3_dram.md
+PREFILTER_TRAFFIC = {("c3", "mixed"): 1.668e9}
 FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
 
 
@@ -337,9 +340,13 @@ def main() -> int:
     P, src = peaks()
     achieved = flops / (pk_ms / 1000.0) / 1e12 if pk_ms > 0 else 0.0
     peak = P["bf16_tflops"]
+    traffic = PREFILTER_TRAFFIC.get((args.workload, args.precision))
+    avg_s = pk_ms / max(pk_n, 1) / 1000.0
     roofline = {"bound": "tensor", "kernel": pk_name, "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
+                "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": traffic,
                 "peak_source": f"{src} bf16 dense (burst)",
+                "hbm": ({"achieved_gbs": traffic / avg_s / 1e9, "peak_gbs": P["hbm_gbs"],
+                         "frac": traffic / avg_s / 1e9 / P["hbm_gbs"]} if traffic and avg_s > 0 else None),
                 "launches": pk_n, "avg_launch_ms": pk_ms / max(pk_n, 1),
                 "evals": evals, "kernel_share": {k: v[0] for k, v in kt.items()}}
 

@@ -102,17 +102,30 @@ def test_max_n_stop(ug, oracle):
     assert st.n == 20
 
 
-def test_group_subpath_mode(ug, oracle):
+@pytest.mark.parametrize("precision", [0, 1])
+def test_group_subpath_mode(ug, oracle, precision):
     u = ug.Universe(dim=2, T=12, seed=4, attempts=3000, group_mode=1, sub_attempts=20000,
                     round_size=1024)
-    st, _ = _check(ug, oracle, u)
+    st, _ = _check(ug, oracle, u, precision=precision)
     assert st.n_sub > 0
 
 
-def test_group_unique_mode(ug, oracle):
+@pytest.mark.parametrize("precision", [0, 1])
+def test_group_unique_mode(ug, oracle, precision):
     u = ug.Universe(dim=2, T=16, zgrid=1, excl=1, seed=8, attempts=20000, group_mode=2,
                     round_size=2048)
-    st, _ = _check(ug, oracle, u)
+    st, _ = _check(ug, oracle, u, precision=precision)
+    assert st.n_sub > 0
+
+
+@pytest.mark.parametrize("dim,T,att,mode", [(2, 256, 60000, 2), (3, 48, 40000, 2), (2, 96, 8000, 1)])
+def test_group_modes_tensor_core_path(ug, oracle, dim, T, att, mode):
+    """Group rounds through the tensor-core prefilter (certain contacts join or reject,
+    guard-band contacts go to the FP64 retest): accepted sets and group labels equal the
+    oracle's; the unique-group case at F = 256 is the shape of the c4 workload."""
+    u = ug.Universe(dim=dim, T=T, zgrid=1, excl=1, seed=5 + T, attempts=att, group_mode=mode,
+                    sub_attempts=4 * att if mode == 1 else 0, round_size=4096)
+    st, _ = _check(ug, oracle, u, precision=1)
     assert st.n_sub > 0
 
 

@@ -215,12 +215,26 @@ __device__ __forceinline__ double gen_quarter(const UniDev& d, uint64_t idx, int
 
 // ------------------------------------------------- guard-band grid test
 
+// Group round, certain contact with point p at timestep t: joins the row to the
+// point's group (*grp, shared by the row's threads).  True when the row already
+// holds a different group (two groups touched: rejected).  Out of line: it is
+// rare and keeps the neighbour scans small.
+__device__ __noinline__ bool group_contact(const UniDev& d, int32_t p, int t, int* grp) {
+    const int32_t gq = __ldg(&d.pts[UG_IDX((int64_t)p * d.T + t, d.slot_cap * d.T)].gid);
+    int cur = *(volatile int*)grp;
+    if (cur == -1) cur = atomicCAS(grp, -1, gq);
+    return cur != -1 && cur != gq;
+}
+
 // FP32 Chebyshev test of X (dim coords) at timestep t against the committed
-// packing.  Returns 1 on a certain contact; sets *gray when a pair lies in the
-// guard band.  The cell range covers every point within r + m of X.
+// packing.  Returns 1 when the candidate is certainly rejected; sets *gray when
+// a pair lies in the guard band.  The cell range covers every point within
+// r + m of X.  Group rounds (grp != nullptr): a certain contact joins the
+// candidate to the contact's group in *grp (shared by the row's threads); a
+// certain contact with a second group rejects.
 template <int D>
 __device__ __forceinline__ int test32_d(const UniDev& d, int t, const float* X, float r, float m,
-                                        float inv_cell, int64_t cpt, bool* gray) {
+                                        float inv_cell, int64_t cpt, bool* gray, int* grp) {
     const float band = m * inv_cell + 1e-4f;
     int c[D], elo[D], ehi[D];
 #pragma unroll
@@ -254,7 +268,7 @@ __device__ __forceinline__ int test32_d(const UniDev& d, int t, const float* X, 
             in &= dd < rin;
         }
         if (miss) return false;
-        if (in) return true;
+        if (in) return grp ? group_contact(d, p, t, grp) : true;
         g = true;
         return false;
     });
@@ -262,14 +276,11 @@ __device__ __forceinline__ int test32_d(const UniDev& d, int t, const float* X, 
     return deep ? 1 : 0;
 }
 
-// FP32 Chebyshev test of X at timestep t against the committed packing.
-// Returns 1 on a certain contact; sets *gray when a pair lies in the guard
-// band.  The neighbourhood covers every cell within r + m of X.
 __device__ __forceinline__ int test32_at(const UniDev& d, int t, const float* X, float r, float m,
-                                         float inv_cell, int64_t cpt, bool* gray) {
-    if (d.dim == 3) return test32_d<3>(d, t, X, r, m, inv_cell, cpt, gray);
-    if (d.dim == 2) return test32_d<2>(d, t, X, r, m, inv_cell, cpt, gray);
-    return test32_d<1>(d, t, X, r, m, inv_cell, cpt, gray);
+                                         float inv_cell, int64_t cpt, bool* gray, int* grp) {
+    if (d.dim == 3) return test32_d<3>(d, t, X, r, m, inv_cell, cpt, gray, grp);
+    if (d.dim == 2) return test32_d<2>(d, t, X, r, m, inv_cell, cpt, gray, grp);
+    return test32_d<1>(d, t, X, r, m, inv_cell, cpt, gray, grp);
 }
 
 // --------------------------------------------------------------- kernel
@@ -300,7 +311,8 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
     double* s_sum = reinterpret_cast<double*>(sm + 2 * stage_bytes);      // [kTile][kMxParts][2]
     int* s_rej = reinterpret_cast<int*>(s_sum + kTile * kMxParts * 2);   // [kTile]
     int* s_gray = s_rej + kTile;                                          // [kTile]
-    uint64_t* bar = reinterpret_cast<uint64_t*>(s_gray + kTile);
+    int* s_grp = s_gray + kTile;                                          // [kTile] group rounds
+    uint64_t* bar = reinterpret_cast<uint64_t*>(s_grp + kTile);
     uint64_t* bar_b = bar;       // [2] B chunk landed
     uint64_t* bar_m = bar + 2;   // [2] MMAs reading the stage finished
     uint64_t* bar_d = bar + 4;   // all MMAs of the pass finished
@@ -367,11 +379,15 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
         const uint32_t idesc = idesc_bf16(128, nm);
         const float r = (float)d.cell, mrg = d.mx_margin, inv_cell = (float)(1.0 / d.cell);
         const int64_t cpt = cells_per_t(d);
+        // group semantics this round (unique-group mode, or phase 2 of the subpath mode)
+        const bool group = !dump && (d.group_mode == GROUP_UNIQUE ||
+                                     (d.group_mode == GROUP_SUBPATH && ctl[u].phase == 2));
         float inv_sum[3] = {0.f, 0.f, 0.f}, a2f[3] = {0.f, 0.f, 0.f};
         float rho = 0.f;  // largest sum_b (E_b / b) / sum E over the axes
         if (part == 0) {
             s_rej[row] = valid ? 0 : 1;
             s_gray[row] = 0;
+            s_grp[row] = -1;
         }
         int nev = 0;
         for (int pass = 0; pass < d.mx_npass && !timeout; pass++) {
@@ -536,7 +552,8 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                     if (vrej[row]) break;
                     nev++;
                     bool gr = false;
-                    if (test32_at(d, t, X, r, mt, inv_cell, cpt, &gr)) vrej[row] = 1;
+                    if (test32_at(d, t, X, r, mt, inv_cell, cpt, &gr, group ? s_grp + row : nullptr))
+                        vrej[row] = 1;
                     if (gr) vgray[row] = 1;
                 }
             }
@@ -552,6 +569,7 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                 const bool gr = valid && !rej && (gry || timeout);
                 const uint32_t sb = __ballot_sync(0xffffffffu, surv);
                 const uint32_t gb = __ballot_sync(0xffffffffu, gr);
+                if (surv && d.group_mode != GROUP_NONE) d.g0[UG_IDX(off, d.B_max)] = s_grp[row];
                 if (lane == 0) {
                     d.surv_bits[UG_IDX(off >> 5, d.B_max / 32)] = sb;
                     d.gray_bits[UG_IDX(off >> 5, d.B_max / 32)] = gb;
@@ -605,7 +623,7 @@ static int g_ctas_per_sm = 1;
 
 static size_t smem_bytes() {
     return (size_t)2 * (2 * kAImgBytes + g_tpad_max * kKC * 2 * 2) + (size_t)kTile * kMxParts * 16 +
-           2 * kTile * 4 + 64;
+           3 * kTile * 4 + 64;
 }
 
 static uint16_t bf16_bits(float x) {
@@ -621,7 +639,8 @@ static float bf16_val(uint16_t b) {
 
 int mixed_setup(const ug_universe_cfg& cfg, UniDev& d, MixedTables& mt) {
     const int T = cfg.T, F = cfg.T, dim = cfg.dim;
-    d.mx_ok = (cfg.rng == UG_RNG_PHILOX && cfg.group_mode == UG_GROUP_NONE) ? 1 : 0;
+    // group rounds of the 1+1D crossing rule stay on the FP64 path
+    d.mx_ok = (cfg.rng == UG_RNG_PHILOX && !(cfg.cross1d && cfg.group_mode != UG_GROUP_NONE)) ? 1 : 0;
     const bool natural = cfg.dim == 1 && cfg.cross1d;  // the crossing test walks t in order
     const int P = F / 2;
     const int nch = (P + kPairsPerChunk - 1) / kPairsPerChunk;
