@@ -85,6 +85,7 @@ struct Batch {
     bool synced = false;
     int max_T = 0;
     bool any_mixed = false;
+    bool any_group = false;  // some universe runs group rounds
     int64_t launches = 0;  // kernels issued (graph replays count every node)
     int64_t h2d = 0, d2h = 0;  // bytes copied between host and device
     int kernels_per_round = 9;
@@ -367,7 +368,7 @@ static int launch_round(Batch& B, bool timed) {
     te(K_PLAN);
     if (B.opts.precision == UG_PREC_MIXED && B.any_mixed) {
         tb(K_MIXED);
-        launch_prefilter_mixed(B.dU, B.dCtl, B.dInfo, B.nsm, B.st);
+        launch_prefilter_mixed(B.dU, B.dCtl, B.dInfo, B.nsm, B.any_group, B.st);
         te(K_MIXED);
         tb(K_CONFIRM);
         k_gray_compact<<<B.n, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
@@ -584,6 +585,7 @@ int ug_batch_create(const ug_universe_cfg* cfgs, int32_t n, const ug_run_opts* o
             if ((rc = mixed_setup(B->U[i].cfg, B->U[i].d, B->U[i].mt))) return bail(rc);
             B->any_mixed = true;
         }
+        if (cfgs[i].group_mode != UG_GROUP_NONE) B->any_group = true;
     }
     if (cudaMalloc(&B->dU, sizeof(UniDev) * n) != cudaSuccess ||
         cudaMalloc(&B->dCtl, sizeof(UniCtl) * n) != cudaSuccess ||

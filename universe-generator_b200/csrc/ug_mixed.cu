@@ -299,6 +299,9 @@ struct MixedLaunch {
 constexpr int kMxThreads = 512;  // 4 threads per candidate row
 constexpr int kMxParts = kMxThreads / kTile;
 
+// kGroup: the batch holds group-mode universes (group rounds need the join /
+// two-group logic in the neighbour scans; batches without them run without it).
+template <bool kGroup>
 __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev* __restrict__ U, UniCtl* ctl,
                                                                     RoundInfo* info, MixedLaunch L) {
     extern __shared__ __align__(1024) uint8_t sm[];
@@ -380,8 +383,8 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
         const float r = (float)d.cell, mrg = d.mx_margin, inv_cell = (float)(1.0 / d.cell);
         const int64_t cpt = cells_per_t(d);
         // group semantics this round (unique-group mode, or phase 2 of the subpath mode)
-        const bool group = !dump && (d.group_mode == GROUP_UNIQUE ||
-                                     (d.group_mode == GROUP_SUBPATH && ctl[u].phase == 2));
+        const bool group = kGroup && !dump &&
+                           (d.group_mode == GROUP_UNIQUE || (d.group_mode == GROUP_SUBPATH && ctl[u].phase == 2));
         float inv_sum[3] = {0.f, 0.f, 0.f}, a2f[3] = {0.f, 0.f, 0.f};
         float rho = 0.f;  // largest sum_b (E_b / b) / sum E over the axes
         if (part == 0) {
@@ -552,7 +555,7 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                     if (vrej[row]) break;
                     nev++;
                     bool gr = false;
-                    if (test32_at(d, t, X, r, mt, inv_cell, cpt, &gr, group ? s_grp + row : nullptr))
+                    if (test32_at(d, t, X, r, mt, inv_cell, cpt, &gr, (kGroup && group) ? s_grp + row : nullptr))
                         vrej[row] = 1;
                     if (gr) vgray[row] = 1;
                 }
@@ -569,7 +572,7 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                 const bool gr = valid && !rej && (gry || timeout);
                 const uint32_t sb = __ballot_sync(0xffffffffu, surv);
                 const uint32_t gb = __ballot_sync(0xffffffffu, gr);
-                if (surv && d.group_mode != GROUP_NONE) d.g0[UG_IDX(off, d.B_max)] = s_grp[row];
+                if (kGroup && surv && d.group_mode != GROUP_NONE) d.g0[UG_IDX(off, d.B_max)] = s_grp[row];
                 if (lane == 0) {
                     d.surv_bits[UG_IDX(off >> 5, d.B_max / 32)] = sb;
                     d.gray_bits[UG_IDX(off >> 5, d.B_max / 32)] = gb;
@@ -762,15 +765,21 @@ int mixed_init_kernels() {
     if (fit > by_tmem) req = smem_sm / (by_tmem + 1) - per_cta_reserved + 16;
     g_smem = std::max(req, g_smem);
     g_ctas_per_sm = std::max(1, std::min(by_tmem, (int)(smem_sm / (g_smem + per_cta_reserved))));
-    if (cudaFuncSetAttribute(k_prefilter_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g_smem) !=
-        cudaSuccess)
+    if (cudaFuncSetAttribute(k_prefilter_mixed<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)g_smem) != cudaSuccess ||
+        cudaFuncSetAttribute(k_prefilter_mixed<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)g_smem) != cudaSuccess)
         return UG_ECUDA;
     return UG_OK;
 }
 
-void launch_prefilter_mixed(const UniDev* dU, UniCtl* dCtl, RoundInfo* dInfo, int nsm, cudaStream_t st) {
+void launch_prefilter_mixed(const UniDev* dU, UniCtl* dCtl, RoundInfo* dInfo, int nsm, bool any_group,
+                            cudaStream_t st) {
     MixedLaunch L{(uint32_t)g_ncols, g_tpad_max, nullptr, nullptr, 0, 0, 0};
-    k_prefilter_mixed<<<nsm * g_ctas_per_sm, kMxThreads, g_smem, st>>>(dU, dCtl, dInfo, L);
+    if (any_group)
+        k_prefilter_mixed<true><<<nsm * g_ctas_per_sm, kMxThreads, g_smem, st>>>(dU, dCtl, dInfo, L);
+    else
+        k_prefilter_mixed<false><<<nsm * g_ctas_per_sm, kMxThreads, g_smem, st>>>(dU, dCtl, dInfo, L);
 }
 
 int mixed_error(const UniDev* dU, int u, const UniDev& d, const MixedTables& mt, int64_t first, int64_t count,
@@ -791,7 +800,7 @@ int mixed_error(const UniDev* dU, int u, const UniDev& d, const MixedTables& mt,
     MixedLaunch L{(uint32_t)g_ncols, g_tpad_max, d32, dm, u, first, count};
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
-    k_prefilter_mixed<<<nsm * g_ctas_per_sm, kMxThreads, g_smem, st>>>(dU, nullptr, nullptr, L);
+    k_prefilter_mixed<false><<<nsm * g_ctas_per_sm, kMxThreads, g_smem, st>>>(dU, nullptr, nullptr, L);
     k_pos64<<<(int)std::min<int64_t>((count + 127) / 128, 2048), 128, 0, st>>>(dU, u, first, count, d64);
     std::vector<float> h32(n), hm(nm);
     std::vector<double> h64(n);
