@@ -66,6 +66,8 @@ typedef struct ug_universe_cfg {
     int64_t sub_attempts; /* --sub-attempts (0 = same as attempts) */
     double accept_rate;   /* --until-accept-rate (0 = off), braid_cuda.cu:931-943 */
     double sub_accept_rate;
+    double sub_fill_rate; /* --sub-until-fill-rate: phase-2 stop on windowed newly occupied
+                             grid cells per attempt (0 = off), braid_cuda.cu:960-1035 */
 } ug_universe_cfg;
 
 typedef struct ug_run_opts {
@@ -93,6 +95,8 @@ typedef struct ug_stats {
     int64_t evals_fp64; /* of which in FP64 */
     int32_t state;      /* 1 = done */
     int32_t grid_kind;  /* 0 dense, 1 hash */
+    int64_t filled;     /* occupied (timestep, cell) buckets of the collision grid
+                           (the `filled` of braid_cuda.cu:695, 877) */
 } ug_stats;
 
 /* Per-kernel device time accumulated while kernel_timing is on. */

@@ -87,7 +87,7 @@ def test_mirror_identities():
 @pytest.mark.parametrize("argv,msg", [
     (["--smart"], "--smart"), (["-t", "16", "--maxfreq", "12"], "maxfreq"),
     (["--bogus"], "unknown flag"), (["--euclid-collision"], "L2"),
-    (["--sub-until-fill-rate", "1e-6"], "fill-rate"), (["-t"], "needs a value"),
+    (["--nu-attempts", "10"], "nu"), (["-t"], "needs a value"),
 ])
 def test_cli_rejects_bad_flags_before_any_device_work(argv, msg):
     r = subprocess.run([sys.executable, os.path.join(PKG, "bin", "braid_cuda"), *argv],

@@ -70,3 +70,18 @@ def test_braid_cuda_subpaths_curve_columns(tmp_path):
     assert lines[0] == "attempts,n,nsub,filled"
     last = [int(v) for v in lines[-1].split(",")]
     assert last[0] == 23000 and last[2] > 0 and last[3] > 0
+    # the done lines carry the occupied cells as braid_cuda.cu:945 and :1039-1042 print them
+    assert ", filled " in r.stderr and "sub done (attempt budget): Nsub=" in r.stderr
+    assert f"filled {last[3]}/" in r.stderr.split("sub done")[1]
+
+
+def test_braid_cuda_sub_until_fill_rate(tmp_path):
+    """--sub-until-fill-rate stops phase 2 on the windowed new-volume rate (windows of at
+    least 2e7 attempts, after 1e6 phase-2 attempts, braid_cuda.cu:1024-1035)."""
+    r = _run("braid_cuda", ["-t", "24", "--excl", "open", "--zgrid", "mid", "--seed", "4",
+                            "--attempts", "20000", "--terms", "24", "--subpaths",
+                            "--sub-attempts", "60000000", "--sub-until-fill-rate", "5e-4"])
+    assert r.returncode == 0, r.stderr
+    assert "sub done (fill-rate): Nsub=" in r.stderr
+    sub_att = int(r.stderr.split("sub done (fill-rate): Nsub=")[1].split(" in ")[1].split()[0])
+    assert 20_000_000 <= sub_att < 60_000_000

@@ -93,7 +93,10 @@ def test_brf1_round_trip_and_density(ug, tmp_path):
         h = bk.hits[fi][0]
         cx = np.floor((h["dx"].astype(np.float32) + np.float32(chi_max)) * np.float32(bins / (2 * chi_max)))
         cy = np.floor((h["dy"].astype(np.float32) + np.float32(chi_max)) * np.float32(bins / (2 * chi_max)))
-        ok = (cx >= 0) & (cy >= 0) & (cx < bins) & (cy < bins)
+        # closed square: an offset rounded a hair past an edge counts in the edge bin
+        cx = np.clip(cx, 0, bins - 1).astype(int)
+        cy = np.clip(cy, 0, bins - 1).astype(int)
         ref = np.zeros((bins, bins), np.uint32)
-        np.add.at(ref, (cy[ok].astype(int), cx[ok].astype(int)), 1)
+        np.add.at(ref, (cy, cx), 1)
         assert np.array_equal(bk.density[fi, 0], ref)
+        assert int(bk.density[fi, 0].sum()) == len(h)

@@ -181,3 +181,41 @@ def test_seam_blocks_when_cells_are_not_a_multiple_of_eight(ug, oracle, precisio
                 p.run()
                 idx, _ = p.accepted(0)
             assert np.array_equal(idx, ref.acc_idx), (dim, seed)
+
+
+@pytest.mark.parametrize("dim,T,excl,mode,prec,hashed", [(2, 16, 0, 0, 0, False), (2, 24, 1, 1, 1, False),
+                                                         (3, 20, 1, 0, 1, True), (3, 32, 0, 2, 0, True),
+                                                         (1, 40, 1, 0, 1, False)])
+def test_filled_cells_count(ug, dim, T, excl, mode, prec, hashed):
+    """The device count of occupied (timestep, cell) buckets equals the count from the
+    accepted trajectories (the `filled` of braid_cuda.cu:695, 865-879)."""
+    from ugb200.cli import filled_cells
+    u = ug.Universe(dim=dim, T=T, zgrid=1, excl=excl, seed=3 + T, attempts=20000, group_mode=mode,
+                    sub_attempts=20000 if mode == 1 else 0, round_size=2048)
+    with ug.Packer([u], precision=prec, force_hash=hashed) as p:
+        p.run()
+        st = p.stats(0)
+        pos = p.positions(0)
+    cell = 2.0 / T if excl == 0 else 1.0 / T
+    assert st.n > 0 and st.filled == int(filled_cells(pos, cell)[-1])
+
+
+def test_sub_fill_rate_stop_is_a_prefix(ug):
+    """A phase 2 ended by the new-volume stop admits exactly what a budget-limited run to
+    the same attempt count admits (same candidate stream, in-order resolution)."""
+    kw = dict(dim=2, T=24, zgrid=1, excl=1, seed=4, attempts=20000, group_mode=1, round_size=65536)
+    u = ug.Universe(**kw, sub_attempts=60_000_000, sub_fill_rate=5e-4)
+    with ug.Packer([u], precision=1) as p:
+        p.run()
+        st = p.stats(0)
+        a, g = p.accepted(0)
+    sub = st.attempts - st.phase1_end
+    assert 20_000_000 <= sub < 60_000_000
+    v = ug.Universe(**kw, sub_attempts=sub)
+    with ug.Packer([v], precision=1) as p:
+        p.run()
+        st2 = p.stats(0)
+        b, h = p.accepted(0)
+    assert st2.attempts == st.attempts
+    assert np.array_equal(a, b) and np.array_equal(g, h)
+    assert st2.filled == st.filled

@@ -180,6 +180,16 @@ struct UniCtl {
     int32_t win_head, win_len;
     int64_t win_b[64];
     int64_t win_a[64];
+    // occupied (timestep, cell) buckets and the windowed new-volume stop of
+    // phase 2 (braid_cuda.cu:960-1035): newly occupied cells per attempt
+    int64_t filled;         // occupied cells so far
+    int64_t round_new;      // cells first occupied by this round's commit
+    int64_t last_used;      // candidates decided by the last round
+    double sub_fill_rate;   // threshold (0 = off)
+    int64_t fwin_target, fwin_att, fwin_new;
+    int32_t fwin_head, fwin_len;
+    int64_t fwin_b[64];
+    int64_t fwin_n[64];
 };
 
 // ------------------------------------------------------------------ helpers

@@ -186,7 +186,9 @@ __global__ void k_fb_hits(FPaths P, FFront F, double ox, double oy, int K, int o
     }
 }
 
-// Density scatter: hit offsets binned over [-chi_max, chi_max]^2.
+// Density scatter: hit offsets binned over the closed square [-chi_max, chi_max]^2.
+// Every hit lies on a front of radius chi <= chi_max, so every hit is counted:
+// an offset that FP32 rounding puts a hair past an edge goes to the edge bin.
 __global__ void k_fb_density(const ug_hit* hits, int64_t n, double chiMax, int bins, uint32_t* grid) {
     const float inv = (float)(bins / (2.0 * chiMax));
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -194,7 +196,8 @@ __global__ void k_fb_density(const ug_hit* hits, int64_t n, double chiMax, int b
         const ug_hit h = hits[i];
         int cx = (int)floorf((h.dx + (float)chiMax) * inv);
         int cy = (int)floorf((h.dy + (float)chiMax) * inv);
-        if (cx < 0 || cy < 0 || cx >= bins || cy >= bins) continue;
+        cx = cx < 0 ? 0 : (cx >= bins ? bins - 1 : cx);
+        cy = cy < 0 ? 0 : (cy >= bins ? bins - 1 : cy);
         atomicAdd(&grid[(size_t)cy * bins + cx], 1u);
     }
 }

@@ -335,6 +335,8 @@ static void init_ctl(const ug_universe_cfg& c, const UniDev& d, UniCtl& k) {
     k.accept_rate = c.accept_rate;
     k.sub_accept_rate = c.sub_accept_rate;
     k.win_target = c.accept_rate > 0 ? (int64_t)std::min(5e9, std::max(2e7, 30.0 / c.accept_rate)) : 0;
+    k.sub_fill_rate = c.sub_fill_rate;
+    k.fwin_target = 0;  // armed when phase 2 starts
 }
 
 static int push_unidev(Batch& B) {
@@ -700,6 +702,7 @@ int ug_batch_stats(void* h, int32_t u, ug_stats* out) {
     out->evals_fp64 = k.evals_fp64;
     out->state = k.state;
     out->grid_kind = B->U[u].d.grid_kind;
+    out->filled = k.filled + k.round_new;
     return UG_OK;
 }
 

@@ -32,6 +32,43 @@ __global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* inf
         UniCtl& c = ctl[u];
         const UniDev& d = U[u];
         int B = 0;
+        // the last round's newly occupied cells (counted by k_commit); in phase 2
+        // they feed the windowed new-volume stop (braid_cuda.cu:1024-1035)
+        {
+            const int64_t nc = c.round_new;
+            c.round_new = 0;
+            c.filled += nc;
+            if (c.phase == 2 && c.fwin_target > 0 && c.last_used > 0 && c.state == ST_ACTIVE) {
+                const int64_t bucket = c.fwin_target / 32 > 0 ? c.fwin_target / 32 : 1;
+                int last = (c.fwin_head + c.fwin_len - 1) & 63;
+                if (c.fwin_len == 0 || c.fwin_b[last] >= bucket) {
+                    if (c.fwin_len == 64) {
+                        c.fwin_att -= c.fwin_b[c.fwin_head];
+                        c.fwin_new -= c.fwin_n[c.fwin_head];
+                        c.fwin_head = (c.fwin_head + 1) & 63;
+                        c.fwin_len--;
+                    }
+                    last = (c.fwin_head + c.fwin_len) & 63;
+                    c.fwin_b[last] = 0;
+                    c.fwin_n[last] = 0;
+                    c.fwin_len++;
+                }
+                c.fwin_b[last] += c.last_used;
+                c.fwin_n[last] += nc;
+                c.fwin_att += c.last_used;
+                c.fwin_new += nc;
+                while (c.fwin_len > 1 && c.fwin_att - c.fwin_b[c.fwin_head] >= c.fwin_target) {
+                    c.fwin_att -= c.fwin_b[c.fwin_head];
+                    c.fwin_new -= c.fwin_n[c.fwin_head];
+                    c.fwin_head = (c.fwin_head + 1) & 63;
+                    c.fwin_len--;
+                }
+                if (c.fwin_att >= c.fwin_target && c.next_cand - c.phase1_end > 1000000 &&
+                    (double)c.fwin_new / (double)c.fwin_att < c.sub_fill_rate)
+                    c.phase_end = c.next_cand;  // stops below
+            }
+            c.last_used = 0;
+        }
         if (c.state == ST_ACTIVE) {
             for (int guard = 0; guard < 2; guard++) {
                 const bool over = c.next_cand >= c.phase_end ||
@@ -47,6 +84,11 @@ __global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* inf
                     c.win_target = c.sub_accept_rate > 0
                                        ? (int64_t)fmin(5e9, fmax(2e7, 30.0 / c.sub_accept_rate))
                                        : 0;
+                    c.fwin_att = c.fwin_new = 0;
+                    c.fwin_head = c.fwin_len = 0;
+                    c.fwin_target = c.sub_fill_rate > 0
+                                        ? (int64_t)fmin(5e9, fmax(2e7, 30.0 / c.sub_fill_rate))
+                                        : 0;
                     continue;
                 }
                 c.state = ST_DONE;
@@ -651,8 +693,6 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
         const UniDev& d = U[u];
         UniCtl& c = ctl[u];
         const int T = d.T;
-        // survivors past a truncation point are re-proposed next round: skip them
-        if (r > *(volatile const int32_t*)&c.trunc) continue;
         if (lane == 0) *cnt = 0;
         __syncwarp();
         auto add = [&](int32_t r2) {
@@ -715,13 +755,13 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
             }
         }
         __syncwarp();
+        // more than kConflictCap contacts: the list keeps kConflictCap of them and the
+        // count says so; the resolver rejects on any admitted one and otherwise stops
+        // the round at this survivor
         const int n = *cnt;
-        if (n > kConflictCap) {
-            if (lane == 0) atomicMin(&c.trunc, r);
-        } else {
-            for (int i = lane; i < n; i += 32) d.clist[UG_IDX((int64_t)r * kConflictCap + i, (int64_t)d.S_max * kConflictCap)] = lst[i];
-            if (lane == 0) d.ccount[UG_IDX(r, d.S_max)] = n;
-        }
+        const int ns = n < kConflictCap ? n : kConflictCap;
+        for (int i = lane; i < ns; i += 32) d.clist[UG_IDX((int64_t)r * kConflictCap + i, (int64_t)d.S_max * kConflictCap)] = lst[i];
+        if (lane == 0) d.ccount[UG_IDX(r, d.S_max)] = n;
         __syncwarp();
     }
 }
@@ -747,14 +787,16 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
     const int64_t room = d.slot_cap - c.n_slots;
     int k = 0, stop_at = S_eff;
     int64_t n_unique = c.n_unique, n_sub = c.n_sub;
-    bool grow = false, hit_max = false;
+    bool grow = false, hit_max = false, undecided = false;
     for (int r = 0; r < S_eff; r++) {
         if (k >= room) {
             stop_at = r;
             grow = true;
             break;
         }
-        const int n = d.ccount[UG_IDX(r, d.S_max)];
+        const int n_all = d.ccount[UG_IDX(r, d.S_max)];
+        const bool over = n_all > kConflictCap;  // the list holds only kConflictCap contacts
+        const int n = over ? kConflictCap : n_all;
         const int32_t* lst = d.clist + UG_IDX((int64_t)r * kConflictCap, (int64_t)d.S_max * kConflictCap);
         bool accept;
         int32_t gid;
@@ -762,6 +804,11 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
             bool any = false;
             for (int i = lane; i < n; i += 32) any |= acc_s[UG_IDX(lst[i], kSmaxCap)] >= 0;
             accept = !__any_sync(0xffffffffu, any);
+            if (accept && over) {  // an unlisted contact might be admitted: decide next round
+                stop_at = r;
+                undecided = true;
+                break;
+            }
             gid = (int32_t)(c.n_slots + k);
         } else {
             // union of the pre-round group and the groups of admitted earlier survivors
@@ -785,6 +832,11 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
             }
             two = two || (mine != -1 && mine != first);
             two = __any_sync(0xffffffffu, two);
+            if (!two && over) {  // unlisted contacts might add a group: decide next round
+                stop_at = r;
+                undecided = true;
+                break;
+            }
             if (two) {
                 accept = false;
                 gid = -1;
@@ -835,13 +887,16 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
     c.accepted_round = k;
     c.next_cand = next;
     c.attempts = next;
+    c.last_used = used;
     c.rounds++;
     if (grow) c.state = ST_GROW;
     // round-size adaptation (the reference steers toward 64..512 survivors for
     // its serial host admission, braid_cuda.cu:921-924; the device resolver
     // takes up to S_max, so steer toward the survivor capacity instead).
     // Admission results do not depend on it.
-    if (c.S_raw > d.S_max && c.round_B > c.B_min)
+    if (undecided && c.round_B > kTile)  // crowded in-round contacts: smaller rounds
+        c.round_B = max(c.round_B >> 1, kTile);
+    else if (c.S_raw > d.S_max && c.round_B > c.B_min)
         c.round_B = max(c.round_B >> 1, c.B_min);
     else if (c.S_raw < d.S_max / 4 && c.round_B < c.B_cap)
         c.round_B = min(c.round_B << 1, c.B_cap);
@@ -931,7 +986,7 @@ __global__ void __launch_bounds__(256) k_commit(const UniDev* __restrict__ U, Un
     for (int w0 = blockIdx.x * blockDim.x; w0 < total; w0 += gridDim.x * blockDim.x) {
         const int w = w0 + threadIdx.x;
         int u = -1;
-        bool new_key = false;
+        bool new_key = false, new_cell = false;
         if (w < total) {
             u = find_uni(info->spt_off, n_uni, w);
             const UniDev& d = U[u];
@@ -946,6 +1001,7 @@ __global__ void __launch_bounds__(256) k_commit(const UniDev* __restrict__ U, Un
                 for (int ax = 0; ax < d.dim; ax++) cc[ax] = cell_of(q.c[ax], d.cell, d.gw);
                 int32_t old;
                 grid_insert(d, c, t, lin_cell(cc, d.dim, d.gw), cells_per_t(d), (int32_t)slot, &old, &new_key);
+                new_cell = old < 0;
                 occ_set(d.occ, occ_bit(d, t, cc), d.occ_words);
                 occ_set(d.occ1, occ1_bit(d, t, cc), d.occ1_words);
                 q.next = old;
@@ -961,12 +1017,16 @@ __global__ void __launch_bounds__(256) k_commit(const UniDev* __restrict__ U, Un
                     d.acc_idx[UG_IDX(slot, d.slot_cap)] = c.round_base + d.surv_off[UG_IDX(r, d.S_max + 1)];
             }
         }
-        // new hash keys: one atomic per (warp, universe) instead of one per key
+        // new hash keys and newly occupied cells: one atomic per (warp, universe)
         const uint32_t nk = __ballot_sync(0xffffffffu, new_key);
-        if (nk) {
-            const uint32_t mine = nk & __match_any_sync(0xffffffffu, u);
+        const uint32_t ncl = __ballot_sync(0xffffffffu, new_cell);
+        if (nk | ncl) {
+            const uint32_t peers = __match_any_sync(0xffffffffu, u);
+            const uint32_t mine = nk & peers, minec = ncl & peers;
             if (new_key && lane == __ffs(mine) - 1)
                 atomicAdd((unsigned long long*)&ctl[u].hash_used, (unsigned long long)__popc(mine));
+            if (new_cell && lane == __ffs(minec) - 1)
+                atomicAdd((unsigned long long*)&ctl[u].round_new, (unsigned long long)__popc(minec));
         }
     }
 }

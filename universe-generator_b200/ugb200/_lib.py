@@ -37,7 +37,7 @@ class UniverseCfg(C.Structure):
         ("pin_sin1", C.c_int32), ("group_mode", C.c_int32), ("round_size", C.c_int32),
         ("seed", C.c_uint64), ("attempts", C.c_int64), ("max_n", C.c_int64),
         ("sub_attempts", C.c_int64), ("accept_rate", C.c_double),
-        ("sub_accept_rate", C.c_double),
+        ("sub_accept_rate", C.c_double), ("sub_fill_rate", C.c_double),
     ]
 
 
@@ -54,7 +54,7 @@ class Stats(C.Structure):
         ("n", C.c_int64), ("n_unique", C.c_int64), ("n_sub", C.c_int64),
         ("attempts", C.c_int64), ("phase1_end", C.c_int64), ("rounds", C.c_int64),
         ("gray", C.c_int64), ("evals", C.c_int64), ("evals_fp64", C.c_int64),
-        ("state", C.c_int32), ("grid_kind", C.c_int32),
+        ("state", C.c_int32), ("grid_kind", C.c_int32), ("filled", C.c_int64),
     ]
 
 

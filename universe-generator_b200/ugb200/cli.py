@@ -32,7 +32,6 @@ UNSUPPORTED = {
     "--angle-sample": "--angle-sample is not built",
     "--diag": "--diag probes are not built",
     "--probe-n": "--diag probes are not built",
-    "--sub-until-fill-rate": "--sub-until-fill-rate is not built",
     "--nu-attempts": "the second (nu) species of braid_knot is not built",
     "--nu-div": "the second (nu) species of braid_knot is not built",
 }
@@ -80,7 +79,7 @@ def main(argv: list[str] | None = None, engine: str | None = None) -> int:
     terms = 0 if knot else 2
     curve = dump = None
     maxfreq = 0
-    accept = sub_accept = 0.0
+    accept = sub_accept = sub_fill = 0.0
     pin = subpaths = False
     sub_budget = 0.0
     sub_terms = 0
@@ -125,6 +124,8 @@ def main(argv: list[str] | None = None, engine: str | None = None) -> int:
                 sub_budget = float(val())
             elif a == "--sub-until-accept-rate":
                 sub_accept = float(val())
+            elif a == "--sub-until-fill-rate":
+                sub_fill = float(val())
             elif a == "--sub-terms":
                 sub_terms = int(val())
             elif a == "--max-n":
@@ -163,7 +164,8 @@ def main(argv: list[str] | None = None, engine: str | None = None) -> int:
     u = Universe(dim=dim, T=T, terms=0 if terms == T else terms, rng=rng, zgrid=zgrid,
                  excl=excl, pin_sin1=int(pin), group_mode=L.GROUP_SUBPATH if subpaths else 0,
                  round_size=round_size, seed=seed, attempts=int(budget), max_n=max_n,
-                 sub_attempts=int(sub_budget), accept_rate=accept, sub_accept_rate=sub_accept)
+                 sub_attempts=int(sub_budget), accept_rate=accept, sub_accept_rate=sub_accept,
+                 sub_fill_rate=sub_fill)
     kind = {2: "2+1", 3: "3+1", 1: "1+1"}[dim]
     print(f"{kind} (torus, phase): T={T}  modmax={max(T - 1, 2)} (maxfreq={max(T - 1, 2) + 1})  "
           f"terms={terms}  rng={'knot' if rng == L.RNG_KNOT else 'philox'}", file=sys.stderr)
@@ -173,17 +175,35 @@ def main(argv: list[str] | None = None, engine: str | None = None) -> int:
         st = p.stats(0)
         idx, gid = p.accepted(0)
         params = p.params(0) if dump else None
-        pos = p.positions(0) if (subpaths and curve) else None
+        pos = p.positions(0) if subpaths else None
         p.close()
     except L.UgError as e:
         return _die(str(e))
+    cell = 2.0 / T if excl == L.EXCL_REF else 1.0 / T
+    ncell = T * int(round(2.0 / cell)) ** dim
+    filled = filled_cells(pos, cell) if subpaths else None
     if knot:
         print(f"done: N={st.n} (primary {st.n}, nu 0) in {st.attempts} attempts", file=sys.stderr)
-    else:
+    elif base == "braid_cuda3d":
         print(f"done: N={st.n_unique} in {st.phase1_end} attempts", file=sys.stderr)
-        if subpaths:
-            print(f"sub done: Nsub={st.n_sub} in {st.attempts - st.phase1_end} attempts",
-                  file=sys.stderr)
+    else:
+        # braid_cuda.cu:945 -- the 2+1 engine also reports the occupied grid cells
+        k1 = int(np.count_nonzero(idx < st.phase1_end))
+        f1 = (int(filled[k1 - 1]) if k1 else 0) if subpaths else st.filled
+        print(f"done: N={st.n_unique} in {st.phase1_end} attempts, filled {f1}/{ncell} cells "
+              f"({100.0 * f1 / ncell:.3f}%)", file=sys.stderr)
+    if subpaths:
+        sub_att = st.attempts - st.phase1_end
+        if sub_att >= (int(sub_budget) if sub_budget > 0 else int(budget)):
+            why = "attempt budget"
+        elif sub_fill > 0 and sub_accept <= 0:
+            why = "fill-rate"
+        elif sub_accept > 0 and sub_fill <= 0:
+            why = "accept-rate"
+        else:
+            why = "accept-rate or fill-rate"
+        print(f"sub done ({why}): Nsub={st.n_sub} in {sub_att} attempts, filled {st.filled}/{ncell} "
+              f"cells ({100.0 * st.filled / ncell:.3f}%)", file=sys.stderr)
     if curve:
         if knot:
             with open(curve, "w") as f:
@@ -192,7 +212,6 @@ def main(argv: list[str] | None = None, engine: str | None = None) -> int:
                     f.write(f"{int(ix) + 1},{k + 1},0\n")
         else:
             uniq = (gid == np.arange(len(gid))) if subpaths else None
-            filled = filled_cells(pos, 2.0 / T if excl == L.EXCL_REF else 1.0 / T) if subpaths else None
             write_curve(curve, curve_rows(idx, st.attempts, n_unique_mask=uniq, filled=filled),
                         subpaths=subpaths)
     if dump:

@@ -34,6 +34,7 @@ class Universe:
     sub_attempts: int = 0
     accept_rate: float = 0.0
     sub_accept_rate: float = 0.0
+    sub_fill_rate: float = 0.0     # --sub-until-fill-rate (newly occupied cells per attempt)
 
     @property
     def nw(self) -> int:
@@ -44,7 +45,7 @@ class Universe:
                              self.cross1d, self.pin_sin1, self.group_mode, self.round_size,
                              self.seed & (2**64 - 1), int(self.attempts), int(self.max_n),
                              int(self.sub_attempts), float(self.accept_rate),
-                             float(self.sub_accept_rate))
+                             float(self.sub_accept_rate), float(self.sub_fill_rate))
 
 
 @dataclass
@@ -60,6 +61,7 @@ class Stats:
     evals_fp64: int
     done: bool
     grid: str
+    filled: int = 0              # occupied (timestep, cell) buckets of the collision grid
 
 
 @dataclass
@@ -113,7 +115,8 @@ class Packer:
         s = L.Stats()
         L.check(L.load().ug_batch_stats(self._h, u, C.byref(s)))
         return Stats(s.n, s.n_unique, s.n_sub, s.attempts, s.phase1_end, s.rounds, s.gray,
-                     s.evals, s.evals_fp64, s.state == 1, "hash" if s.grid_kind else "dense")
+                     s.evals, s.evals_fp64, s.state == 1, "hash" if s.grid_kind else "dense",
+                     s.filled)
 
     def accepted(self, u: int = 0) -> tuple[np.ndarray, np.ndarray]:
         lib = L.load()
