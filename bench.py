@@ -143,23 +143,24 @@ def cpu_baseline(us, budget_s: float = 20.0):
                       f"{secs:.1f} s; oracle threaded prefilter + in-order recheck"}
 
 
-def frames_line(par):
+def frames_line(packer):
     """c4's second stage: frame_bake of the packed universe (last timed job), 256 instants
     z_obs in [0.25, 0.75] pi, one path observer, the 'fit' front, a 1024 x 1024 uint32
-    density grid per frame.  Timed end to end through ugb200.frames.bake (dump arrays in
-    host memory, hits and densities back in host memory)."""
+    density grid per frame.  Timed end to end through ugb200.frames.bake_packed: the
+    paths stay on the device, the 1 GiB of densities comes back to host memory."""
     from ugb200 import frames as FR
 
     kw = dict(observers=[("path", 0)], from_pi=0.25, to_pi=0.75, frames=256, front="fit",
-              density_bins=1024, hit_cap=1 << 24)
-    FR.bake(par["a2"], par["a"], par["b"], par["f"], **{**kw, "frames": 2})  # warm-up
+              density_bins=1024, hits=False)
+    FR.bake_packed(packer, 0, **{**kw, "frames": 2})  # warm-up
     t0 = time.perf_counter()
-    bk = FR.bake(par["a2"], par["a"], par["b"], par["f"], **kw)
+    bk = FR.bake_packed(packer, 0, **kw)
     dt = time.perf_counter() - t0
-    hits = int(sum(len(h) for fr in bk.hits for h in fr))
-    return {"frames_per_s": 256 / dt, "ms": dt * 1e3, "paths": int(len(par["a2"])), "hits": hits,
-            "density_sum": int(bk.density.sum()), "density_bytes": int(bk.density.nbytes),
-            "sample": "256 frames, z_obs 0.25..0.75 pi, 1 path observer, fit front, 1024^2 density"}
+    return {"frames_per_s": 256 / dt, "ms": dt * 1e3, "paths": int(packer.stats(0).n),
+            "hits": int(bk.counts.sum()), "density_sum": int(bk.density.sum()),
+            "density_bytes": int(bk.density.nbytes),
+            "sample": "256 frames, z_obs 0.25..0.75 pi, 1 path observer, fit front, 1024^2 density; "
+                      "device-resident paths, densities copied to host"}
 
 
 def reference_arm(args, rank, world):
@@ -315,7 +316,7 @@ def main() -> int:
     sample = list(range(0, len(us), 8)) if len(us) > 1 else [0]
     last_seeds = seeds(args.warmup + args.steps - 1)
     acc_batched = {k: packer.accepted(k)[0] for k in sample}
-    frame_par = packer.params(0) if args.workload == "c4" else None
+    frames = frames_line(packer) if (args.workload == "c4" and rank == 0) else None
     if sampler:
         sampler.terminate()
         sampler.wait()
@@ -408,7 +409,7 @@ def main() -> int:
                            "parallelism": f"replicas x{world}"},
                 "e2e": e2e, "gpu_launches": launches,
                 "roofline": roofline, "fp64_plain_single_universe": fp64_plain,
-                "frames": frames_line(frame_par) if frame_par is not None else None,
+                "frames": frames,
                 "clocks": clocks_summary(clk_path)}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(us)

@@ -227,6 +227,13 @@ typedef struct ug_frames_out {
 int ug_frame_bake(const ug_frames_cfg* cfg, int32_t n, int32_t nw, const double* a2, const double* a,
                   const double* b, const double* f, ug_frames_out* out);
 
+/* Bake frames of the accepted paths of universe u of a batch (2+1) straight from
+ * the device: the packer's parameters never leave the GPU (the reference's
+ * dump CSV -> frame_bake pipeline, frame_bake.cu:398-635, without the file).
+ * Path p of the frames is the p-th admission (the dump row order).  With
+ * out->hits == NULL only hit counts and densities come back. */
+int ug_batch_frames(void* h, int32_t u, const ug_frames_cfg* cfg, ug_frames_out* out);
+
 /* ---- single-universe convenience: a batch of one (the ug_pack_* surface) */
 int ug_pack_create(const ug_universe_cfg* cfg, const ug_run_opts* opts, void** out);
 int ug_pack_run(void* h);

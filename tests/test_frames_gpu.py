@@ -100,3 +100,33 @@ def test_brf1_round_trip_and_density(ug, tmp_path):
         np.add.at(ref, (cy, cx), 1)
         assert np.array_equal(bk.density[fi, 0], ref)
         assert int(bk.density[fi, 0].sum()) == len(h)
+
+
+def test_device_pipeline_equals_host_arrays(ug):
+    """Frames baked from the packer's device-resident paths equal frames baked from the
+    same paths' dump arrays; the density-only mode returns the same counts and grids."""
+    from ugb200.frames import bake, bake_packed
+    u = ug.Universe(dim=2, T=32, zgrid=1, excl=1, seed=9, attempts=30000, round_size=4096)
+    kw = dict(observers=[("path", 3), ("point", 0.1, -0.2)], from_pi=0.3, to_pi=0.7, frames=5,
+              zmin_pi=0.02, front="fit", density_bins=128)
+    with ug.Packer([u], precision=ug.PREC_MIXED) as p:
+        p.run()
+        par = p.params(0)
+        dev = bake_packed(p, 0, **kw)
+        dev_d = bake_packed(p, 0, hits=False, **kw)
+    host = bake(par["a2"], par["a"], par["b"], par["f"], **kw)
+    host_d = bake(par["a2"], par["a"], par["b"], par["f"], hits=False, **kw)
+    assert dev.n_paths == host.n_paths == len(par["a2"])
+    np.testing.assert_array_equal(dev.frame_meta, host.frame_meta)
+    np.testing.assert_array_equal(dev.obs_meta, host.obs_meta)
+    order = ["chi", "src", "dx", "dy", "z_emit"]  # (chi, src) ties come in device order
+    for fi in range(5):
+        for o in range(2):
+            x, y = np.sort(dev.hits[fi][o], order=order), np.sort(host.hits[fi][o], order=order)
+            assert len(x) == len(y) == dev_d.counts[fi, o] == host_d.counts[fi, o]
+            diff = np.nonzero(x != y)[0]
+            assert diff.size == 0, (fi, o, x[diff[:3]], y[diff[:3]])
+    assert dev.counts.sum() > 0
+    for d in (dev_d, host, host_d):
+        assert np.array_equal(d.density, dev.density)
+    assert int(dev.density.sum()) == int(dev.counts.sum())

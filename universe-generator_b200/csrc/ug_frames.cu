@@ -26,7 +26,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/ug.h"
+#include "ug_frames.cuh"
 
 namespace ug {
 
@@ -239,77 +239,108 @@ struct DevBuf {
     }
 };
 
-}  // namespace
-}  // namespace ug
+// Per (path, axis): s0 = sum_j a_j sin f_j and the Horner coefficients
+// a_b e^{i f_b} (coef zeroed by the caller; frequencies are unique per axis).
+__global__ void k_fb_prep(int n, int nw, int bmax, int horner, const double* a, const double* b,
+                          const double* f, double* s0, double2* coef) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)n * 2;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int j = 0; j < nw; j++) {
+            const int64_t o = i * nw + j;
+            const double sf = sin(f[o]);
+            acc += a[o] * sf;
+            if (horner) {
+                double2& c = coef[i * (bmax + 1) + (int)b[o]];
+                c.x += a[o] * cos(f[o]);
+                c.y += a[o] * sf;
+            }
+        }
+        s0[i] = acc;
+    }
+}
 
-using namespace ug;
+// Dump-layout parameters from the packer (2+1): b as double for the direct sums.
+__global__ void k_fb_from_params(int64_t m, const int32_t* bi, double* bd) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+        bd[i] = (double)bi[i];
+}
 
-extern "C" int ug_frame_bake(const ug_frames_cfg* cfg, int32_t n, int32_t nw, const double* a2,
-                             const double* a, const double* b, const double* f, ug_frames_out* out) {
-    if (!cfg || !out || n < 1 || nw < 1 || !a2 || !a || !b || !f)
-        return set_error(UG_EINVAL, "frame_bake: bad arguments");
+// Density scatter of one (frame, observer): the hit count is read on the device.
+__global__ void k_fb_density_dev(const ug_hit* hits, const unsigned long long* count, unsigned long long cap,
+                                 double chiMax, int bins, uint32_t* grid) {
+    const unsigned long long c = *count;
+    const int64_t n = (int64_t)(c < cap ? c : cap);
+    const float inv = (float)(bins / (2.0 * chiMax));
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const ug_hit h = hits[i];
+        int cx = (int)floorf((h.dx + (float)chiMax) * inv);
+        int cy = (int)floorf((h.dy + (float)chiMax) * inv);
+        cx = cx < 0 ? 0 : (cx >= bins ? bins - 1 : cx);
+        cy = cy < 0 ? 0 : (cy >= bins ? bins - 1 : cy);
+        atomicAdd(&grid[(size_t)cy * bins + cx], 1u);
+    }
+}
+
+// One observer path's parameters on the host (for its comoving position and velocity).
+struct ObsPath {
+    std::vector<double> a2, a, b, f;  // [2], [2][nw] x3
+};
+
+int check_cfg(const ug_frames_cfg* cfg, ug_frames_out* out, int n) {
+    if (!cfg || !out || n < 1) return set_error(UG_EINVAL, "frame_bake: bad arguments");
     if (cfg->front < 0 || cfg->front > 2) return set_error(UG_EINVAL, "--front must be speed|fit|budget");
     if (cfg->n_frames < 1 || cfg->n_obs < 1) return set_error(UG_EINVAL, "need >= 1 frame and observer");
     for (int o = 0; o < cfg->n_obs; o++)
         if (cfg->obs_type[o] == 0 && (cfg->obs_path[o] < 0 || cfg->obs_path[o] >= n))
             return set_error(UG_EINVAL, "observer path out of range");
-    std::vector<double> A2(a2, a2 + (size_t)n * 2), A(a, a + (size_t)n * 2 * nw), Bv(b, b + (size_t)n * 2 * nw),
-        Fv(f, f + (size_t)n * 2 * nw);
-    int bMax = 2;
-    for (double x : Bv) bMax = std::max(bMax, (int)x);
+    return UG_OK;
+}
+
+// The frame loop over device-resident paths (dump layout, b as double).  With a hit
+// buffer the hits of every (frame, observer) come back sorted by (chi, src); without
+// one only counts and densities do, and no step waits for the host.
+int bake_device(const ug_frames_cfg* cfg, int n, int nw, int bMax, const double* dA2, const double* dA,
+                const double* dB, const double* dF, const std::vector<ObsPath>& obs, ug_frames_out* out) {
+    DevBuf buf;
     // Horner when the band is dense enough that one polynomial beats nw sines
     const int horner = (bMax <= 4 * nw) ? 1 : 0;
-    std::vector<double> s0((size_t)n * 2, 0.0);
-    std::vector<double2> coef;
-    if (horner) coef.assign((size_t)n * 2 * (bMax + 1), make_double2(0.0, 0.0));
-    for (int p = 0; p < n; p++)
-        for (int ax = 0; ax < 2; ax++)
-            for (int j = 0; j < nw; j++) {
-                const size_t o = ((size_t)p * 2 + ax) * nw + j;
-                s0[(size_t)p * 2 + ax] += A[o] * sin(Fv[o]);
-                if (horner) {
-                    double2& c = coef[((size_t)p * 2 + ax) * (bMax + 1) + (int)Bv[o]];
-                    c.x += A[o] * cos(Fv[o]);
-                    c.y += A[o] * sin(Fv[o]);
-                }
-            }
-    DevBuf buf;
-    double* dA2 = buf.get<double>(A2.size());
-    double* dS0 = buf.get<double>(s0.size());
-    double* dA = buf.get<double>(A.size());
-    double* dB = buf.get<double>(Bv.size());
-    double* dF = buf.get<double>(Fv.size());
-    double2* dC = buf.get<double2>(std::max<size_t>(coef.size(), 1));
+    double* dS0 = buf.get<double>((size_t)n * 2);
+    double2* dC = buf.get<double2>(horner ? (size_t)n * 2 * (bMax + 1) : 1);
     const int Mmax = std::min(kBudgetCap, std::max(kGridRows, 2 * bMax));
-    double* dZg = buf.get<double>(Mmax + 1);
-    double* dChig = buf.get<double>(Mmax + 1);
+    const int NF = cfg->n_frames, NO = cfg->n_obs;
+    double* dZg = buf.get<double>((size_t)NF * (Mmax + 1));
+    double* dChig = buf.get<double>((size_t)NF * (Mmax + 1));
     double* dPx = buf.get<double>((size_t)n * (Mmax + 1));
     double* dPy = buf.get<double>((size_t)n * (Mmax + 1));
+    const bool want_hits = out->hits != nullptr;
     const bool want_density = cfg->density_bins > 0 && out->density;
     const size_t bins2 = want_density ? (size_t)cfg->density_bins * cfg->density_bins : 0;
-    uint32_t* dDen = want_density ? buf.get<uint32_t>(bins2) : nullptr;
+    // densities: per (frame, observer) when hits come back one launch at a time,
+    // all of them on the device otherwise (one copy at the end)
+    uint32_t* dDen = want_density ? buf.get<uint32_t>(want_hits ? bins2 : bins2 * NF * NO) : nullptr;
     const unsigned long long hitCap = 1ull << 24;  // per (frame, observer) launch, frame_bake.cu:515
     ug_hit* dHits = buf.get<ug_hit>(hitCap);
-    unsigned long long* dCount = buf.get<unsigned long long>(1);
-    if (!dA2 || !dS0 || !dA || !dB || !dF || !dC || !dZg || !dChig || !dPx || !dPy || !dHits || !dCount ||
-        (want_density && !dDen))
+    unsigned long long* dCount = buf.get<unsigned long long>((size_t)NF * NO);
+    if (!dS0 || !dC || !dZg || !dChig || !dPx || !dPy || !dHits || !dCount || (want_density && !dDen))
         return set_error(UG_ENOMEM, "frame_bake: device allocation failed");
-    cudaMemcpy(dA2, A2.data(), A2.size() * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(dS0, s0.data(), s0.size() * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(dA, A.data(), A.size() * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(dB, Bv.data(), Bv.size() * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(dF, Fv.data(), Fv.size() * 8, cudaMemcpyHostToDevice);
-    if (horner) cudaMemcpy(dC, coef.data(), coef.size() * sizeof(double2), cudaMemcpyHostToDevice);
+    if (horner) cudaMemset(dC, 0, (size_t)n * 2 * (bMax + 1) * sizeof(double2));
+    k_fb_prep<<<(int)std::min<int64_t>(((int64_t)n * 2 + 127) / 128, 65536), 128>>>(n, nw, bMax, horner, dA, dB,
+                                                                                     dF, dS0, dC);
+    cudaMemset(dCount, 0, (size_t)NF * NO * sizeof(unsigned long long));
+    if (want_density && !want_hits) cudaMemset(dDen, 0, bins2 * NF * NO * 4);
     FPaths P{n, nw, bMax, horner, dA2, dS0, dA, dB, dF, dC};
     const double zMin = std::max(2e-3, cfg->zmin_pi * kPiF);
-    int64_t written = 0;
-    out->hits_total = 0;
-    std::vector<ug_hit> hh;
-    for (int fi = 0; fi < cfg->n_frames; fi++) {
-        const double frac = cfg->n_frames == 1 ? 0.0 : (double)fi / (cfg->n_frames - 1);
+    // fronts and rewind grids of every frame, uploaded once
+    std::vector<FFront> fronts(NF);
+    std::vector<int> Ks(NF);
+    std::vector<double> zgAll((size_t)NF * (Mmax + 1)), chigAll((size_t)NF * (Mmax + 1));
+    for (int fi = 0; fi < NF; fi++) {
+        const double frac = NF == 1 ? 0.0 : (double)fi / (NF - 1);
         const double zObs = std::min((cfg->from_pi + (cfg->to_pi - cfg->from_pi) * frac) * kPiF, kPiF - 1e-3);
         if (zMin >= zObs) return set_error(UG_EINVAL, "rewind floor >= z_obs");
-        FFront F{};
+        FFront& F = fronts[fi];
+        F = FFront{};
         F.budget = cfg->front == 2;
         F.cheb = F.budget || cfg->cheb;
         F.zObs = zObs;
@@ -317,7 +348,8 @@ extern "C" int ug_frame_bake(const ug_frames_cfg* cfg, int32_t n, int32_t nw, co
         F.spd = cfg->front == 0 ? std::max(1e-3, cfg->speed) : -1.0 / h_eta(zMin);
         F.bMax = bMax;
         F.M = F.budget ? std::min(kBudgetCap, std::max(kGridRows, 2 * bMax)) : kGridRows;
-        std::vector<double> zg(F.M + 1), chig(F.M + 1);
+        double* zg = zgAll.data() + (size_t)fi * (Mmax + 1);
+        double* chig = chigAll.data() + (size_t)fi * (Mmax + 1);
         if (F.budget) {
             F.chiMax = 0.0;
             for (int i = 0; i <= F.M; i++) {
@@ -332,44 +364,60 @@ extern "C" int ug_frame_bake(const ug_frames_cfg* cfg, int32_t n, int32_t nw, co
                 zg[i] = 2.0 * atan(exp(F.etaObs - chig[i] / F.spd));
             }
         }
-        const int K = cfg->wraps >= 0 ? cfg->wraps : (int)ceil((F.chiMax + 4.0) / 2.0);
+        Ks[fi] = cfg->wraps >= 0 ? cfg->wraps : (int)ceil((F.chiMax + 4.0) / 2.0);
         if (out->frame_meta) {
             out->frame_meta[fi * 3 + 0] = zObs;
             out->frame_meta[fi * 3 + 1] = F.chiMax;
-            out->frame_meta[fi * 3 + 2] = K;
+            out->frame_meta[fi * 3 + 2] = Ks[fi];
         }
-        cudaMemcpy(dZg, zg.data(), (F.M + 1) * 8, cudaMemcpyHostToDevice);
-        cudaMemcpy(dChig, chig.data(), (F.M + 1) * 8, cudaMemcpyHostToDevice);
+    }
+    cudaMemcpy(dZg, zgAll.data(), zgAll.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(dChig, chigAll.data(), chigAll.size() * 8, cudaMemcpyHostToDevice);
+    int64_t written = 0;
+    out->hits_total = 0;
+    std::vector<ug_hit> hh;
+    for (int fi = 0; fi < NF; fi++) {
+        const FFront& F = fronts[fi];
+        const int K = Ks[fi];
+        const double* zg = dZg + (size_t)fi * (Mmax + 1);
+        const double* chig = dChig + (size_t)fi * (Mmax + 1);
         {
             const int64_t tot = (int64_t)n * (F.M + 1);
-            k_fb_grid<<<(int)std::min<int64_t>((tot + 255) / 256, 65536), 256>>>(P, F.M, dZg, dPx, dPy);
+            k_fb_grid<<<(int)std::min<int64_t>((tot + 255) / 256, 65536), 256>>>(P, F.M, zg, dPx, dPy);
         }
-        for (int o = 0; o < cfg->n_obs; o++) {
+        for (int o = 0; o < NO; o++) {
             double ox, oy, bxv = 0.0, byv = 0.0;
             if (cfg->obs_type[o] == 0) {
                 double vx, vy;
-                h_comov(A2, A, Bv, Fv, nw, cfg->obs_path[o], zObs, &ox, &oy, &vx, &vy);
-                bxv = sin(zObs) * vx / F.spd;
-                byv = sin(zObs) * vy / F.spd;
+                const ObsPath& q = obs[o];
+                h_comov(q.a2, q.a, q.b, q.f, nw, 0, F.zObs, &ox, &oy, &vx, &vy);
+                bxv = sin(F.zObs) * vx / F.spd;
+                byv = sin(F.zObs) * vy / F.spd;
             } else {
                 ox = cfg->obs_xy[2 * o];
                 oy = cfg->obs_xy[2 * o + 1];
             }
             if (out->obs_meta) {
-                double* m = out->obs_meta + ((size_t)fi * cfg->n_obs + o) * 4;
+                double* m = out->obs_meta + ((size_t)fi * NO + o) * 4;
                 m[0] = ox;
                 m[1] = oy;
                 m[2] = bxv;
                 m[3] = byv;
             }
-            cudaMemset(dCount, 0, 8);
+            unsigned long long* cnt = dCount + (size_t)fi * NO + o;
             const int side = 2 * K + 1;
             const int64_t tot = (int64_t)n * side * side;
             k_fb_hits<<<(int)std::min<int64_t>((tot + 127) / 128, 1 << 20), 128>>>(
-                P, F, ox, oy, K, cfg->obs_type[o] == 0 ? cfg->obs_path[o] : -1, dZg, dChig, dPx, dPy, dHits,
-                dCount, hitCap);
+                P, F, ox, oy, K, cfg->obs_type[o] == 0 ? cfg->obs_path[o] : -1, zg, chig, dPx, dPy, dHits, cnt,
+                hitCap);
+            if (!want_hits) {
+                if (want_density)
+                    k_fb_density_dev<<<1184, 256>>>(dHits, cnt, hitCap, F.chiMax, cfg->density_bins,
+                                                    dDen + ((size_t)fi * NO + o) * bins2);
+                continue;
+            }
             unsigned long long nh = 0;
-            cudaError_t e = cudaMemcpy(&nh, dCount, 8, cudaMemcpyDeviceToHost);
+            cudaError_t e = cudaMemcpy(&nh, cnt, 8, cudaMemcpyDeviceToHost);
             if (e != cudaSuccess) {
                 std::string m = std::string("frame_bake: ") + cudaGetErrorString(e);
                 return set_error(UG_ECUDA, m.c_str());
@@ -380,12 +428,11 @@ extern "C" int ug_frame_bake(const ug_frames_cfg* cfg, int32_t n, int32_t nw, co
                 if (nh)
                     k_fb_density<<<(int)std::min<unsigned long long>((nh + 255) / 256, 65536), 256>>>(
                         dHits, (int64_t)nh, F.chiMax, cfg->density_bins, dDen);
-                cudaMemcpy(out->density + ((size_t)fi * cfg->n_obs + o) * bins2, dDen, bins2 * 4,
-                           cudaMemcpyDeviceToHost);
+                cudaMemcpy(out->density + ((size_t)fi * NO + o) * bins2, dDen, bins2 * 4, cudaMemcpyDeviceToHost);
             }
-            if (out->hit_count) out->hit_count[(size_t)fi * cfg->n_obs + o] = (int64_t)nh;
+            if (out->hit_count) out->hit_count[(size_t)fi * NO + o] = (int64_t)nh;
             out->hits_total += (int64_t)nh;
-            if (out->hits && written + (int64_t)nh <= out->hit_cap) {
+            if (written + (int64_t)nh <= out->hit_cap) {
                 hh.resize(nh);
                 if (nh) cudaMemcpy(hh.data(), dHits, nh * sizeof(ug_hit), cudaMemcpyDeviceToHost);
                 // device append order is scheduling-dependent: sort by (chi, src)
@@ -402,6 +449,102 @@ extern "C" int ug_frame_bake(const ug_frames_cfg* cfg, int32_t n, int32_t nw, co
         std::string m = std::string("frame_bake: ") + cudaGetErrorString(e);
         return set_error(UG_ECUDA, m.c_str());
     }
-    if (out->hits && out->hits_total > out->hit_cap) return set_error(UG_ECAP, "frame_bake: hit buffer too small");
+    if (!want_hits) {
+        std::vector<unsigned long long> counts((size_t)NF * NO);
+        cudaMemcpy(counts.data(), dCount, counts.size() * 8, cudaMemcpyDeviceToHost);
+        for (size_t i = 0; i < counts.size(); i++) {
+            if (counts[i] > hitCap) return set_error(UG_ECAP, "frame_bake: hit cap overflow (lower the wraps)");
+            if (out->hit_count) out->hit_count[i] = (int64_t)counts[i];
+            out->hits_total += (int64_t)counts[i];
+        }
+        if (want_density &&
+            cudaMemcpy(out->density, dDen, bins2 * NF * NO * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return set_error(UG_ECUDA, "frame_bake: density copy failed");
+    }
+    if (want_hits && out->hits_total > out->hit_cap) return set_error(UG_ECAP, "frame_bake: hit buffer too small");
     return UG_OK;
+}
+
+}  // namespace
+
+__global__ void k_fb_maxb(int64_t m, const int32_t* b, int* out) {
+    int mx = 2;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+        mx = max(mx, b[i]);
+    atomicMax(out, mx);
+}
+
+// Largest frequency of device-resident dump parameters.
+int max_b_device(const int32_t* b, int64_t m, int* out) {
+    int* d = nullptr;
+    if (cudaMalloc(&d, 4) != cudaSuccess) return set_error(UG_ENOMEM, "frame_bake: device allocation failed");
+    cudaMemset(d, 0, 4);
+    k_fb_maxb<<<592, 256>>>(m, b, d);
+    const cudaError_t e = cudaMemcpy(out, d, 4, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? UG_OK : set_error(UG_ECUDA, "frame_bake: reduction failed");
+}
+
+// Frames of the accepted paths of a packer universe, straight from the device
+// (the dump -> frame_bake pipeline without a CSV or host round trip).
+int frames_from_params(const ug_frames_cfg* cfg, int n, int nw, int bMax, const double* dA2, const double* dA,
+                       const int32_t* dBi, const double* dF, ug_frames_out* out) {
+    int rc = check_cfg(cfg, out, n);
+    if (rc) return rc;
+    DevBuf buf;
+    double* dB = buf.get<double>((size_t)n * 2 * nw);
+    if (!dB) return set_error(UG_ENOMEM, "frame_bake: device allocation failed");
+    k_fb_from_params<<<1184, 256>>>((int64_t)n * 2 * nw, dBi, dB);
+    std::vector<ObsPath> obs(cfg->n_obs);
+    for (int o = 0; o < cfg->n_obs; o++) {
+        if (cfg->obs_type[o] != 0) continue;
+        const int p = cfg->obs_path[o];
+        ObsPath& q = obs[o];
+        q.a2.resize(2);
+        q.a.resize(2 * nw);
+        q.b.resize(2 * nw);
+        q.f.resize(2 * nw);
+        std::vector<int32_t> bi(2 * nw);
+        if (cudaMemcpy(q.a2.data(), dA2 + (size_t)p * 2, 16, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(q.a.data(), dA + (size_t)p * 2 * nw, 16 * nw, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(bi.data(), dBi + (size_t)p * 2 * nw, 8 * nw, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(q.f.data(), dF + (size_t)p * 2 * nw, 16 * nw, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return set_error(UG_ECUDA, "frame_bake: observer copy failed");
+        for (int j = 0; j < 2 * nw; j++) q.b[j] = bi[j];
+    }
+    return bake_device(cfg, n, nw, bMax, dA2, dA, dB, dF, obs, out);
+}
+
+}  // namespace ug
+
+using namespace ug;
+
+extern "C" int ug_frame_bake(const ug_frames_cfg* cfg, int32_t n, int32_t nw, const double* a2,
+                             const double* a, const double* b, const double* f, ug_frames_out* out) {
+    if (nw < 1 || !a2 || !a || !b || !f) return set_error(UG_EINVAL, "frame_bake: bad arguments");
+    int rc = check_cfg(cfg, out, n);
+    if (rc) return rc;
+    int bMax = 2;
+    for (size_t i = 0; i < (size_t)n * 2 * nw; i++) bMax = std::max(bMax, (int)b[i]);
+    DevBuf buf;
+    const size_t m = (size_t)n * 2 * nw;
+    double* dA2 = buf.get<double>((size_t)n * 2);
+    double* dA = buf.get<double>(m);
+    double* dB = buf.get<double>(m);
+    double* dF = buf.get<double>(m);
+    if (!dA2 || !dA || !dB || !dF) return set_error(UG_ENOMEM, "frame_bake: device allocation failed");
+    cudaMemcpy(dA2, a2, (size_t)n * 2 * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(dA, a, m * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(dB, b, m * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(dF, f, m * 8, cudaMemcpyHostToDevice);
+    std::vector<ObsPath> obs(cfg->n_obs);
+    for (int o = 0; o < cfg->n_obs; o++) {
+        if (cfg->obs_type[o] != 0) continue;
+        const size_t p = (size_t)cfg->obs_path[o];
+        obs[o].a2.assign(a2 + p * 2, a2 + p * 2 + 2);
+        obs[o].a.assign(a + p * 2 * nw, a + (p + 1) * 2 * nw);
+        obs[o].b.assign(b + p * 2 * nw, b + (p + 1) * 2 * nw);
+        obs[o].f.assign(f + p * 2 * nw, f + (p + 1) * 2 * nw);
+    }
+    return bake_device(cfg, n, nw, bMax, dA2, dA, dB, dF, obs, out);
 }

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/ug.h"
+#include "ug_frames.cuh"
 #include "ug_kernels.cuh"
 #include "ug_mixed.cuh"
 
@@ -771,6 +772,40 @@ int ug_batch_params(void* h, int32_t u, double* a2, double* a, int32_t* b, doubl
     cudaFree(db);
     if (e != cudaSuccess) return fail(UG_ECUDA, "params: %s", cudaGetErrorString(e));
     return UG_OK;
+}
+
+int ug_batch_frames(void* h, int32_t u, const ug_frames_cfg* cfg, ug_frames_out* out) {
+    Batch* B = (Batch*)h;
+    if (!B || u < 0 || u >= B->n || !cfg || !out) return fail(UG_EINVAL, "bad arguments");
+    if (B->U[u].cfg.dim != 2) return fail(UG_ENOTSUP, "frames are baked for 2+1 universes");
+    int rc = pull_ctl(*B);
+    if (rc) return rc;
+    const int64_t N = B->hCtl[u].n_slots;
+    if (N < 1) return fail(UG_EINVAL, "frames: the universe has no accepted paths");
+    if (N > INT32_MAX / 2) return fail(UG_ECAP, "frames: too many paths");
+    const int nw = B->U[u].d.nw;
+    double *da2 = nullptr, *da = nullptr, *df = nullptr;
+    int32_t* db = nullptr;
+    auto release = [&]() {
+        cudaFree(da2);
+        cudaFree(da);
+        cudaFree(df);
+        cudaFree(db);
+    };
+    if (cudaMalloc(&da2, (size_t)N * 2 * 8) != cudaSuccess || cudaMalloc(&da, (size_t)N * 2 * nw * 8) != cudaSuccess ||
+        cudaMalloc(&df, (size_t)N * 2 * nw * 8) != cudaSuccess || cudaMalloc(&db, (size_t)N * 2 * nw * 4) != cudaSuccess) {
+        release();
+        return fail(UG_ENOMEM, "frames: device allocation failed");
+    }
+    launch_params(B->dU, u, N, da2, da, db, df, B->st);
+    int bMax = 2;
+    if (cudaStreamSynchronize(B->st) != cudaSuccess || (rc = max_b_device(db, N * 2 * nw, &bMax))) {
+        release();
+        return rc ? rc : fail(UG_ECUDA, "frames: parameter kernel failed");
+    }
+    rc = frames_from_params(cfg, (int)N, nw, bMax, da2, da, db, df, out);
+    release();
+    return rc;
 }
 
 int ug_batch_kernel_times(void* h, ug_kernel_times* out) {

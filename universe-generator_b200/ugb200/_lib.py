@@ -26,7 +26,7 @@ EXPORTS = (
     "ug_batch_params_noalloc",
     "ug_batch_kernel_times", "ug_batch_reset_times", "ug_batch_counters", "ug_batch_mixed_error",
     "ug_batch_destroy", "ug_pack_create", "ug_pack_run", "ug_pack_stats", "ug_pack_destroy",
-    "ug_frame_bake",
+    "ug_frame_bake", "ug_batch_frames",
 )
 
 
@@ -99,6 +99,7 @@ def load():
                                        C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.ug_batch_destroy.argtypes = [vp]
     L.ug_frame_bake.argtypes = [vp, i32, i32, vp, vp, vp, vp, vp]
+    L.ug_batch_frames.argtypes = [vp, i32, vp, vp]
     for name in EXPORTS:
         f = getattr(L, name)
         if f.restype is None or name != "ug_last_error":

@@ -46,48 +46,75 @@ class Baked:
     observers: list          # (type, path_idx, px, py)
     frame_meta: np.ndarray   # [frames][3] z_obs, chi_max, K
     obs_meta: np.ndarray     # [frames][obs][4] ox, oy, beta_x, beta_y
-    hits: list               # [frames][obs] -> HIT_DTYPE arrays sorted by (chi, src)
+    hits: list | None        # [frames][obs] -> HIT_DTYPE arrays sorted by (chi, src); None: not kept
     density: np.ndarray | None  # [frames][obs][bins][bins] uint32
     n_paths: int
+    counts: np.ndarray | None = None  # [frames][obs] hits per (frame, observer)
 
 
-def bake(a2, a, b, f, *, observers, from_pi=0.25, to_pi=0.75, frames=1, zmin_pi=0.02,
-         front="fit", metric="square", speed=0.33, wraps=-1, density_bins=0,
-         hit_cap=1 << 22) -> Baked:
-    """observers: list of ("path", idx) or ("point", x, y)."""
-    lib = L.load()
-    a2 = np.ascontiguousarray(a2, np.float64)
-    a = np.ascontiguousarray(a, np.float64)
-    b = np.ascontiguousarray(b, np.float64)
-    f = np.ascontiguousarray(f, np.float64)
-    n, _, nw = a.shape
+def _bake(call, n, *, observers, from_pi, to_pi, frames, zmin_pi, front, metric, speed, wraps,
+          density_bins, hit_cap, hits) -> Baked:
     ot = np.array([0 if o[0] == "path" else 1 for o in observers], np.int32)
     op = np.array([o[1] if o[0] == "path" else -1 for o in observers], np.int32)
     oxy = np.array([[0.0, 0.0] if o[0] == "path" else [o[1], o[2]] for o in observers], np.float64)
     cheb = 1 if (front == "budget" or metric == "square") else 0
     cfg = _Cfg(FRONTS[front], cheb, frames, wraps, from_pi, to_pi, zmin_pi, speed, len(observers),
                density_bins, ot.ctypes.data, op.ctypes.data, oxy.ctypes.data)
-    hits = np.zeros(hit_cap, HIT_DTYPE)
+    hbuf = np.empty(hit_cap, HIT_DTYPE) if hits else None
     counts = np.zeros((frames, len(observers)), np.int64)
     fmeta = np.zeros((frames, 3))
     ometa = np.zeros((frames, len(observers), 4))
-    den = (np.zeros((frames, len(observers), density_bins, density_bins), np.uint32)
+    den = (np.empty((frames, len(observers), density_bins, density_bins), np.uint32)
            if density_bins else None)
-    out = _Out(hits.ctypes.data, hit_cap, counts.ctypes.data, fmeta.ctypes.data, ometa.ctypes.data,
+    out = _Out(hbuf.ctypes.data if hbuf is not None else None, hit_cap if hits else 0,
+               counts.ctypes.data, fmeta.ctypes.data, ometa.ctypes.data,
                den.ctypes.data if den is not None else None, 0)
-    L.check(lib.ug_frame_bake(C.byref(cfg), n, nw, a2.ctypes.data, a.ctypes.data, b.ctypes.data,
-                              f.ctypes.data, C.byref(out)))
-    per, k = [], 0
-    for fi in range(frames):
-        row = []
-        for o in range(len(observers)):
-            c = int(counts[fi, o])
-            row.append(hits[k:k + c].copy())
-            k += c
-        per.append(row)
+    L.check(call(C.byref(cfg), C.byref(out)))
+    per = None
+    if hits:
+        per, k = [], 0
+        for fi in range(frames):
+            row = []
+            for o in range(len(observers)):
+                c = int(counts[fi, o])
+                row.append(hbuf[k:k + c].copy())
+                k += c
+            per.append(row)
     obs = [(int(ot[i]), int(op[i]), float(oxy[i, 0]), float(oxy[i, 1])) for i in range(len(observers))]
     return Baked(front, bool(cheb), speed, max(2e-3, zmin_pi * np.pi), wraps, obs, fmeta, ometa, per,
-                 den, n)
+                 den, n, counts)
+
+
+def bake(a2, a, b, f, *, observers, from_pi=0.25, to_pi=0.75, frames=1, zmin_pi=0.02,
+         front="fit", metric="square", speed=0.33, wraps=-1, density_bins=0,
+         hit_cap=1 << 22, hits=True) -> Baked:
+    """Frames of dump arrays a2 [n][2], a/b/f [n][2][nw] (host memory).
+    observers: list of ("path", idx) or ("point", x, y).  hits=False keeps only the
+    hit counts and densities (no per-frame wait for the host)."""
+    lib = L.load()
+    a2 = np.ascontiguousarray(a2, np.float64)
+    a = np.ascontiguousarray(a, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    f = np.ascontiguousarray(f, np.float64)
+    n, _, nw = a.shape
+    return _bake(lambda cfg, out: lib.ug_frame_bake(cfg, n, nw, a2.ctypes.data, a.ctypes.data,
+                                                    b.ctypes.data, f.ctypes.data, out), n,
+                 observers=observers, from_pi=from_pi, to_pi=to_pi, frames=frames, zmin_pi=zmin_pi,
+                 front=front, metric=metric, speed=speed, wraps=wraps, density_bins=density_bins,
+                 hit_cap=hit_cap, hits=hits)
+
+
+def bake_packed(packer, u=0, *, observers, from_pi=0.25, to_pi=0.75, frames=1, zmin_pi=0.02,
+                front="fit", metric="square", speed=0.33, wraps=-1, density_bins=0,
+                hit_cap=1 << 22, hits=True) -> Baked:
+    """Frames of universe u of a Packer (2+1) baked from its device-resident paths: the
+    dump -> frame_bake pipeline without the CSV.  Path indices are admission order."""
+    lib = L.load()
+    n = packer.stats(u).n
+    return _bake(lambda cfg, out: lib.ug_batch_frames(packer._h, u, cfg, out), n,
+                 observers=observers, from_pi=from_pi, to_pi=to_pi, frames=frames, zmin_pi=zmin_pi,
+                 front=front, metric=metric, speed=speed, wraps=wraps, density_bins=density_bins,
+                 hit_cap=hit_cap, hits=hits)
 
 
 def write_brf1(path, bk: Baked) -> None:
