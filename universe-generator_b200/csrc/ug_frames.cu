@@ -104,19 +104,75 @@ __device__ inline double metric(double dx, double dy, int cheb) {
     return cheb ? fmax(fabs(dx), fabs(dy)) : sqrt(dx * dx + dy * dy);
 }
 
+// Rewind-grid positions, one thread per (path, 4 consecutive rows): four
+// independent Horner chains per thread (each row the same operations as comov).
 __global__ void k_fb_grid(FPaths P, int M, const double* zg, double* px, double* py) {
-    const int64_t total = (int64_t)P.n * (M + 1);
+    const int R = M + 1, G = (R + 3) / 4;
+    const int64_t total = (int64_t)P.n * G;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const int p = (int)(i / (M + 1)), r = (int)(i % (M + 1));
-        comov(P, p, zg[r], &px[i], &py[i]);
+        const int p = (int)(i / G), r0 = (int)(i % G) * 4;
+        double z[4], s[4], w[2][4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            z[q] = zg[min(r0 + q, R - 1)];
+            s[q] = sin(z[q]);
+        }
+        for (int ax = 0; ax < 2; ax++) {
+            const size_t o = (size_t)p * 2 + ax;
+            if (P.horner) {
+                const double2* c = P.coef + o * (P.bmax + 1);
+                double sz[4], cz[4], pr[4], pi[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    sincos(z[q], &sz[q], &cz[q]);
+                    pr[q] = c[P.bmax].x;
+                    pi[q] = c[P.bmax].y;
+                }
+                for (int k = P.bmax - 1; k >= 0; k--) {
+                    const double2 ck = c[k];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const double nr = fma(pr[q], cz[q], fma(-pi[q], sz[q], ck.x));
+                        const double ni = fma(pr[q], sz[q], fma(pi[q], cz[q], ck.y));
+                        pr[q] = nr;
+                        pi[q] = ni;
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 4; q++) w[ax][q] = pi[q];
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    w[ax][q] = wiggle_direct(P.a + o * P.nw, P.b + o * P.nw, P.f + o * P.nw, P.nw, z[q]);
+            }
+        }
+        const double a2x = P.a2[(size_t)p * 2], a2y = P.a2[(size_t)p * 2 + 1];
+        const double s0x = P.s0[(size_t)p * 2], s0y = P.s0[(size_t)p * 2 + 1];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (r0 + q >= R) break;
+            const int64_t at = (int64_t)p * R + r0 + q;
+            px[at] = (a2x * s[q] + w[0][q] - s0x) / s[q];
+            py[at] = (a2y * s[q] + w[1][q] - s0y) / s[q];
+        }
     }
 }
 
-// One thread per (path, torus image): the crossing finder.
-__global__ void k_fb_hits(FPaths P, FFront F, double ox, double oy, int K, int obsIdx, const double* zg,
-                          const double* chig, const double* px, const double* py, ug_hit* hits,
-                          unsigned long long* count, unsigned long long cap) {
+// A sign change of dist(image) - chi_front between rewind rows i-1 and i.
+struct FCross {
+    int32_t p;
+    int16_t nx, ny;
+    int32_t i;
+    int32_t inside;  // the image was inside the front at row i-1
+};
+
+// One thread per (path, torus image): walks the rewind grid and records every
+// crossing; the bisections run in k_fb_refine, one thread per crossing, so no
+// warp waits for a single lane's refinement.
+__global__ void k_fb_cross(FPaths P, FFront F, double ox, double oy, int K, int obsIdx, const double* chig,
+                           const double* px, const double* py, FCross* cross, unsigned long long* count,
+                           unsigned long long cap) {
     const int side = 2 * K + 1;
     const int64_t total = (int64_t)P.n * side * side;
     for (int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; tid < total;
@@ -140,49 +196,62 @@ __global__ void k_fb_hits(FPaths P, FFront F, double ox, double oy, int K, int o
         for (int i = i0; i <= F.M; i++) {
             const double g = metric(px[row + i] + bx, py[row + i] + by, F.cheb) - chig[i];
             if ((prev < 0.0) != (g < 0.0)) {
-                const bool inside = prev < 0.0;
-                double chi, zEmit, qx, qy;
-                if (F.budget) {
-                    double lo = zg[i - 1], hi = zg[i];
-                    for (int it = 0; it < kBisect; it++) {
-                        const double mid = (lo + hi) / 2.0;
-                        comov(P, p, mid, &qx, &qy);
-                        const double gm = metric(qx + bx, qy + by, F.cheb) - reach_of(mid, F.zObs, F.bMax);
-                        if ((gm < 0.0) == inside)
-                            lo = mid;
-                        else
-                            hi = mid;
-                    }
-                    zEmit = (lo + hi) / 2.0;
-                    chi = reach_of(zEmit, F.zObs, F.bMax);
-                } else {
-                    double lo = chig[i - 1], hi = chig[i];
-                    for (int it = 0; it < kBisect; it++) {
-                        const double mid = (lo + hi) / 2.0;
-                        comov(P, p, 2.0 * atan(exp(F.etaObs - mid / F.spd)), &qx, &qy);
-                        const double gm = metric(qx + bx, qy + by, F.cheb) - mid;
-                        if ((gm < 0.0) == inside)
-                            lo = mid;
-                        else
-                            hi = mid;
-                    }
-                    chi = (lo + hi) / 2.0;
-                    zEmit = 2.0 * atan(exp(F.etaObs - chi / F.spd));
-                }
-                comov(P, p, zEmit, &qx, &qy);
                 const unsigned long long slot = atomicAdd(count, 1ull);
-                if (slot < cap) {
-                    ug_hit h;
-                    h.src = (uint32_t)p;
-                    h.dx = (float)(qx + bx);
-                    h.dy = (float)(qy + by);
-                    h.chi = (float)chi;
-                    h.z_emit = (float)zEmit;
-                    hits[slot] = h;
-                }
+                if (slot < cap) cross[slot] = FCross{p, (int16_t)nx, (int16_t)ny, i, prev < 0.0 ? 1 : 0};
             }
             prev = g;
         }
+    }
+}
+
+// One thread per crossing: 24 bisection steps with fresh evaluations
+// (frame_bake.cu:281-371), hit slot = crossing slot.
+__global__ void k_fb_refine(FPaths P, FFront F, double ox, double oy, const double* zg, const double* chig,
+                            const FCross* cross, const unsigned long long* count, unsigned long long cap,
+                            ug_hit* hits) {
+    const unsigned long long c = *count;
+    const int64_t n = (int64_t)(c < cap ? c : cap);
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const FCross x = cross[k];
+        const int p = x.p, i = x.i;
+        const bool inside = x.inside != 0;
+        const double bx = 2.0 * x.nx - ox, by = 2.0 * x.ny - oy;
+        double chi, zEmit, qx, qy;
+        if (F.budget) {
+            double lo = zg[i - 1], hi = zg[i];
+            for (int it = 0; it < kBisect; it++) {
+                const double mid = (lo + hi) / 2.0;
+                comov(P, p, mid, &qx, &qy);
+                const double gm = metric(qx + bx, qy + by, F.cheb) - reach_of(mid, F.zObs, F.bMax);
+                if ((gm < 0.0) == inside)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            zEmit = (lo + hi) / 2.0;
+            chi = reach_of(zEmit, F.zObs, F.bMax);
+        } else {
+            double lo = chig[i - 1], hi = chig[i];
+            for (int it = 0; it < kBisect; it++) {
+                const double mid = (lo + hi) / 2.0;
+                comov(P, p, 2.0 * atan(exp(F.etaObs - mid / F.spd)), &qx, &qy);
+                const double gm = metric(qx + bx, qy + by, F.cheb) - mid;
+                if ((gm < 0.0) == inside)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            chi = (lo + hi) / 2.0;
+            zEmit = 2.0 * atan(exp(F.etaObs - chi / F.spd));
+        }
+        comov(P, p, zEmit, &qx, &qy);
+        ug_hit h;
+        h.src = (uint32_t)p;
+        h.dx = (float)(qx + bx);
+        h.dy = (float)(qy + by);
+        h.chi = (float)chi;
+        h.z_emit = (float)zEmit;
+        hits[k] = h;
     }
 }
 
@@ -321,8 +390,9 @@ int bake_device(const ug_frames_cfg* cfg, int n, int nw, int bMax, const double*
     uint32_t* dDen = want_density ? buf.get<uint32_t>(want_hits ? bins2 : bins2 * NF * NO) : nullptr;
     const unsigned long long hitCap = 1ull << 24;  // per (frame, observer) launch, frame_bake.cu:515
     ug_hit* dHits = buf.get<ug_hit>(hitCap);
+    FCross* dCross = buf.get<FCross>(hitCap);
     unsigned long long* dCount = buf.get<unsigned long long>((size_t)NF * NO);
-    if (!dS0 || !dC || !dZg || !dChig || !dPx || !dPy || !dHits || !dCount || (want_density && !dDen))
+    if (!dS0 || !dC || !dZg || !dChig || !dPx || !dPy || !dHits || !dCross || !dCount || (want_density && !dDen))
         return set_error(UG_ENOMEM, "frame_bake: device allocation failed");
     if (horner) cudaMemset(dC, 0, (size_t)n * 2 * (bMax + 1) * sizeof(double2));
     k_fb_prep<<<(int)std::min<int64_t>(((int64_t)n * 2 + 127) / 128, 65536), 128>>>(n, nw, bMax, horner, dA, dB,
@@ -382,8 +452,8 @@ int bake_device(const ug_frames_cfg* cfg, int n, int nw, int bMax, const double*
         const double* zg = dZg + (size_t)fi * (Mmax + 1);
         const double* chig = dChig + (size_t)fi * (Mmax + 1);
         {
-            const int64_t tot = (int64_t)n * (F.M + 1);
-            k_fb_grid<<<(int)std::min<int64_t>((tot + 255) / 256, 65536), 256>>>(P, F.M, zg, dPx, dPy);
+            const int64_t tot = (int64_t)n * ((F.M + 1 + 3) / 4);
+            k_fb_grid<<<(int)std::min<int64_t>((tot + 127) / 128, 65536), 128>>>(P, F.M, zg, dPx, dPy);
         }
         for (int o = 0; o < NO; o++) {
             double ox, oy, bxv = 0.0, byv = 0.0;
@@ -407,9 +477,9 @@ int bake_device(const ug_frames_cfg* cfg, int n, int nw, int bMax, const double*
             unsigned long long* cnt = dCount + (size_t)fi * NO + o;
             const int side = 2 * K + 1;
             const int64_t tot = (int64_t)n * side * side;
-            k_fb_hits<<<(int)std::min<int64_t>((tot + 127) / 128, 1 << 20), 128>>>(
-                P, F, ox, oy, K, cfg->obs_type[o] == 0 ? cfg->obs_path[o] : -1, zg, chig, dPx, dPy, dHits, cnt,
-                hitCap);
+            k_fb_cross<<<(int)std::min<int64_t>((tot + 127) / 128, 1 << 20), 128>>>(
+                P, F, ox, oy, K, cfg->obs_type[o] == 0 ? cfg->obs_path[o] : -1, chig, dPx, dPy, dCross, cnt, hitCap);
+            k_fb_refine<<<1184, 128>>>(P, F, ox, oy, zg, chig, dCross, cnt, hitCap, dHits);
             if (!want_hits) {
                 if (want_density)
                     k_fb_density_dev<<<1184, 256>>>(dHits, cnt, hitCap, F.chiMax, cfg->density_bins,
