@@ -182,6 +182,19 @@ int ug_batch_reset_times(void* h);
 int ug_batch_mixed_error(void* h, int32_t u, int64_t first, int64_t count, double* max_err,
                          double* margin, double* max_ratio);
 
+/* ---- checkpoint / resume of a run (in-run counterpart of the store's job-level
+ * resume, braidlab/store.py:89-108).  A checkpoint of universe u is its
+ * admissions (ug_batch_accepted: candidate indices in admission order and their
+ * groups) plus an opaque state block of ug_state_bytes() bytes
+ * (ug_batch_save_state): round position, counters, stop windows.  Because the
+ * candidate stream is counter-based, ug_batch_restore rebuilds the packing from
+ * the admissions alone (trajectories regenerated, grid re-appended in admission
+ * order) and the run continues exactly as if it had not stopped, in this or any
+ * other batch holding a universe of the same model and seed. */
+int64_t ug_state_bytes(void);
+int ug_batch_save_state(void* h, int32_t u, void* state);
+int ug_batch_restore(void* h, int32_t u, int64_t n, const int64_t* idx, const int32_t* gid, const void* state);
+
 /* Release all device memory of the batch. */
 int ug_batch_destroy(void* h);
 

@@ -607,6 +607,8 @@ int ug_batch_create(const ug_universe_cfg* cfgs, int32_t n, const ug_run_opts* o
                              (int)(2 * kSmaxCap * sizeof(int32_t))) != cudaSuccess)
         return bail(fail(UG_ECUDA, "smem attribute failed"));
     if (cudaFuncSetAttribute(k_surv_gen, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(kSurvWarps * kSurvSmemPerWarp)) != cudaSuccess ||
+        cudaFuncSetAttribute(k_restore_gen, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(kSurvWarps * kSurvSmemPerWarp)) != cudaSuccess)
         return bail(fail(UG_ECUDA, "smem attribute failed"));
     if (B->any_mixed && (rc = mixed_init_kernels())) return bail(rc);
@@ -806,6 +808,162 @@ int ug_batch_frames(void* h, int32_t u, const ug_frames_cfg* cfg, ug_frames_out*
     rc = frames_from_params(cfg, (int)N, nw, bMax, da2, da, db, df, out);
     release();
     return rc;
+}
+
+// ---------------------------------------------------------- checkpoints
+
+namespace {
+// Saved control block of one universe: what it was built from, then the block.
+struct CkHeader {
+    char magic[4];  // "UGCK"
+    int32_t version;
+    int32_t ctl_bytes;
+    int32_t pad;
+    ug_universe_cfg cfg;
+};
+constexpr int32_t kCkVersion = 1;
+
+bool same_model(const ug_universe_cfg& a, const ug_universe_cfg& b) {
+    return a.dim == b.dim && a.T == b.T && a.terms == b.terms && a.rng == b.rng && a.zgrid == b.zgrid &&
+           a.excl == b.excl && a.cross1d == b.cross1d && a.pin_sin1 == b.pin_sin1 && a.group_mode == b.group_mode &&
+           a.seed == b.seed;
+}
+}  // namespace
+
+int64_t ug_state_bytes(void) { return (int64_t)(sizeof(CkHeader) + sizeof(UniCtl)); }
+
+int ug_batch_save_state(void* h, int32_t u, void* buf) {
+    Batch* B = (Batch*)h;
+    if (!B || u < 0 || u >= B->n || !buf) return fail(UG_EINVAL, "bad arguments");
+    int rc = pull_ctl(*B);
+    if (rc) return rc;
+    CkHeader hd{};
+    memcpy(hd.magic, "UGCK", 4);
+    hd.version = kCkVersion;
+    hd.ctl_bytes = (int32_t)sizeof(UniCtl);
+    hd.cfg = B->U[u].cfg;
+    memcpy(buf, &hd, sizeof hd);
+    memcpy((char*)buf + sizeof hd, &B->hCtl[u], sizeof(UniCtl));
+    return UG_OK;
+}
+
+// Rebuilds universe u from its admissions (candidate indices in admission order
+// and their groups) and a saved control block: the trajectories are regenerated
+// from the candidate stream and appended to a cleared grid in admission order,
+// S_max paths per step, by the survivor product and commit kernels.
+int ug_batch_restore(void* h, int32_t u, int64_t n, const int64_t* idx, const int32_t* gid, const void* buf) {
+    Batch* B = (Batch*)h;
+    if (!B || u < 0 || u >= B->n || !buf || n < 0 || (n > 0 && (!idx || !gid)))
+        return fail(UG_EINVAL, "bad arguments");
+    CkHeader hd;
+    memcpy(&hd, buf, sizeof hd);
+    if (memcmp(hd.magic, "UGCK", 4) || hd.version != kCkVersion || hd.ctl_bytes != (int32_t)sizeof(UniCtl))
+        return fail(UG_EINVAL, "restore: not a state of this library version");
+    UniHost& U = B->U[u];
+    if (!same_model(hd.cfg, U.cfg)) return fail(UG_EINVAL, "restore: the state belongs to another universe model");
+    UniCtl saved;
+    memcpy(&saved, (const char*)buf + sizeof hd, sizeof saved);
+    if (saved.n_slots != n) return fail(UG_EINVAL, "restore: %lld admissions given, the state has %lld",
+                                        (long long)n, (long long)saved.n_slots);
+    if (saved.state == ST_ERROR) return fail(UG_EINVAL, "restore: the saved universe had failed");
+    int rc = pull_ctl(*B);
+    if (rc) return rc;
+    UniDev& d = U.d;
+    const int T = U.cfg.T;
+    // clear the universe's grid, bitmaps and round hash
+    if (d.grid_kind == GRID_DENSE) {
+        int64_t cpt = 1;
+        for (int ax = 0; ax < d.dim; ax++) cpt *= d.gw;
+        CKR(cudaMemsetAsync(d.heads, 0xff, (size_t)T * cpt * sizeof(int32_t), B->st));
+    } else {
+        const int64_t need = std::max<int64_t>(1 << 16, pow2_at_least((n * T + (int64_t)d.S_max * T) * 4));
+        if (need > U.hcap) {
+            CKR(cudaStreamSynchronize(B->st));
+            cudaFree(d.hkeys);
+            cudaFree(d.heads);
+            if ((rc = alloc_hash(U, need))) return rc;
+        } else {
+            CKR(cudaMemsetAsync(d.hkeys, 0xff, (size_t)U.hcap * sizeof(uint64_t), B->st));
+            CKR(cudaMemsetAsync(d.heads, 0xff, (size_t)U.hcap * sizeof(int32_t), B->st));
+        }
+    }
+    CKR(cudaMemsetAsync(d.occ, 0, (size_t)U.occ_words * sizeof(uint32_t), B->st));
+    CKR(cudaMemsetAsync(d.occ1, 0, (size_t)U.occ1_words * sizeof(uint32_t), B->st));
+    CKR(cudaMemsetAsync(d.rkeys, 0xff, (size_t)(d.rmask + 1) * sizeof(uint64_t), B->st));
+    // room for the admissions and the next rounds
+    if (n + (int64_t)d.S_max * 2 > d.slot_cap) {
+        CKR(cudaStreamSynchronize(B->st));
+        cudaFree(d.pts);
+        cudaFree(d.ptf);
+        cudaFree(d.acc_idx);
+        if ((rc = alloc_points(U, n + (int64_t)d.S_max * 2))) return rc;
+    }
+    if ((rc = push_unidev(*B))) return rc;
+    // rebuild control block: k_commit reads these and accumulates hash keys and cells
+    UniCtl k = B->hCtl[u];
+    const int32_t epoch = k.epoch;
+    init_ctl(U.cfg, d, k);
+    k.epoch = epoch;
+    k.state = ST_ACTIVE;
+    std::vector<int32_t> iota(d.S_max), zero(d.S_max + 1, 0);
+    for (int i = 0; i < d.S_max; i++) iota[i] = i;
+    int64_t* dIdx = nullptr;
+    CKR(cudaMalloc(&dIdx, (size_t)d.S_max * sizeof(int64_t)));
+    RoundInfo* ri = new RoundInfo();
+    int64_t done = 0;
+    while (done < n && rc == UG_OK) {
+        const int m = (int)std::min<int64_t>(d.S_max, n - done);
+        k.S = k.S_raw = k.trunc = k.stop_at = m;
+        k.n_slots_prev = done;
+        k.n_slots = done;
+        k.round_base = 0;
+        memset(ri, 0, sizeof(RoundInfo));
+        ri->n_uni = B->n;
+        const int sev = ((m * d.dim + 31) >> 5) * ((T + 31) >> 5);
+        for (int v = 0; v <= B->n; v++) {
+            const bool past = v > u;
+            ri->surv_off[v] = past ? m : 0;
+            ri->sev_off[v] = past ? sev : 0;
+            ri->spt_off[v] = past ? m * T : 0;
+        }
+        ri->total_surv = m;
+        ri->total_sev = sev;
+        ri->total_spt = m * T;
+        cudaError_t e = cudaMemcpyAsync(B->dInfo, ri, sizeof(RoundInfo), cudaMemcpyHostToDevice, B->st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&B->dCtl[u], &k, sizeof(UniCtl), cudaMemcpyHostToDevice, B->st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d.acc_rank, iota.data(), (size_t)m * 4, cudaMemcpyHostToDevice, B->st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d.sgid, gid + done, (size_t)m * 4, cudaMemcpyHostToDevice, B->st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d.surv_off, zero.data(), (size_t)(m + 1) * 4, cudaMemcpyHostToDevice, B->st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dIdx, idx + done, (size_t)m * 8, cudaMemcpyHostToDevice, B->st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(d.spos, 0, (size_t)m * T * sizeof(Pt64), B->st);  // unused axes
+        if (e == cudaSuccess) {
+            k_restore_gen<<<B->nsm * 4, 32 * kSurvWarps, kSurvWarps * kSurvSmemPerWarp, B->st>>>(B->dU, u, dIdx, m);
+            k_surv_gemm<<<B->nsm * 4, 128, 0, B->st>>>(B->dU, B->dCtl, B->dInfo);
+            k_commit<<<B->nsm * 8, 256, 0, B->st>>>(B->dU, B->dCtl, B->dInfo);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d.acc_idx + done, dIdx, (size_t)m * 8, cudaMemcpyDeviceToDevice, B->st);
+        // carry the device-accumulated counters into the next step's block
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&k, &B->dCtl[u], sizeof(UniCtl), cudaMemcpyDeviceToHost, B->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(B->st);
+        if (e != cudaSuccess) rc = fail(UG_ECUDA, "restore: %s", cudaGetErrorString(e));
+        else if (k.state == ST_ERROR) rc = fail(UG_ECAP, "restore: device error %d", k.err_code);
+        done += m;
+    }
+    delete ri;
+    cudaFree(dIdx);
+    if (rc) return rc;
+    const int64_t filled = k.filled + k.round_new;
+    if (filled != saved.filled + saved.round_new)
+        return fail(UG_EINVAL, "restore: rebuilt grid holds %lld cells, the state %lld (admissions do not match)",
+                    (long long)filled, (long long)(saved.filled + saved.round_new));
+    // the saved block, with this batch's hash usage and round-hash epoch
+    saved.hash_used = k.hash_used;
+    saved.epoch = epoch;
+    B->hCtl[u] = saved;
+    CKR(cudaMemcpyAsync(&B->dCtl[u], &saved, sizeof(UniCtl), cudaMemcpyHostToDevice, B->st));
+    CKR(cudaStreamSynchronize(B->st));
+    return UG_OK;
 }
 
 int ug_batch_kernel_times(void* h, ug_kernel_times* out) {

@@ -390,6 +390,24 @@ __device__ __forceinline__ void warp_gen64(const UniDev& d, uint64_t idx, double
     }
 }
 
+// Rows r * dim + ax of the term-ordered coefficient matrix of one survivor.
+__device__ __forceinline__ void store_coef_rows(const UniDev& d, int r, const double* alpha, const double* beta,
+                                                const double* a2, int lane) {
+    const int F = d.F, F1 = F + 1, R = d.Rpad;
+    [[maybe_unused]] const int64_t ncoef = (int64_t)d.K * R;
+    for (int ax = 0; ax < d.dim; ax++) {
+        const int row = r * d.dim + ax;
+        const double* al = alpha + ax * F1;
+        const double* bt = beta + ax * F1;
+        for (int b = 2 + lane; b <= F; b += 32) {
+            const int64_t k = kseq_s(b);
+            d.coef[UG_IDX(k * R + row, ncoef)] = al[b];
+            if (!(b & 1)) d.coef[UG_IDX((k + 1) * R + row, ncoef)] = bt[b];
+        }
+        if (lane == 0) d.a2row[UG_IDX(row, R)] = a2[ax];
+    }
+}
+
 // Survivor trajectories in three steps.
 //
 // k_surv_gen: one warp per survivor regenerates its FP64 coefficients
@@ -414,20 +432,29 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_surv_gen(const UniDev* __re
         const UniDev& d = U[u];
         const UniCtl& c = ctl[u];
         const uint64_t idx = (uint64_t)(c.round_base + d.surv_off[UG_IDX(r, d.S_max + 1)]);
-        const int F = d.F, F1 = F + 1, R = d.Rpad;
-        [[maybe_unused]] const int64_t ncoef = (int64_t)d.K * R;
         warp_gen64(d, idx, alpha, beta, a2, bj, wj, lane);
-        for (int ax = 0; ax < d.dim; ax++) {
-            const int row = r * d.dim + ax;
-            const double* al = alpha + ax * F1;
-            const double* bt = beta + ax * F1;
-            for (int b = 2 + lane; b <= F; b += 32) {
-                const int64_t k = kseq_s(b);
-                d.coef[UG_IDX(k * R + row, ncoef)] = al[b];
-                if (!(b & 1)) d.coef[UG_IDX((k + 1) * R + row, ncoef)] = bt[b];
-            }
-            if (lane == 0) d.a2row[UG_IDX(row, R)] = a2[ax];
-        }
+        store_coef_rows(d, r, alpha, beta, a2, lane);
+        __syncwarp();
+    }
+}
+
+// Checkpoint restore: the coefficient rows of m given admissions (explicit
+// candidate indices) of universe u, as k_surv_gen writes them for survivors.
+__global__ void __launch_bounds__(32 * kSurvWarps) k_restore_gen(const UniDev* __restrict__ U, int u,
+                                                                   const int64_t* __restrict__ idx, int m) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    unsigned char* my = smem_raw + (size_t)wib * kSurvSmemPerWarp;
+    double* alpha = (double*)my;
+    double* beta = alpha + 3 * (kMaxF + 1);
+    double* a2 = beta + 3 * (kMaxF + 1);
+    double* wj = a2 + 3;
+    int32_t* bj = (int32_t*)(wj + kMaxF);
+    const UniDev& d = U[u];
+    const int gwarp = blockIdx.x * kSurvWarps + wib, nwarps = gridDim.x * kSurvWarps;
+    for (int r = gwarp; r < m; r += nwarps) {
+        warp_gen64(d, (uint64_t)idx[r], alpha, beta, a2, bj, wj, lane);
+        store_coef_rows(d, r, alpha, beta, a2, lane);
         __syncwarp();
     }
 }

@@ -10,4 +10,4 @@ from ._lib import (  # noqa: F401
     EXCL_OPEN, EXCL_REF, GROUP_NONE, GROUP_SUBPATH, GROUP_UNIQUE, PREC_FP64, PREC_MIXED,
     RNG_KNOT, RNG_PHILOX, ZGRID_MID, ZGRID_REF, UgError, load,
 )
-from .packer import Packer, Stats, Universe, pack  # noqa: F401
+from .packer import Packer, Stats, Universe, load_checkpoint, pack, save_checkpoint  # noqa: F401

@@ -26,7 +26,7 @@ EXPORTS = (
     "ug_batch_params_noalloc",
     "ug_batch_kernel_times", "ug_batch_reset_times", "ug_batch_counters", "ug_batch_mixed_error",
     "ug_batch_destroy", "ug_pack_create", "ug_pack_run", "ug_pack_stats", "ug_pack_destroy",
-    "ug_frame_bake", "ug_batch_frames",
+    "ug_frame_bake", "ug_batch_frames", "ug_state_bytes", "ug_batch_save_state", "ug_batch_restore",
 )
 
 
@@ -100,10 +100,14 @@ def load():
     L.ug_batch_destroy.argtypes = [vp]
     L.ug_frame_bake.argtypes = [vp, i32, i32, vp, vp, vp, vp, vp]
     L.ug_batch_frames.argtypes = [vp, i32, vp, vp]
+    L.ug_state_bytes.argtypes = []
+    L.ug_batch_save_state.argtypes = [vp, i32, vp]
+    L.ug_batch_restore.argtypes = [vp, i32, i64, vp, vp, vp]
     for name in EXPORTS:
         f = getattr(L, name)
         if f.restype is None or name != "ug_last_error":
             f.restype = C.c_int
+    L.ug_state_bytes.restype = i64
     _lib = L
     return L
 

@@ -176,6 +176,27 @@ class Packer:
                                               C.byref(q)))
         return e.value, m.value, q.value
 
+    # -- checkpoint / resume
+    def checkpoint(self, u: int = 0) -> dict:
+        """Everything needed to resume universe u: admissions (candidate indices in
+        admission order, groups) and the opaque state block."""
+        lib = L.load()
+        idx, gid = self.accepted(u)
+        state = (C.c_uint8 * int(lib.ug_state_bytes()))()
+        L.check(lib.ug_batch_save_state(self._h, u, state))
+        return {"idx": np.ascontiguousarray(idx, np.int64), "gid": np.ascontiguousarray(gid, np.int32),
+                "state": bytes(state)}
+
+    def restore(self, u: int, ck: dict) -> "Packer":
+        """Rebuild universe u from a checkpoint of a universe of the same model and
+        seed; run() then continues where the checkpointed run stopped."""
+        lib = L.load()
+        idx = np.ascontiguousarray(ck["idx"], np.int64)
+        gid = np.ascontiguousarray(ck["gid"], np.int32)
+        state = C.create_string_buffer(bytes(ck["state"]), len(ck["state"]))
+        L.check(lib.ug_batch_restore(self._h, u, len(idx), idx.ctypes.data, gid.ctypes.data, state))
+        return self
+
     def close(self) -> None:
         if self._h:
             L.load().ug_batch_destroy(self._h)
@@ -192,6 +213,15 @@ class Packer:
             self.close()
         except Exception:
             pass
+
+
+def save_checkpoint(path, ck: dict) -> None:
+    np.savez(path, idx=ck["idx"], gid=ck["gid"], state=np.frombuffer(ck["state"], np.uint8))
+
+
+def load_checkpoint(path) -> dict:
+    z = np.load(path)
+    return {"idx": z["idx"], "gid": z["gid"], "state": z["state"].tobytes()}
 
 
 def pack(universe: Universe, precision: int = L.PREC_FP64, **kw):
