@@ -68,6 +68,9 @@ typedef struct ug_universe_cfg {
     double sub_accept_rate;
     double sub_fill_rate; /* --sub-until-fill-rate: phase-2 stop on windowed newly occupied
                              grid cells per attempt (0 = off), braid_cuda.cu:960-1035 */
+    int32_t euclid;       /* --euclid-collision: exclusion by the L2 ball of radius cell
+                             instead of the Chebyshev cube (braid_cuda3d.cu:605-608) */
+    int32_t pad;
 } ug_universe_cfg;
 
 typedef struct ug_run_opts {

@@ -36,6 +36,7 @@ class _Model(C.Structure):
         ("excl", C.c_int32),
         ("cross1d", C.c_int32),
         ("pin", C.c_int32),
+        ("euclid", C.c_int32),
         ("seed", C.c_uint64),
     ]
 
@@ -105,6 +106,7 @@ class Model:
     cross1d: int = 0
     pin: int = 0
     seed: int = 0
+    euclid: int = 0  # --euclid-collision: L2 ball instead of the Chebyshev cube
 
     @property
     def nw(self) -> int:
@@ -112,7 +114,7 @@ class Model:
 
     def _c(self) -> _Model:
         return _Model(self.dim, self.T, self.nw, self.rng, self.zgrid, self.excl,
-                      self.cross1d, self.pin, self.seed & (2**64 - 1))
+                      self.cross1d, self.pin, self.euclid, self.seed & (2**64 - 1))
 
 
 def _p(a: np.ndarray):

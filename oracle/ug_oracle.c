@@ -208,6 +208,7 @@ typedef struct {
     int T, F, dim, gw;
     double cell;     /* exclusion radius == grid cell width */
     int inclusive;   /* 1: |d| <= cell, 0: |d| < cell */
+    int euclid;      /* L2 ball of radius cell (cuda/braid_cuda3d.cu:605-608) */
     double* z;
     double* sinz;
     double* invsinz;
@@ -221,6 +222,7 @@ static int tabs_init(const ora_model* m, tabs_t* tb) {
     tb->T = T;
     tb->F = F;
     tb->dim = m->dim;
+    tb->euclid = m->euclid;
     if (m->excl == ORA_EXCL_REF) {
         tb->cell = 2.0 / T;
         tb->gw = T;
@@ -522,6 +524,25 @@ static int hit1(double d, double cell, int inclusive) {
     return inclusive ? ad <= cell : ad < cell;
 }
 
+/* Exclusion test of two points (axis ax of P at P[ax * ps], of Q at Q[ax * qs]):
+ * the Chebyshev cube of half-width cell, or with euclid the L2 ball
+ * dX*dX + dY*dY + dW*dW <= cell*cell (cuda/braid_cuda3d.cu:605-608, summed
+ * in that order; this file is built without floating-point contraction). */
+static int pair_hit(const tabs_t* tb, int dim, const double* P, int64_t ps, const double* Q, int64_t qs) {
+    if (!tb->euclid) {
+        for (int ax = 0; ax < dim; ax++)
+            if (!hit1(torus_delta(P[ax * ps] - Q[ax * qs]), tb->cell, tb->inclusive)) return 0;
+        return 1;
+    }
+    double s = 0.0;
+    for (int ax = 0; ax < dim; ax++) {
+        const double d = torus_delta(P[ax * ps] - Q[ax * qs]);
+        s = s + d * d;
+    }
+    const double r2 = tb->cell * tb->cell;
+    return tb->inclusive ? s <= r2 : s < r2;
+}
+
 /* Contacts of position vector Pt (one timestep) with stored paths at t.
  * Unique mode returns 1 on the first contact.  Group mode collects ids into
  * *g0 and returns 1 as soon as a second distinct id appears. */
@@ -542,9 +563,7 @@ static int contacts_at(const store_t* s, const tabs_t* tb, int t, const double* 
         int32_t p = hget(s, cell_key(t, cc, s->dim, tb->gw));
         while (p >= 0) {
             const double* Q = &s->pos[(int64_t)p * s->dim * s->T];
-            int hit = 1;
-            for (int ax = 0; ax < s->dim && hit; ax++)
-                hit = hit1(torus_delta(Pt[ax] - Q[ax * s->T + t]), tb->cell, tb->inclusive);
+            const int hit = pair_hit(tb, s->dim, Pt, 1, Q + t, s->T);
             if (hit) {
                 if (!group) return 1;
                 if (*g0 == -1)
@@ -706,13 +725,7 @@ static int pack_threaded(const ora_model* m, const ora_run* run, const tabs_t* t
             for (int64_t p = n0; p < s->n && !clash; p++) {
                 const double* Q = &s->pos[p * D * T];
                 if (D == 1 && m->cross1d && crosses(ce->P, Q, T)) clash = 1;
-                for (int t = 0; t < T && !clash; t++) {
-                    int hit = 1;
-                    for (int ax = 0; ax < D && hit; ax++)
-                        hit = hit1(torus_delta(ce->P[ax * T + t] - Q[ax * T + t]), tb->cell,
-                                   tb->inclusive);
-                    clash = hit;
-                }
+                for (int t = 0; t < T && !clash; t++) clash = pair_hit(tb, D, ce->P + t, T, Q + t, T);
             }
             if (clash) continue;
             if (store_add(s, ce->P, (int32_t)s->n, tb->cell) || record(res, idx + i, (int32_t)s->n - 1)) {

@@ -43,6 +43,7 @@ typedef struct ora_model {
     int32_t excl;    /* ORA_EXCL_* */
     int32_t cross1d; /* 1+1D sign-change (crossing) rejection */
     int32_t pin;     /* --pin-sin1: sin1 amplitudes forced to zero */
+    int32_t euclid;  /* --euclid-collision: L2 ball instead of the Chebyshev cube */
     uint64_t seed;
 } ora_model;
 

@@ -85,3 +85,11 @@ def test_braid_cuda_sub_until_fill_rate(tmp_path):
     assert "sub done (fill-rate): Nsub=" in r.stderr
     sub_att = int(r.stderr.split("sub done (fill-rate): Nsub=")[1].split(" in ")[1].split()[0])
     assert 20_000_000 <= sub_att < 60_000_000
+
+
+def test_braid_cuda3d_euclid_collision(tmp_path, oracle):
+    r = _run("braid_cuda3d", ["-t", "16", "--seed", "3", "--attempts", "20000", "--terms", "16",
+                              "--euclid-collision", "--rng", "philox"])
+    assert r.returncode == 0, r.stderr
+    ref = oracle.pack(oracle.Model(dim=3, T=16, seed=3, euclid=1), 20000)
+    assert f"done: N={len(ref.acc_idx)} in 20000 attempts" in r.stderr

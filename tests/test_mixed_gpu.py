@@ -9,7 +9,7 @@ pytestmark = pytest.mark.gpu
 
 def _model(O, u):
     return O.Model(dim=u.dim, T=u.T, terms=u.terms, rng=u.rng, zgrid=u.zgrid, excl=u.excl,
-                   cross1d=u.cross1d, pin=u.pin_sin1, seed=u.seed)
+                   cross1d=u.cross1d, pin=u.pin_sin1, seed=u.seed, euclid=u.euclid)
 
 
 @pytest.mark.parametrize("dim,T,zg,ex", [(2, 16, 0, 0), (2, 64, 1, 1), (3, 128, 1, 1),

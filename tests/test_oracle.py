@@ -167,3 +167,33 @@ def test_oracle_matches_reference_gpu_binary():
             p = _parse(row, r["dim"], m.nw)
             c = O.candidate(m, p["idx"])
             assert np.array_equal(c["a"], np.array(p["a"])) and np.array_equal(c["f"], np.array(p["f"]))
+
+
+@pytest.mark.parametrize("dim,excl", [(2, 0), (3, 1), (2, 1)])
+def test_euclid_exclusion_against_brute_force(oracle, dim, excl):
+    """The L2-ball exclusion (--euclid-collision, cuda/braid_cuda3d.cu:605-608) of the
+    oracle against sequential RSA written out pairwise over all timesteps; both the
+    threaded batch form and the plain sequential form."""
+    m = oracle.Model(dim=dim, T=10, zgrid=1, excl=excl, seed=17 + dim, euclid=1)
+    n = 400
+    pos = np.stack([oracle.positions(m, i) for i in range(n)])  # [n][dim][T]
+    cell = 2.0 / 10 if excl == 0 else 1.0 / 10
+    acc = []
+    for i in range(n):
+        ok = True
+        for j in acc:
+            d = pos[i] - pos[j]
+            d = np.where(d > 1.0, d - 2.0, np.where(d < -1.0, d + 2.0, d))
+            s = np.zeros(d.shape[1])
+            for ax in range(dim):
+                s = s + d[ax] * d[ax]
+            if np.any(s <= cell * cell if excl == 0 else s < cell * cell):
+                ok = False
+                break
+        if ok:
+            acc.append(i)
+    for nth in (1, 4):
+        res = oracle.pack(m, n, nthreads=nth, round_size=64)
+        assert res.acc_idx.tolist() == acc
+    cheb = oracle.pack(oracle.Model(dim=dim, T=10, zgrid=1, excl=excl, seed=17 + dim), n)
+    assert len(acc) > len(cheb.acc_idx)  # the ball excludes less than the cube

@@ -12,7 +12,7 @@ PAR_TOL = 1e-14
 
 def _model(O, u):
     return O.Model(dim=u.dim, T=u.T, terms=u.terms, rng=u.rng, zgrid=u.zgrid, excl=u.excl,
-                   cross1d=u.cross1d, pin=u.pin_sin1, seed=u.seed)
+                   cross1d=u.cross1d, pin=u.pin_sin1, seed=u.seed, euclid=u.euclid)
 
 
 def _check(ug, O, u, precision=0, **kw):
@@ -219,3 +219,19 @@ def test_sub_fill_rate_stop_is_a_prefix(ug):
     assert st2.attempts == st.attempts
     assert np.array_equal(a, b) and np.array_equal(g, h)
     assert st2.filled == st.filled
+
+
+@pytest.mark.parametrize("dim,T,excl,prec,mode", [(2, 32, 0, 0, 0), (2, 32, 1, 1, 0), (3, 24, 1, 1, 0),
+                                                   (3, 40, 0, 0, 0), (3, 40, 0, 1, 0), (2, 48, 1, 1, 2),
+                                                   (3, 24, 1, 1, 2)])
+def test_euclid_exclusion(ug, oracle, dim, T, excl, prec, mode):
+    """--euclid-collision (the L2 ball of radius cell, cuda/braid_cuda3d.cu:605-608) on the
+    FP64 path and through the tensor-core prefilter's guard band: accepted sets (and
+    groups) equal the oracle's."""
+    u = ug.Universe(dim=dim, T=T, zgrid=1, excl=excl, seed=21 + T, attempts=30000, euclid=1,
+                    group_mode=mode, round_size=2048)
+    st, idx = _check(ug, oracle, u, precision=prec)
+    cube = ug.Universe(**{**u.__dict__, "euclid": 0})
+    with ug.Packer([cube], precision=prec) as p:
+        p.run()
+        assert p.stats(0).n < st.n  # the ball excludes less than the cube

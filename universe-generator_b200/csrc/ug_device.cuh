@@ -74,7 +74,7 @@ struct UniDev {
     uint32_t modmax;     // knot: frequencies drawn in [2, modmax+1]
     int32_t B_max;       // candidates per round cap
     int32_t S_max;       // survivors per round cap
-    int32_t pad0;
+    int32_t euclid;      // exclusion by the L2 ball of radius cell (else the Chebyshev cube)
     // tables
     const double* S;       // [(F+1) * T]
     const double* Cm;      // [(F+1) * T]
@@ -217,6 +217,25 @@ __device__ __forceinline__ int cell_of(double X, double cell, int gw) {
 __device__ __forceinline__ bool hit1(double d, double cell, int inclusive) {
     const double ad = fabs(d);
     return inclusive ? ad <= cell : ad < cell;
+}
+
+// Exclusion test of two points: the Chebyshev cube of half-width cell, or the
+// L2 ball dX*dX + dY*dY + dW*dW <= cell*cell (cuda/braid_cuda3d.cu:605-608),
+// summed in that order without contraction so every decision matches the
+// reference expression bit for bit.
+__device__ __forceinline__ bool pair_hit64(const UniDev& U, const double* P, const double* Q) {
+    if (!U.euclid) {
+        for (int ax = 0; ax < U.dim; ax++)
+            if (!hit1(torus_delta(P[ax] - Q[ax]), U.cell, U.inclusive)) return false;
+        return true;
+    }
+    double s = 0.0;
+    for (int ax = 0; ax < U.dim; ax++) {
+        const double d = torus_delta(P[ax] - Q[ax]);
+        s = __dadd_rn(s, __dmul_rn(d, d));
+    }
+    const double r2 = __dmul_rn(U.cell, U.cell);
+    return U.inclusive ? s <= r2 : s < r2;
 }
 
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: as
@@ -626,11 +645,10 @@ __device__ __forceinline__ bool contacts64_d(const UniDev& U, int t, const doubl
     return nbhd_scan<D>(U, t, nb, cpt, [&](int32_t p, int32_t& nx) -> bool {
         const Pt64* q = U.pts + UG_IDX((int64_t)p * U.T + t, U.slot_cap * U.T);
         nx = __ldg(&q->next);
-        bool hit = true;
+        double Q[3];
 #pragma unroll
-        for (int ax = 0; ax < D; ax++)
-            hit = hit && hit1(torus_delta(P[ax] - __ldg(&q->c[ax])), U.cell, U.inclusive);
-        if (!hit) return false;
+        for (int ax = 0; ax < D; ax++) Q[ax] = __ldg(&q->c[ax]);
+        if (!pair_hit64(U, P, Q)) return false;
         if (!group) return true;
         const int32_t gq = __ldg(&q->gid);
         if (*g == -1) {

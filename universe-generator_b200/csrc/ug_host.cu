@@ -86,7 +86,8 @@ struct Batch {
     bool synced = false;
     int max_T = 0;
     bool any_mixed = false;
-    bool any_group = false;  // some universe runs group rounds
+    bool any_group = false;   // some universe runs group rounds
+    bool any_euclid = false;  // some universe excludes by the L2 ball
     int64_t launches = 0;  // kernels issued (graph replays count every node)
     int64_t h2d = 0, d2h = 0;  // bytes copied between host and device
     int kernels_per_round = 9;
@@ -127,6 +128,7 @@ static int validate(const ug_universe_cfg& c) {
     if (c.round_size < 0 || c.round_size > (1 << 20) || (c.round_size % kTile))
         return fail(UG_EINVAL, "round_size must be a multiple of %d up to 2^20", kTile);
     if (c.cross1d && c.dim != 1) return fail(UG_EINVAL, "cross1d applies to dim 1 only");
+    if (c.euclid != 0 && c.euclid != 1) return fail(UG_EINVAL, "bad euclid flag");
     return UG_OK;
 }
 
@@ -193,6 +195,7 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
     d.nw = (c.terms ? c.terms : c.T) - 1;
     d.rng = c.rng;
     d.cross1d = c.cross1d;
+    d.euclid = c.euclid;
     d.pin = c.pin_sin1;
     d.group_mode = c.group_mode;
     d.seed = c.seed;
@@ -371,7 +374,7 @@ static int launch_round(Batch& B, bool timed) {
     te(K_PLAN);
     if (B.opts.precision == UG_PREC_MIXED && B.any_mixed) {
         tb(K_MIXED);
-        launch_prefilter_mixed(B.dU, B.dCtl, B.dInfo, B.nsm, B.any_group, B.st);
+        launch_prefilter_mixed(B.dU, B.dCtl, B.dInfo, B.nsm, B.any_group, B.any_euclid, B.st);
         te(K_MIXED);
         tb(K_CONFIRM);
         k_gray_compact<<<B.n, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
@@ -589,6 +592,7 @@ int ug_batch_create(const ug_universe_cfg* cfgs, int32_t n, const ug_run_opts* o
             B->any_mixed = true;
         }
         if (cfgs[i].group_mode != UG_GROUP_NONE) B->any_group = true;
+        if (cfgs[i].euclid) B->any_euclid = true;
     }
     if (cudaMalloc(&B->dU, sizeof(UniDev) * n) != cudaSuccess ||
         cudaMalloc(&B->dCtl, sizeof(UniCtl) * n) != cudaSuccess ||
@@ -826,7 +830,7 @@ constexpr int32_t kCkVersion = 1;
 bool same_model(const ug_universe_cfg& a, const ug_universe_cfg& b) {
     return a.dim == b.dim && a.T == b.T && a.terms == b.terms && a.rng == b.rng && a.zgrid == b.zgrid &&
            a.excl == b.excl && a.cross1d == b.cross1d && a.pin_sin1 == b.pin_sin1 && a.group_mode == b.group_mode &&
-           a.seed == b.seed;
+           a.seed == b.seed && a.euclid == b.euclid;
 }
 }  // namespace
 

@@ -770,12 +770,7 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
                             int32_t r2 = rhash_head(d, rkey_of(c.epoch, t, lin_cell(bc, d.dim, gwb)));
                             while (r2 >= 0) {
                                 const Pt64* Q = d.spos + UG_IDX((int64_t)r2 * T + t, (int64_t)d.S_max * T);
-                                if (r2 < r) {
-                                    bool hit = true;
-                                    for (int ax = 0; ax < d.dim && hit; ax++)
-                                        hit = hit1(torus_delta(P.c[ax] - Q->c[ax]), d.cell, d.inclusive);
-                                    if (hit) add(r2);
-                                }
+                                if (r2 < r && pair_hit64(d, P.c, Q->c)) add(r2);
                                 r2 = Q->next;
                             }
                         }

@@ -232,10 +232,14 @@ __device__ __noinline__ bool group_contact(const UniDev& d, int32_t p, int t, in
 // r + m of X.  Group rounds (grp != nullptr): a certain contact joins the
 // candidate to the contact's group in *grp (shared by the row's threads); a
 // certain contact with a second group rejects.
-template <int D>
+template <int D, bool kEuclid>
 __device__ __forceinline__ int test32_d(const UniDev& d, int t, const float* X, float r, float m,
                                         float inv_cell, int64_t cpt, bool* gray, int* grp) {
-    const float band = m * inv_cell + 1e-4f;
+    // L2 ball: the FP32 distance vector is within sqrt(D) m of the exact one; r 1e-6
+    // more covers the FP32 rounding of the squared sums compared below (relative
+    // 3 2^-24 each).  The cell range covers the cube of half-width r + that bound.
+    const float mE = kEuclid ? m * (D == 3 ? 1.7320508f : (D == 2 ? 1.4142136f : 1.0f)) * 1.001f + r * 1e-6f : m;
+    const float band = mE * inv_cell + 1e-4f;
     int c[D], elo[D], ehi[D];
 #pragma unroll
     for (int ax = 0; ax < D; ax++) {
@@ -250,7 +254,8 @@ __device__ __forceinline__ int test32_d(const UniDev& d, int t, const float* X, 
     Nbhd<D> nb;
     nbhd_make<D>(d, c, elo, ehi, nb);
     if (!nbhd_occ1<D>(d, t, nb)) return 0;
-    const float rin = r - m, rout = r + m;
+    const float rin = r - mE, rout = r + mE;
+    const float rin2 = rin > 0.f ? rin * rin : -1.f, rout2 = rout * rout;
     bool g = false;
     const bool deep = nbhd_scan<D>(d, t, nb, cpt, [&](int32_t p, int32_t& nx) -> bool {
         const uint4 qr = __ldg(reinterpret_cast<const uint4*>(d.ptf) + UG_IDX((int64_t)p * d.T + t, d.slot_cap * d.T));
@@ -261,11 +266,22 @@ __device__ __forceinline__ int test32_d(const UniDev& d, int t, const float* X, 
         q.next = (int32_t)qr.w;
         nx = q.next;
         bool miss = false, in = true;
+        if (kEuclid) {
+            float s2 = 0.f;
 #pragma unroll
-        for (int ax = 0; ax < D; ax++) {
-            const float dd = fabsf(torus_deltaf(X[ax] - q.c[ax]));
-            miss |= dd > rout;
-            in &= dd < rin;
+            for (int ax = 0; ax < D; ax++) {
+                const float dd = torus_deltaf(X[ax] - q.c[ax]);
+                s2 = fmaf(dd, dd, s2);
+            }
+            miss = s2 > rout2;
+            in = s2 < rin2;
+        } else {
+#pragma unroll
+            for (int ax = 0; ax < D; ax++) {
+                const float dd = fabsf(torus_deltaf(X[ax] - q.c[ax]));
+                miss |= dd > rout;
+                in &= dd < rin;
+            }
         }
         if (miss) return false;
         if (in) return grp ? group_contact(d, p, t, grp) : true;
@@ -276,11 +292,12 @@ __device__ __forceinline__ int test32_d(const UniDev& d, int t, const float* X, 
     return deep ? 1 : 0;
 }
 
+template <bool kEuclid>
 __device__ __forceinline__ int test32_at(const UniDev& d, int t, const float* X, float r, float m,
                                          float inv_cell, int64_t cpt, bool* gray, int* grp) {
-    if (d.dim == 3) return test32_d<3>(d, t, X, r, m, inv_cell, cpt, gray, grp);
-    if (d.dim == 2) return test32_d<2>(d, t, X, r, m, inv_cell, cpt, gray, grp);
-    return test32_d<1>(d, t, X, r, m, inv_cell, cpt, gray, grp);
+    if (d.dim == 3) return test32_d<3, kEuclid>(d, t, X, r, m, inv_cell, cpt, gray, grp);
+    if (d.dim == 2) return test32_d<2, kEuclid>(d, t, X, r, m, inv_cell, cpt, gray, grp);
+    return test32_d<1, false>(d, t, X, r, m, inv_cell, cpt, gray, grp);  // 1 axis: ball == cube
 }
 
 // --------------------------------------------------------------- kernel
@@ -301,7 +318,8 @@ constexpr int kMxParts = kMxThreads / kTile;
 
 // kGroup: the batch holds group-mode universes (group rounds need the join /
 // two-group logic in the neighbour scans; batches without them run without it).
-template <bool kGroup>
+// kEuclid: the batch holds universes with the L2-ball exclusion.
+template <bool kGroup, bool kEuclid>
 __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev* __restrict__ U, UniCtl* ctl,
                                                                     RoundInfo* info, MixedLaunch L) {
     extern __shared__ __align__(1024) uint8_t sm[];
@@ -555,8 +573,10 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                     if (vrej[row]) break;
                     nev++;
                     bool gr = false;
-                    if (test32_at(d, t, X, r, mt, inv_cell, cpt, &gr, (kGroup && group) ? s_grp + row : nullptr))
-                        vrej[row] = 1;
+                    int* gp = (kGroup && group) ? s_grp + row : nullptr;
+                    const int dead = (kEuclid && d.euclid) ? test32_at<true>(d, t, X, r, mt, inv_cell, cpt, &gr, gp)
+                                                           : test32_at<false>(d, t, X, r, mt, inv_cell, cpt, &gr, gp);
+                    if (dead) vrej[row] = 1;
                     if (gr) vgray[row] = 1;
                 }
             }
@@ -765,21 +785,30 @@ int mixed_init_kernels() {
     if (fit > by_tmem) req = smem_sm / (by_tmem + 1) - per_cta_reserved + 16;
     g_smem = std::max(req, g_smem);
     g_ctas_per_sm = std::max(1, std::min(by_tmem, (int)(smem_sm / (g_smem + per_cta_reserved))));
-    if (cudaFuncSetAttribute(k_prefilter_mixed<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(k_prefilter_mixed<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)g_smem) != cudaSuccess ||
-        cudaFuncSetAttribute(k_prefilter_mixed<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_prefilter_mixed<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)g_smem) != cudaSuccess ||
+        cudaFuncSetAttribute(k_prefilter_mixed<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)g_smem) != cudaSuccess ||
+        cudaFuncSetAttribute(k_prefilter_mixed<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)g_smem) != cudaSuccess)
         return UG_ECUDA;
     return UG_OK;
 }
 
 void launch_prefilter_mixed(const UniDev* dU, UniCtl* dCtl, RoundInfo* dInfo, int nsm, bool any_group,
-                            cudaStream_t st) {
+                            bool any_euclid, cudaStream_t st) {
     MixedLaunch L{(uint32_t)g_ncols, g_tpad_max, nullptr, nullptr, 0, 0, 0};
-    if (any_group)
-        k_prefilter_mixed<true><<<nsm * g_ctas_per_sm, kMxThreads, g_smem, st>>>(dU, dCtl, dInfo, L);
+    const int g = nsm * g_ctas_per_sm;
+    if (any_group && any_euclid)
+        k_prefilter_mixed<true, true><<<g, kMxThreads, g_smem, st>>>(dU, dCtl, dInfo, L);
+    else if (any_group)
+        k_prefilter_mixed<true, false><<<g, kMxThreads, g_smem, st>>>(dU, dCtl, dInfo, L);
+    else if (any_euclid)
+        k_prefilter_mixed<false, true><<<g, kMxThreads, g_smem, st>>>(dU, dCtl, dInfo, L);
     else
-        k_prefilter_mixed<false><<<nsm * g_ctas_per_sm, kMxThreads, g_smem, st>>>(dU, dCtl, dInfo, L);
+        k_prefilter_mixed<false, false><<<g, kMxThreads, g_smem, st>>>(dU, dCtl, dInfo, L);
 }
 
 int mixed_error(const UniDev* dU, int u, const UniDev& d, const MixedTables& mt, int64_t first, int64_t count,
@@ -800,7 +829,7 @@ int mixed_error(const UniDev* dU, int u, const UniDev& d, const MixedTables& mt,
     MixedLaunch L{(uint32_t)g_ncols, g_tpad_max, d32, dm, u, first, count};
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
-    k_prefilter_mixed<false><<<nsm * g_ctas_per_sm, kMxThreads, g_smem, st>>>(dU, nullptr, nullptr, L);
+    k_prefilter_mixed<false, false><<<nsm * g_ctas_per_sm, kMxThreads, g_smem, st>>>(dU, nullptr, nullptr, L);
     k_pos64<<<(int)std::min<int64_t>((count + 127) / 128, 2048), 128, 0, st>>>(dU, u, first, count, d64);
     std::vector<float> h32(n), hm(nm);
     std::vector<double> h64(n);

@@ -20,7 +20,7 @@ int mixed_setup(const ug_universe_cfg& cfg, UniDev& d, MixedTables& mt);
 void mixed_free(MixedTables& mt);
 int mixed_init_kernels();
 void launch_prefilter_mixed(const UniDev* dU, UniCtl* dCtl, RoundInfo* dInfo, int nsm, bool any_group,
-                            cudaStream_t st);
+                            bool any_euclid, cudaStream_t st);
 int mixed_error(const UniDev* dU, int u, const UniDev& d, const MixedTables& mt, int64_t first,
                 int64_t count, double* max_err, double* margin, double* max_ratio, cudaStream_t st);
 void launch_params(const UniDev* dU, int u, int64_t n, double* a2, double* a, int32_t* b, double* f,

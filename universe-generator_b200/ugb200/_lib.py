@@ -38,6 +38,7 @@ class UniverseCfg(C.Structure):
         ("seed", C.c_uint64), ("attempts", C.c_int64), ("max_n", C.c_int64),
         ("sub_attempts", C.c_int64), ("accept_rate", C.c_double),
         ("sub_accept_rate", C.c_double), ("sub_fill_rate", C.c_double),
+        ("euclid", C.c_int32), ("pad", C.c_int32),
     ]
 
 

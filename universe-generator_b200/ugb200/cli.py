@@ -28,7 +28,6 @@ from .io import curve_rows, write_curve, write_dump, write_knot_dump
 from .packer import Packer, Universe
 
 UNSUPPORTED = {
-    "--euclid-collision": "the L2-ball exclusion is not built (Chebyshev only)",
     "--angle-sample": "--angle-sample is not built",
     "--diag": "--diag probes are not built",
     "--probe-n": "--diag probes are not built",
@@ -80,7 +79,7 @@ def main(argv: list[str] | None = None, engine: str | None = None) -> int:
     curve = dump = None
     maxfreq = 0
     accept = sub_accept = sub_fill = 0.0
-    pin = subpaths = False
+    pin = subpaths = euclid = False
     sub_budget = 0.0
     sub_terms = 0
     max_n = 0
@@ -118,6 +117,10 @@ def main(argv: list[str] | None = None, engine: str | None = None) -> int:
                 terms = int(val())
             elif a == "--pin-sin1":
                 pin = True
+            elif a == "--euclid-collision":
+                if base != "braid_cuda3d":
+                    return _die("--euclid-collision is a braid_cuda3d flag (the L2-ball exclusion)")
+                euclid = True  # braid_cuda3d.cu:890-891
             elif a == "--subpaths":
                 subpaths = True
             elif a == "--sub-attempts":
@@ -165,7 +168,7 @@ def main(argv: list[str] | None = None, engine: str | None = None) -> int:
                  excl=excl, pin_sin1=int(pin), group_mode=L.GROUP_SUBPATH if subpaths else 0,
                  round_size=round_size, seed=seed, attempts=int(budget), max_n=max_n,
                  sub_attempts=int(sub_budget), accept_rate=accept, sub_accept_rate=sub_accept,
-                 sub_fill_rate=sub_fill)
+                 sub_fill_rate=sub_fill, euclid=int(euclid))
     kind = {2: "2+1", 3: "3+1", 1: "1+1"}[dim]
     print(f"{kind} (torus, phase): T={T}  modmax={max(T - 1, 2)} (maxfreq={max(T - 1, 2) + 1})  "
           f"terms={terms}  rng={'knot' if rng == L.RNG_KNOT else 'philox'}", file=sys.stderr)

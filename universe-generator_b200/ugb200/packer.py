@@ -35,6 +35,7 @@ class Universe:
     accept_rate: float = 0.0
     sub_accept_rate: float = 0.0
     sub_fill_rate: float = 0.0     # --sub-until-fill-rate (newly occupied cells per attempt)
+    euclid: int = 0                # --euclid-collision: L2 ball instead of the Chebyshev cube
 
     @property
     def nw(self) -> int:
@@ -45,7 +46,8 @@ class Universe:
                              self.cross1d, self.pin_sin1, self.group_mode, self.round_size,
                              self.seed & (2**64 - 1), int(self.attempts), int(self.max_n),
                              int(self.sub_attempts), float(self.accept_rate),
-                             float(self.sub_accept_rate), float(self.sub_fill_rate))
+                             float(self.sub_accept_rate), float(self.sub_fill_rate),
+                             int(self.euclid), 0)
 
 
 @dataclass
