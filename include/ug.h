@@ -198,6 +198,13 @@ int64_t ug_state_bytes(void);
 int ug_batch_save_state(void* h, int32_t u, void* state);
 int ug_batch_restore(void* h, int32_t u, int64_t n, const int64_t* idx, const int32_t* gid, const void* state);
 
+/* --diag probe (braid_cuda3d.cu:1645-1667): n fresh candidates of the stream keyed
+ * by `seed` (the run's own stream uses the universe seed) tested against the
+ * current packing without admitting any; proposed / accepted counts per bin of
+ * the x axis's sin1 offset a2 over [-1, 1), `bins` bins. */
+int ug_batch_probe(void* h, int32_t u, uint64_t seed, int64_t n, int32_t bins, int64_t* proposed,
+                   int64_t* accepted);
+
 /* Release all device memory of the batch. */
 int ug_batch_destroy(void* h);
 

@@ -93,3 +93,45 @@ def test_braid_cuda3d_euclid_collision(tmp_path, oracle):
     assert r.returncode == 0, r.stderr
     ref = oracle.pack(oracle.Model(dim=3, T=16, seed=3, euclid=1), 20000)
     assert f"done: N={len(ref.acc_idx)} in 20000 attempts" in r.stderr
+
+
+def test_braid_cuda3d_diag_probe(tmp_path, oracle):
+    """--diag: occupancy histogram of the accepted x over all timesteps and the probe of
+    fresh proposals against the final packing (braid_cuda3d.cu:1615-1670)."""
+    pre = tmp_path / "d"
+    r = _run("braid_cuda3d", ["-t", "12", "--seed", "2", "--attempts", "20000", "--terms", "12",
+                              "--rng", "philox", "--diag", str(pre), "--probe-n", "20000"])
+    assert r.returncode == 0, r.stderr
+    assert f"diag: wrote {pre}_occ.csv and {pre}_probe.csv (probeN=20000)" in r.stderr
+    occ = np.loadtxt(f"{pre}_occ.csv", delimiter=",", skiprows=1)
+    prb = np.loadtxt(f"{pre}_probe.csv", delimiter=",", skiprows=1)
+    n = len(oracle.pack(oracle.Model(dim=3, T=12, seed=2), 20000).acc_idx)
+    assert occ.shape == (50, 2) and int(occ[:, 1].sum()) == n * 12
+    assert int(prb[:, 1].sum()) == 20000 and 0 < int(prb[:, 2].sum()) < 20000
+    assert np.all(prb[:, 2] <= prb[:, 1])
+
+
+def test_probe_counts_match_the_oracle(ug, oracle):
+    """Probe candidates are the candidates of the stream keyed by the probe seed, tested
+    against the packing: the accepted count equals the oracle's test of the same stream."""
+    u = ug.Universe(dim=2, T=16, seed=5, attempts=20000, round_size=2048)
+    ref = oracle.pack(oracle.Model(dim=2, T=16, seed=5), 20000)
+    with ug.Packer([u]) as p:
+        p.run()
+        prop, acc = p.probe(0, n=1000, bins=50, seed=777)
+    probe_m = oracle.Model(dim=2, T=16, seed=777)
+    m = oracle.Model(dim=2, T=16, seed=5)
+    packed = [oracle.positions(m, int(i)) for i in ref.acc_idx]
+    cell = 2.0 / 16
+    free = 0
+    for i in range(1000):
+        P = oracle.positions(probe_m, i)
+        hit = False
+        for Q in packed:
+            d = np.abs(P - Q)
+            d = np.minimum(d, 2.0 - d)
+            if np.any(np.all(d <= cell, axis=0)):
+                hit = True
+                break
+        free += not hit
+    assert int(prop.sum()) == 1000 and int(acc.sum()) == free

@@ -814,6 +814,35 @@ int ug_batch_frames(void* h, int32_t u, const ug_frames_cfg* cfg, ug_frames_out*
     return rc;
 }
 
+int ug_batch_probe(void* h, int32_t u, uint64_t seed, int64_t n, int32_t bins, int64_t* proposed,
+                   int64_t* accepted) {
+    Batch* B = (Batch*)h;
+    if (!B || u < 0 || u >= B->n || n < 0 || bins < 1 || bins > 4096 || !proposed || !accepted)
+        return fail(UG_EINVAL, "bad arguments");
+    int rc = pull_ctl(*B);
+    if (rc) return rc;
+    unsigned long long* dh = nullptr;
+    CKR(cudaMalloc(&dh, sizeof(unsigned long long) * 2 * bins));
+    cudaError_t e = cudaMemsetAsync(dh, 0, sizeof(unsigned long long) * 2 * bins, B->st);
+    if (e == cudaSuccess && n > 0) {
+        const int blocks = (int)std::min<int64_t>((n + kTile - 1) / kTile, (int64_t)B->nsm * 16);
+        k_probe<<<blocks, kTile, sizeof(unsigned long long) * 2 * bins, B->st>>>(
+            B->dU, u, B->hCtl[u].n_slots, seed, n, bins, dh, dh + bins);
+        e = cudaGetLastError();
+    }
+    std::vector<unsigned long long> hh(2 * bins);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(hh.data(), dh, sizeof(unsigned long long) * 2 * bins, cudaMemcpyDeviceToHost, B->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(B->st);
+    cudaFree(dh);
+    if (e != cudaSuccess) return fail(UG_ECUDA, "probe: %s", cudaGetErrorString(e));
+    for (int i = 0; i < bins; i++) {
+        proposed[i] = (int64_t)hh[i];
+        accepted[i] = (int64_t)hh[bins + i];
+    }
+    return UG_OK;
+}
+
 // ---------------------------------------------------------- checkpoints
 
 namespace {

@@ -167,6 +167,41 @@ __device__ bool test64(const UniDev& d, int64_t n_slots, const double* alpha, co
     return false;
 }
 
+// Diagnostic probe (braid_cuda3d.cu:1650-1660): n fresh candidates of the stream
+// keyed by `seed` tested against the final packing (plain exclusion), counted per
+// bin of the x axis's sin1 offset a2 over [-1, 1).
+__global__ void __launch_bounds__(kTile) k_probe(const UniDev* __restrict__ U, int u, int64_t n_slots,
+                                                 uint64_t seed, int64_t n, int bins,
+                                                 unsigned long long* proposed, unsigned long long* accepted) {
+    extern __shared__ unsigned long long probe_hist[];  // [2][bins]
+    for (int i = threadIdx.x; i < 2 * bins; i += blockDim.x) probe_hist[i] = 0;
+    __syncthreads();
+    UniDev d = U[u];
+    d.seed = seed;
+    double alpha[3 * (kMaxF + 1)], beta[3 * (kMaxF + 1)], a2[3];
+    int32_t bj[kMaxF];
+    double wj[kMaxF];
+    const int F1 = d.F + 1;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (d.rng == RNG_KNOT)
+            gen_knot64(d, (uint64_t)i, alpha, beta, a2, bj, wj, 1);
+        else
+            for (int ax = 0; ax < d.dim; ax++) a2[ax] = gen_philox64(d, (uint64_t)i, ax, alpha + ax * F1, beta + ax * F1, 1);
+        int32_t g;
+        int nev;
+        const bool free = !test64(d, n_slots, alpha, beta, a2, false, &g, &nev);
+        int b = (int)floor((a2[0] + 1.0) * 0.5 * bins);
+        b = b < 0 ? 0 : (b >= bins ? bins - 1 : b);
+        atomicAdd(&probe_hist[b], 1ull);
+        if (free) atomicAdd(&probe_hist[bins + b], 1ull);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < bins; i += blockDim.x) {
+        if (probe_hist[i]) atomicAdd(&proposed[i], probe_hist[i]);
+        if (probe_hist[bins + i]) atomicAdd(&accepted[i], probe_hist[bins + i]);
+    }
+}
+
 __device__ __forceinline__ bool group_phase(const UniDev& d, const UniCtl& c) {
     return d.group_mode == GROUP_UNIQUE || (d.group_mode == GROUP_SUBPATH && c.phase == 2);
 }

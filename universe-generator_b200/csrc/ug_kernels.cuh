@@ -56,6 +56,8 @@ __global__ void k_surv_gen(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo*
 __global__ void k_surv_gemm(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_surv_hash(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_restore_gen(const UniDev* __restrict__ U, int u, const int64_t* __restrict__ idx, int m);
+__global__ void k_probe(const UniDev* __restrict__ U, int u, int64_t n_slots, uint64_t seed, int64_t n, int bins,
+                        unsigned long long* proposed, unsigned long long* accepted);
 __global__ void k_conflicts(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_greedy(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_commit(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);

@@ -29,8 +29,6 @@ from .packer import Packer, Universe
 
 UNSUPPORTED = {
     "--angle-sample": "--angle-sample is not built",
-    "--diag": "--diag probes are not built",
-    "--probe-n": "--diag probes are not built",
     "--nu-attempts": "the second (nu) species of braid_knot is not built",
     "--nu-div": "the second (nu) species of braid_knot is not built",
 }
@@ -59,6 +57,24 @@ def filled_cells(pos: np.ndarray, cell: float) -> np.ndarray:
     return out
 
 
+def write_diag(prefix: str, px: np.ndarray, probe, probe_n: int, nb: int = 50) -> None:
+    """--diag outputs of braid_cuda3d.cu:1615-1670: occupancy of the accepted worldlines'
+    x over every timestep, and the probe's proposed / accepted counts per x-centre bin."""
+    b = np.clip(np.floor((px.ravel() + 1.0) * 0.5 * nb).astype(np.int64), 0, nb - 1)
+    occ = np.bincount(b, minlength=nb)
+    centers = [-1.0 + (k + 0.5) * 2.0 / nb for k in range(nb)]
+    with open(f"{prefix}_occ.csv", "w") as f:
+        f.write("x_center,count\n")
+        for c, v in zip(centers, occ):
+            f.write(f"{c:.4f},{int(v)}\n")
+    prop, acc = probe
+    with open(f"{prefix}_probe.csv", "w") as f:
+        f.write("x_center,proposed,accepted\n")
+        for c, p_, a_ in zip(centers, prop, acc):
+            f.write(f"{c:.4f},{int(p_)},{int(a_)}\n")
+    print(f"diag: wrote {prefix}_occ.csv and {prefix}_probe.csv (probeN={probe_n})", file=sys.stderr)
+
+
 def main(argv: list[str] | None = None, engine: str | None = None) -> int:
     argv = list(sys.argv[1:] if argv is None else argv)
     if engine is None:
@@ -80,6 +96,8 @@ def main(argv: list[str] | None = None, engine: str | None = None) -> int:
     maxfreq = 0
     accept = sub_accept = sub_fill = 0.0
     pin = subpaths = euclid = False
+    diag = None
+    probe_n = 5_000_000
     sub_budget = 0.0
     sub_terms = 0
     max_n = 0
@@ -117,6 +135,13 @@ def main(argv: list[str] | None = None, engine: str | None = None) -> int:
                 terms = int(val())
             elif a == "--pin-sin1":
                 pin = True
+            elif a in ("--diag", "--probe-n"):
+                if base != "braid_cuda3d":
+                    return _die(f"{a} is a braid_cuda3d flag")
+                if a == "--diag":
+                    diag = val()
+                else:
+                    probe_n = int(float(val()))
             elif a == "--euclid-collision":
                 if base != "braid_cuda3d":
                     return _die("--euclid-collision is a braid_cuda3d flag (the L2-ball exclusion)")
@@ -178,7 +203,8 @@ def main(argv: list[str] | None = None, engine: str | None = None) -> int:
         st = p.stats(0)
         idx, gid = p.accepted(0)
         params = p.params(0) if dump else None
-        pos = p.positions(0) if subpaths else None
+        pos = p.positions(0) if (subpaths or diag) else None
+        probe = p.probe(0, probe_n, 50) if diag else None
         p.close()
     except L.UgError as e:
         return _die(str(e))
@@ -207,6 +233,8 @@ def main(argv: list[str] | None = None, engine: str | None = None) -> int:
             why = "accept-rate or fill-rate"
         print(f"sub done ({why}): Nsub={st.n_sub} in {sub_att} attempts, filled {st.filled}/{ncell} "
               f"cells ({100.0 * st.filled / ncell:.3f}%)", file=sys.stderr)
+    if diag:
+        write_diag(diag, pos[:, 0, :], probe, probe_n)
     if curve:
         if knot:
             with open(curve, "w") as f:

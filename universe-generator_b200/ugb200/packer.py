@@ -178,6 +178,20 @@ class Packer:
                                               C.byref(q)))
         return e.value, m.value, q.value
 
+    def probe(self, u: int = 0, n: int = 5_000_000, bins: int = 50,
+              seed: int | None = None) -> tuple[np.ndarray, np.ndarray]:
+        """--diag probe: (proposed, accepted) per x-centre bin of n fresh candidates
+        tested against the packing as it stands (braid_cuda3d.cu:1645-1667).  The
+        default stream is keyed by seed ^ 0xABCDEF1234567890, as the reference keys
+        its probe generator."""
+        if seed is None:
+            seed = (self.universes[u].seed ^ 0xABCDEF1234567890) & (2**64 - 1)
+        prop = np.zeros(bins, np.int64)
+        acc = np.zeros(bins, np.int64)
+        L.check(L.load().ug_batch_probe(self._h, u, seed, int(n), bins, prop.ctypes.data,
+                                        acc.ctypes.data))
+        return prop, acc
+
     # -- checkpoint / resume
     def checkpoint(self, u: int = 0) -> dict:
         """Everything needed to resume universe u: admissions (candidate indices in
