@@ -6,9 +6,12 @@ or the executables in universe-generator_b200/bin/ named like the reference bina
 (braidlab.engine.binary_name).  Accepted flags follow the engines' parsers
 (cuda/braid_cuda.cu:534-584, cuda/braid_cuda3d.cu:862-913, cuda/braid_knot.cu:258-289):
 the guard no-ops ``--uniform --torus --phase`` are accepted, ``--maxfreq`` must equal T
-(braid_cuda.cu:597-603), ``--smart`` is refused, and the outputs are the engines':
-curve CSV, ``--dump-params`` / ``--dump`` CSV and the stderr ``done: N=.. in .. attempts``
-line that braidlab.engine.parse_done reads.
+(braid_cuda.cu:597-603), ``--smart`` and ``--angle-sample`` are refused as the engines
+refuse them, ``--subpaths`` with ``--sub-until-accept-rate`` / ``--sub-until-fill-rate``,
+and the braid_cuda3d flags ``--euclid-collision``, ``--diag`` and ``--probe-n`` are
+supported.  The outputs are the engines': curve CSV, ``--dump-params`` / ``--dump`` CSV,
+the ``--diag`` CSVs and the stderr ``done: N=.. in .. attempts`` line that
+braidlab.engine.parse_done reads.
 
 Additions: ``--rng knot|philox`` (default knot: the reference's deterministic per-attempt
 stream, cuda/braid_knot.cu:207), ``--zgrid ref|mid``, ``--excl ref|open``,
@@ -28,7 +31,8 @@ from .io import curve_rows, write_curve, write_dump, write_knot_dump
 from .packer import Packer, Universe
 
 UNSUPPORTED = {
-    "--angle-sample": "--angle-sample is not built",
+    "--angle-sample": ("--angle-sample was removed along with the hard-wall geometry it compensated "
+                       "for; the sin1 offset is always uniform (braid_cuda3d.cu:885-889)"),
     "--nu-attempts": "the second (nu) species of braid_knot is not built",
     "--nu-div": "the second (nu) species of braid_knot is not built",
 }
