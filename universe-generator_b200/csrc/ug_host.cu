@@ -277,8 +277,15 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
         for (;; sh++) {
             const int64_t g = (d.gw + (1 << sh) - 1) >> sh;
             int64_t per = 1;
-            for (int ax = 0; ax < c.dim; ax++) per *= g;
-            bits = (int64_t)T * per;
+            if (c.dim == 3) {  // 4x4x4 bricks of 64 bits
+                const int64_t nbk = (g + 3) >> 2;
+                per = nbk * nbk * nbk;
+                bits = (int64_t)T * per * 64;
+                d.occ_nb = (int32_t)nbk;
+            } else {
+                for (int ax = 0; ax < c.dim; ax++) per *= g;
+                bits = (int64_t)T * per;
+            }
             if (bits <= ((int64_t)1 << 32) || sh >= 4) {
                 d.occ_shift = sh;
                 d.occ_gw = (int32_t)g;
