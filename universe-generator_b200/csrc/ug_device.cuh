@@ -89,16 +89,16 @@ struct UniDev {
     // occupancy bitmap: one bit per (timestep, coarse cell); a coarse cell is
     // 2^occ_shift cells per axis.  A clear bit proves the cells empty, so
     // empty neighbourhoods cost one L2-resident word instead of a grid probe.
-    // 3+1 lays the bits out in 4x4x4 bricks, one 64-bit word per brick, so a
-    // 3x3x3 neighbourhood reads ~3.4 words instead of ~9 rows
+    // 3+1 lays the bits out in 4x4x4 bricks and 2+1 in 8x8 bricks, one 64-bit
+    // word per brick, so a 3x3x3 neighbourhood reads ~3.4 words instead of ~9 rows
     uint32_t* occ;
     int32_t occ_shift;
     int32_t occ_gw;        // coarse cells per axis
-    int64_t occ_per_t;     // coarse cells (3+1: bricks) per timestep
+    int64_t occ_per_t;     // coarse cells (2+1, 3+1: bricks) per timestep
     // second level: one bit per block of 8 (occ cells) per axis, L2-resident
     uint32_t* occ1;
     int32_t occ1_gw;
-    int32_t occ_nb;        // 3+1: bricks per axis
+    int32_t occ_nb;        // 2+1 and 3+1: bricks per axis
     int64_t occ1_per_t;
     // accepted points
     Pt64* pts;             // [slot_cap * T]
@@ -470,8 +470,14 @@ __device__ __forceinline__ int64_t cells_per_t(const UniDev& U) {
 }
 
 // Bit of fine cell c at timestep t.  3+1: brick (c >> sh) >> 2, bit 16 r0 + 4 r1 + r2
-// of its 64-bit word with r = (c >> sh) & 3; 1+1 and 2+1: row-major coarse cells.
+// of its 64-bit word with r = (c >> sh) & 3; 2+1: brick (c >> sh) >> 3, bit 8 r0 + r1
+// with r = (c >> sh) & 7; 1+1: coarse cells in a row.
 __device__ __forceinline__ int64_t occ_bit(const UniDev& U, int t, const int* c) {
+    if (U.dim == 2) {
+        const int o0 = c[0] >> U.occ_shift, o1 = c[1] >> U.occ_shift;
+        const int64_t brick = (int64_t)(o0 >> 3) * U.occ_nb + (o1 >> 3);
+        return ((int64_t)t * U.occ_per_t + brick) * 64 + ((o0 & 7) << 3 | (o1 & 7));
+    }
     if (U.dim == 3) {
         const int o0 = c[0] >> U.occ_shift, o1 = c[1] >> U.occ_shift, o2 = c[2] >> U.occ_shift;
         const int64_t brick = ((int64_t)(o0 >> 2) * U.occ_nb + (o1 >> 2)) * U.occ_nb + (o2 >> 2);
@@ -693,7 +699,7 @@ __device__ __forceinline__ bool nbhd_scan3(const UniDev& U, int t, const Nbhd<3>
     return false;
 }
 
-// 1+1 and 2+1: row-major coarse cells, the last axis along the words.
+// 1+1: coarse cells along the words.
 template <int D, class Visit>
 __device__ __forceinline__ bool nbhd_scan_rows(const UniDev& U, int t, const Nbhd<D>& nb, int64_t cpt,
                                                Visit&& visit) {
@@ -757,6 +763,113 @@ __device__ __forceinline__ bool nbhd_scan_rows(const UniDev& U, int t, const Nbh
     return false;
 }
 
+// 8-bit mask x -> bits 8 i (i in x)
+__device__ __forceinline__ uint64_t spread8(uint32_t x) {
+    uint64_t r = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r |= (uint64_t)((x >> i) & 1u) << (8 * i);
+    return r;
+}
+
+// 2+1 counterpart of brick_cell_visit.
+template <class Visit>
+__device__ __forceinline__ bool brick_cell_visit2(const UniDev& U, int t, const Nbhd<2>& nb, int64_t cpt, int o0,
+                                                  int o1, Visit& visit) {
+    const int sh = U.occ_shift, gw = U.gw, w = 1 << sh;
+    const int f0e = min(gw, (o0 + 1) * w), f1e = min(gw, (o1 + 1) * w);
+    for (int f0 = o0 * w; f0 < f0e; f0++) {
+        if (cyc_dist(f0, nb.v[0][0], gw) >= nb.n[0]) continue;
+        for (int f1 = o1 * w; f1 < f1e; f1++) {
+            if (cyc_dist(f1, nb.v[1][0], gw) >= nb.n[1]) continue;
+            int32_t p = grid_head(U, t, (int64_t)f0 * gw + f1, cpt);
+            while (p >= 0) {
+                int32_t nx;
+                if (visit(p, nx)) return true;
+                p = nx;
+            }
+        }
+    }
+    return false;
+}
+
+// 2+1 neighbourhood scan over 8x8 bricks (as nbhd_scan3: at most two bricks per
+// axis, a third only across the seam of a partial last brick).
+template <class Visit>
+__device__ __forceinline__ bool nbhd_scan2(const UniDev& U, int t, const Nbhd<2>& nb, int64_t cpt,
+                                           Visit&& visit) {
+    const int sh = U.occ_shift, onb = U.occ_nb;
+    int bA[2], bB[2];
+    uint32_t mA[2], mB[2];
+    bool three = false;
+#pragma unroll
+    for (int ax = 0; ax < 2; ax++) {
+        const int oa = nb.v[ax][0] >> sh;
+        bA[ax] = oa >> 3;
+        bB[ax] = -1;
+        mA[ax] = 1u << (oa & 7);
+        mB[ax] = 0u;
+#pragma unroll
+        for (int k = 1; k < 4; k++) {
+            if (k < nb.n[ax]) {
+                const int o = nb.v[ax][k] >> sh, b = o >> 3;
+                const uint32_t bit = 1u << (o & 7);
+                if (b == bA[ax]) {
+                    mA[ax] |= bit;
+                } else if (bB[ax] < 0 || b == bB[ax]) {
+                    bB[ax] = b;
+                    mB[ax] |= bit;
+                } else {
+                    three = true;
+                }
+            }
+        }
+    }
+    const int64_t tb = (int64_t)t * U.occ_per_t;
+    const uint64_t* W = reinterpret_cast<const uint64_t*>(U.occ);
+    if (!three) {
+        uint64_t hits[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int B0 = (c & 2) ? bB[0] : bA[0], B1 = (c & 1) ? bB[1] : bA[1];
+            hits[c] = 0;
+            if (B0 < 0 || B1 < 0) continue;
+            const uint32_t M0 = (c & 2) ? mB[0] : mA[0], M1 = (c & 1) ? mB[1] : mA[1];
+            hits[c] = __ldg(W + UG_IDX(tb + (int64_t)B0 * onb + B1, U.occ_words / 2)) & ((uint64_t)M1 * spread8(M0));
+        }
+        uint32_t pend = 0;
+#pragma unroll
+        for (int c = 0; c < 4; c++) pend |= hits[c] ? 1u << c : 0u;
+        while (pend) {
+            const int c = __ffs(pend) - 1;
+            pend &= pend - 1;
+            uint64_t h = hits[0];
+#pragma unroll
+            for (int q = 1; q < 4; q++)
+                if (q == c) h = hits[q];
+            const int B0 = (c & 2) ? bB[0] : bA[0], B1 = (c & 1) ? bB[1] : bA[1];
+            while (h) {
+                const int bit = __ffsll((long long)h) - 1;
+                h &= h - 1;
+                if (brick_cell_visit2(U, t, nb, cpt, B0 * 8 + (bit >> 3), B1 * 8 + (bit & 7), visit)) return true;
+            }
+        }
+        return false;
+    }
+    for (int k0 = 0; k0 < nb.n[0]; k0++) {
+        const int f0 = nb.v[0][0] + k0 >= U.gw ? nb.v[0][0] + k0 - U.gw : nb.v[0][0] + k0;
+        if (k0 > 0 && (f0 >> sh) == ((f0 == 0 ? U.gw - 1 : f0 - 1) >> sh)) continue;
+        for (int k1 = 0; k1 < nb.n[1]; k1++) {
+            const int f1 = nb.v[1][0] + k1 >= U.gw ? nb.v[1][0] + k1 - U.gw : nb.v[1][0] + k1;
+            if (k1 > 0 && (f1 >> sh) == ((f1 == 0 ? U.gw - 1 : f1 - 1) >> sh)) continue;
+            const int cc[2] = {f0, f1};
+            const int64_t b = occ_bit(U, t, cc);
+            if (!((__ldg(U.occ + UG_IDX(b >> 5, U.occ_words)) >> (b & 31)) & 1u)) continue;
+            if (brick_cell_visit2(U, t, nb, cpt, f0 >> sh, f1 >> sh, visit)) return true;
+        }
+    }
+    return false;
+}
+
 // Visit the chains of the occupied cells of the neighbourhood at timestep t.
 // visit(p) returns true to stop (the scan then returns true).
 template <int D, class Visit>
@@ -764,6 +877,8 @@ __device__ __forceinline__ bool nbhd_scan(const UniDev& U, int t, const Nbhd<D>&
                                           Visit&& visit) {
     if constexpr (D == 3) {
         return nbhd_scan3(U, t, nb, cpt, visit);
+    } else if constexpr (D == 2) {
+        return nbhd_scan2(U, t, nb, cpt, visit);
     } else {
         return nbhd_scan_rows<D>(U, t, nb, cpt, visit);
     }

@@ -282,6 +282,11 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
                 per = nbk * nbk * nbk;
                 bits = (int64_t)T * per * 64;
                 d.occ_nb = (int32_t)nbk;
+            } else if (c.dim == 2) {  // 8x8 bricks of 64 bits
+                const int64_t nbk = (g + 7) >> 3;
+                per = nbk * nbk;
+                bits = (int64_t)T * per * 64;
+                d.occ_nb = (int32_t)nbk;
             } else {
                 for (int ax = 0; ax < c.dim; ax++) per *= g;
                 bits = (int64_t)T * per;
