@@ -33,7 +33,7 @@ import numpy as np  # noqa: E402
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes (read + write) per k_prefilter_mixed launch over one complete job of the
 # workload, from the 1-pass ncu capture in profiles/k_prefilter_mixed_c3_dram.md
-PREFILTER_TRAFFIC = {("c3", "mixed"): 1.668e9}
+PREFILTER_TRAFFIC = {("c3", "mixed"): 1.245e9}
 FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
 
 
@@ -357,19 +357,37 @@ def main() -> int:
     pk_name = "k_prefilter_mixed" if prec == ugb200.PREC_MIXED else "k_prefilter64"
     pk_ms, pk_n = kt.get(pk_name, (0.0, 0))
     evals = sum(s.evals for s in st)
-    flops = sum(2 * u.dim * ((u.T - 1) + u.T // 2) * s.evals for u, s in zip(us, st))
     P, src = peaks()
-    achieved = flops / (pk_ms / 1000.0) / 1e12 if pk_ms > 0 else 0.0
-    peak = P["bf16_tflops"]
+    pk_s = pk_ms / 1000.0
+    avg_s = pk_s / max(pk_n, 1)
     traffic = PREFILTER_TRAFFIC.get((args.workload, args.precision))
-    avg_s = pk_ms / max(pk_n, 1) / 1000.0
-    roofline = {"bound": "tensor", "kernel": pk_name, "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": traffic,
-                "peak_source": f"{src} bf16 dense (burst)",
-                "hbm": ({"achieved_gbs": traffic / avg_s / 1e9, "peak_gbs": P["hbm_gbs"],
-                         "frac": traffic / avg_s / 1e9 / P["hbm_gbs"]} if traffic and avg_s > 0 else None),
+    # algorithmic units of the prefilter (per launch = job total / launches):
+    #  tensor: the contraction 2 d K T per candidate (K = (F-1) + F/2; split-BF16 counted once;
+    #          the mixed path evaluates all T timesteps of every candidate)
+    #  HBM:    per examined (candidate, timestep) the 3^d neighbour cell offsets (8 B each) plus
+    #          (4d + 4) B per accepted point examined; a 1+1 crossing test examines one
+    #          stored point per (path, timestep): 8 B
+    mixed = prec == ugb200.PREC_MIXED
+    flops = sum(2 * u.dim * ((u.T - 1) + u.T // 2) * (u.T * s.attempts if mixed else s.evals)
+                for u, s in zip(us, st))
+    hbm_bytes = sum((8 * s.evals) if (u.dim == 1 and u.cross1d)
+                    else (3 ** u.dim * 8 * s.evals + (4 * u.dim + 4) * s.visits)
+                    for u, s in zip(us, st))
+    t_ach = flops / pk_s / 1e12 if pk_s > 0 else 0.0
+    h_ach = hbm_bytes / pk_s / 1e9 if pk_s > 0 else 0.0
+    t_frac, h_frac = t_ach / P["bf16_tflops"], h_ach / P["hbm_gbs"]
+    tensor = {"achieved": t_ach, "peak": P["bf16_tflops"], "unit": "TFLOP/s", "frac": t_frac,
+              "flops_per_launch": flops / max(pk_n, 1), "peak_source": f"{src} bf16 dense (burst)"}
+    hbm = {"achieved": h_ach, "peak": P["hbm_gbs"], "unit": "GB/s", "frac": h_frac,
+           "bytes_per_launch": hbm_bytes / max(pk_n, 1), "peak_source": f"{src} copy bandwidth",
+           "dram_gbs": traffic / avg_s / 1e9 if traffic and avg_s > 0 else None}
+    main = hbm if h_frac >= t_frac else tensor  # the bound is the larger fraction
+    roofline = {"bound": "hbm" if main is hbm else "tensor", "kernel": pk_name,
+                "achieved": main["achieved"], "peak": main["peak"], "unit": main["unit"],
+                "frac": main["frac"], "traffic": traffic, "tensor": tensor, "hbm": hbm,
                 "launches": pk_n, "avg_launch_ms": pk_ms / max(pk_n, 1),
-                "evals": evals, "kernel_share": {k: v[0] for k, v in kt.items()}}
+                "evals": evals, "visits": sum(s.visits for s in st),
+                "kernel_share": {k: v[0] for k, v in kt.items()}}
 
     # the plain FP64 single-universe form on the same B200 and the same seeds: one
     # universe per packer, thread-per-candidate FP64 prefilter (the metric's denominator)

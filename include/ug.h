@@ -100,6 +100,7 @@ typedef struct ug_stats {
     int32_t grid_kind;  /* 0 dense, 1 hash */
     int64_t filled;     /* occupied (timestep, cell) buckets of the collision grid
                            (the `filled` of braid_cuda.cu:695, 877) */
+    int64_t visits;     /* accepted points examined by the prefilter's neighbour tests */
 } ug_stats;
 
 /* Per-kernel device time accumulated while kernel_timing is on. */

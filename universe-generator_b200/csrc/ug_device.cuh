@@ -168,6 +168,7 @@ struct UniCtl {
     int64_t hash_used;     // main grid hash entries in use
     int64_t n_slots_prev;  // n_slots before this round's commit
     int64_t evals;         // prefilter (candidate, timestep) position evaluations
+    int64_t visits;        // prefilter: accepted points examined by the neighbour tests
     int64_t evals_fp64;    // of which evaluated in FP64 (plain path / guard-band retest)
     int32_t stop_at;       // survivors [0, stop_at) resolved this round
     int32_t pad2;
@@ -891,7 +892,7 @@ __device__ __forceinline__ bool nbhd_scan(const UniDev& U, int t, const Nbhd<D>&
 // touched group in *g and returns true when a second distinct group appears.
 template <int D>
 __device__ __forceinline__ bool contacts64_d(const UniDev& U, int t, const double* P, bool group,
-                                             int32_t* g, int64_t cpt) {
+                                             int32_t* g, int64_t cpt, int* nvis) {
     int c[D], z[D];
 #pragma unroll
     for (int ax = 0; ax < D; ax++) {
@@ -904,6 +905,7 @@ __device__ __forceinline__ bool contacts64_d(const UniDev& U, int t, const doubl
     return nbhd_scan<D>(U, t, nb, cpt, [&](int32_t p, int32_t& nx) -> bool {
         const Pt64* q = U.pts + UG_IDX((int64_t)p * U.T + t, U.slot_cap * U.T);
         nx = __ldg(&q->next);
+        if (nvis) ++*nvis;
         double Q[3];
 #pragma unroll
         for (int ax = 0; ax < D; ax++) Q[ax] = __ldg(&q->c[ax]);
@@ -919,10 +921,10 @@ __device__ __forceinline__ bool contacts64_d(const UniDev& U, int t, const doubl
 }
 
 __device__ __forceinline__ bool contacts64(const UniDev& U, int t, const double* P, bool group,
-                                           int32_t* g, int64_t cpt) {
-    if (U.dim == 3) return contacts64_d<3>(U, t, P, group, g, cpt);
-    if (U.dim == 2) return contacts64_d<2>(U, t, P, group, g, cpt);
-    return contacts64_d<1>(U, t, P, group, g, cpt);
+                                           int32_t* g, int64_t cpt, int* nvis = nullptr) {
+    if (U.dim == 3) return contacts64_d<3>(U, t, P, group, g, cpt, nvis);
+    if (U.dim == 2) return contacts64_d<2>(U, t, P, group, g, cpt, nvis);
+    return contacts64_d<1>(U, t, P, group, g, cpt, nvis);
 }
 
 // 1+1D crossing rule: minimum-image separation changes sign between

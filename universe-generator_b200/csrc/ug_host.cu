@@ -722,6 +722,7 @@ int ug_batch_stats(void* h, int32_t u, ug_stats* out) {
     out->state = k.state;
     out->grid_kind = B->U[u].d.grid_kind;
     out->filled = k.filled + k.round_new;
+    out->visits = k.visits;
     return UG_OK;
 }
 

@@ -129,7 +129,7 @@ __global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* inf
 // FP64 test of candidate idx against the committed packing.  Returns true
 // when it is rejected.  Group mode: *g gets the single group touched (-1 none).
 __device__ bool test64(const UniDev& d, int64_t n_slots, const double* alpha, const double* beta,
-                       const double* a2, bool group, int32_t* g, int* nev) {
+                       const double* a2, bool group, int32_t* g, int* nev, int* nvis = nullptr) {
     *g = -1;
     const int T = d.T, F1 = d.F + 1;
     if (d.dim == 1 && d.cross1d) {
@@ -162,7 +162,7 @@ __device__ bool test64(const UniDev& d, int64_t n_slots, const double* alpha, co
         double P[3];
         for (int ax = 0; ax < d.dim; ax++) P[ax] = eval64(d, alpha + ax * F1, beta + ax * F1, 1, a2[ax], t);
         *nev = oi + 1;
-        if (contacts64(d, t, P, group, g, cpt)) return true;
+        if (contacts64(d, t, P, group, g, cpt, nvis)) return true;
     }
     return false;
 }
@@ -226,7 +226,7 @@ __device__ __forceinline__ void prefilter64_tiles(const UniDev* __restrict__ U, 
         if (kGrayOnly && work) work = (d.gray_bits[off >> 5] >> (off & 31)) & 1u;
         bool surv = false;
         int32_t g = -1;
-        int nev = 0;
+        int nev = 0, nvis = 0;
         if (work) {
             const uint64_t idx = (uint64_t)(c.round_base + off);
             const int F1 = d.F + 1;
@@ -236,9 +236,11 @@ __device__ __forceinline__ void prefilter64_tiles(const UniDev* __restrict__ U, 
                 for (int ax = 0; ax < d.dim; ax++)
                     a2[ax] = gen_philox64(d, idx, ax, alpha + ax * F1, beta + ax * F1, 1);
             }
-            surv = !test64(d, c.n_slots, alpha, beta, a2, group_phase(d, c), &g, &nev);
+            surv = !test64(d, c.n_slots, alpha, beta, a2, group_phase(d, c), &g, &nev, kGrayOnly ? nullptr : &nvis);
         }
         for (int o = 16; o > 0; o >>= 1) nev += __shfl_xor_sync(0xffffffffu, nev, o);
+        for (int o = 16; o > 0; o >>= 1) nvis += __shfl_xor_sync(0xffffffffu, nvis, o);
+        if (lane == 0 && nvis) atomicAdd((unsigned long long*)&ctl[u].visits, (unsigned long long)nvis);
         if (lane == 0 && nev) {
             atomicAdd((unsigned long long*)&ctl[u].evals_fp64, (unsigned long long)nev);
             if (!kGrayOnly) atomicAdd((unsigned long long*)&ctl[u].evals, (unsigned long long)nev);

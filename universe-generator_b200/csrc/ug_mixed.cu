@@ -234,7 +234,7 @@ __device__ __noinline__ bool group_contact(const UniDev& d, int32_t p, int t, in
 // certain contact with a second group rejects.
 template <int D, bool kEuclid>
 __device__ __forceinline__ int test32_d(const UniDev& d, int t, const float* X, float r, float m,
-                                        float inv_cell, int64_t cpt, bool* gray, int* grp) {
+                                        float inv_cell, int64_t cpt, bool* gray, int* grp, int* nvis) {
     // L2 ball: the FP32 distance vector is within sqrt(D) m of the exact one; r 1e-6
     // more covers the FP32 rounding of the squared sums compared below (relative
     // 3 2^-24 each).  The cell range covers the cube of half-width r + that bound.
@@ -265,6 +265,7 @@ __device__ __forceinline__ int test32_d(const UniDev& d, int t, const float* X, 
         q.c[2] = __uint_as_float(qr.z);
         q.next = (int32_t)qr.w;
         nx = q.next;
+        ++*nvis;
         bool miss = false, in = true;
         if (kEuclid) {
             float s2 = 0.f;
@@ -294,10 +295,10 @@ __device__ __forceinline__ int test32_d(const UniDev& d, int t, const float* X, 
 
 template <bool kEuclid>
 __device__ __forceinline__ int test32_at(const UniDev& d, int t, const float* X, float r, float m,
-                                         float inv_cell, int64_t cpt, bool* gray, int* grp) {
-    if (d.dim == 3) return test32_d<3, kEuclid>(d, t, X, r, m, inv_cell, cpt, gray, grp);
-    if (d.dim == 2) return test32_d<2, kEuclid>(d, t, X, r, m, inv_cell, cpt, gray, grp);
-    return test32_d<1, false>(d, t, X, r, m, inv_cell, cpt, gray, grp);  // 1 axis: ball == cube
+                                         float inv_cell, int64_t cpt, bool* gray, int* grp, int* nvis) {
+    if (d.dim == 3) return test32_d<3, kEuclid>(d, t, X, r, m, inv_cell, cpt, gray, grp, nvis);
+    if (d.dim == 2) return test32_d<2, kEuclid>(d, t, X, r, m, inv_cell, cpt, gray, grp, nvis);
+    return test32_d<1, false>(d, t, X, r, m, inv_cell, cpt, gray, grp, nvis);  // 1 axis: ball == cube
 }
 
 // --------------------------------------------------------------- kernel
@@ -410,7 +411,7 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
             s_gray[row] = 0;
             s_grp[row] = -1;
         }
-        int nev = 0;
+        int nev = 0, nvis = 0;
         for (int pass = 0; pass < d.mx_npass && !timeout; pass++) {
             if (pass > 0 && __syncthreads_and(vrej[row] != 0)) break;
             for (int ax = 0; ax < dim && !timeout; ax++) {
@@ -574,8 +575,8 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                     nev++;
                     bool gr = false;
                     int* gp = (kGroup && group) ? s_grp + row : nullptr;
-                    const int dead = (kEuclid && d.euclid) ? test32_at<true>(d, t, X, r, mt, inv_cell, cpt, &gr, gp)
-                                                           : test32_at<false>(d, t, X, r, mt, inv_cell, cpt, &gr, gp);
+                    const int dead = (kEuclid && d.euclid) ? test32_at<true>(d, t, X, r, mt, inv_cell, cpt, &gr, gp, &nvis)
+                                                           : test32_at<false>(d, t, X, r, mt, inv_cell, cpt, &gr, gp, &nvis);
                     if (dead) vrej[row] = 1;
                     if (gr) vgray[row] = 1;
                 }
@@ -585,7 +586,9 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
         }
         if (!dump) {
             for (int o = 16; o > 0; o >>= 1) nev += __shfl_xor_sync(0xffffffffu, nev, o);
+            for (int o = 16; o > 0; o >>= 1) nvis += __shfl_xor_sync(0xffffffffu, nvis, o);
             if (lane == 0 && nev) atomicAdd((unsigned long long*)&ctl[u].evals, (unsigned long long)nev);
+            if (lane == 0 && nvis) atomicAdd((unsigned long long*)&ctl[u].visits, (unsigned long long)nvis);
             if (part == 0) {
                 const bool rej = vrej[row] != 0, gry = vgray[row] != 0;
                 const bool surv = valid && !rej && !gry && !timeout;

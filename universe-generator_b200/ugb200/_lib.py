@@ -57,6 +57,7 @@ class Stats(C.Structure):
         ("attempts", C.c_int64), ("phase1_end", C.c_int64), ("rounds", C.c_int64),
         ("gray", C.c_int64), ("evals", C.c_int64), ("evals_fp64", C.c_int64),
         ("state", C.c_int32), ("grid_kind", C.c_int32), ("filled", C.c_int64),
+        ("visits", C.c_int64),
     ]
 
 

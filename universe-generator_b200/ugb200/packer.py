@@ -64,6 +64,7 @@ class Stats:
     done: bool
     grid: str
     filled: int = 0              # occupied (timestep, cell) buckets of the collision grid
+    visits: int = 0              # accepted points examined by the prefilter's neighbour tests
 
 
 @dataclass
@@ -118,7 +119,7 @@ class Packer:
         L.check(L.load().ug_batch_stats(self._h, u, C.byref(s)))
         return Stats(s.n, s.n_unique, s.n_sub, s.attempts, s.phase1_end, s.rounds, s.gray,
                      s.evals, s.evals_fp64, s.state == 1, "hash" if s.grid_kind else "dense",
-                     s.filled)
+                     s.filled, s.visits)
 
     def accepted(self, u: int = 0) -> tuple[np.ndarray, np.ndarray]:
         lib = L.load()
