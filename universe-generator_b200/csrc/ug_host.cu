@@ -406,7 +406,7 @@ static int launch_round(Batch& B, bool timed) {
                                                                                      B.dInfo);
     te(K_SGEN);
     tb(K_SGEMM);
-    k_surv_gemm<<<B.nsm * 4, 128, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+    k_surv_gemm<<<B.nsm * 4, 128, kGemmSmem, B.st>>>(B.dU, B.dCtl, B.dInfo);
     te(K_SGEMM);
     tb(K_SHASH);
     k_surv_hash<<<B.nsm * 8, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
@@ -984,7 +984,7 @@ int ug_batch_restore(void* h, int32_t u, int64_t n, const int64_t* idx, const in
         if (e == cudaSuccess) e = cudaMemsetAsync(d.spos, 0, (size_t)m * T * sizeof(Pt64), B->st);  // unused axes
         if (e == cudaSuccess) {
             k_restore_gen<<<B->nsm * 4, 32 * kSurvWarps, kSurvWarps * kSurvSmemPerWarp, B->st>>>(B->dU, u, dIdx, m);
-            k_surv_gemm<<<B->nsm * 4, 128, 0, B->st>>>(B->dU, B->dCtl, B->dInfo);
+            k_surv_gemm<<<B->nsm * 4, 128, kGemmSmem, B->st>>>(B->dU, B->dCtl, B->dInfo);
             k_commit<<<B->nsm * 8, 256, 0, B->st>>>(B->dU, B->dCtl, B->dInfo);
             e = cudaGetLastError();
         }

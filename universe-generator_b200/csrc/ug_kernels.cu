@@ -496,13 +496,29 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_restore_gen(const UniDev* _
     }
 }
 
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // k_surv_gemm: X[row][t] = wrap(a2 + invsinz_t * sum_k coef[k][row] KT[k][t]),
 // one warp per 32-row x 32-timestep tile.  Lane (rg, tg) owns rows
 // row0 + 0..3 and timesteps t0 + 8 jj + {0,1}; every (row, t) is a single FMA
-// chain in ascending k, i.e. eval64's operations in eval64's order.
+// chain in ascending k, i.e. eval64's operations in eval64's order.  Each warp
+// streams its tile's A rows and B columns through shared memory in chunks of
+// kGemmKC terms, two stages deep (cp.async), so the next chunk is in flight while
+// the current one is multiplied.
 __global__ void __launch_bounds__(128) k_surv_gemm(const UniDev* __restrict__ U, UniCtl* ctl,
                                                    RoundInfo* info) {
-    const int lane = threadIdx.x & 31;
+    extern __shared__ __align__(16) double gemm_smem[];  // [warp][stage][A | B][kGemmKC][32]
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double* wsm = gemm_smem + (size_t)wib * (2 * 2 * kGemmKC * 32);
     const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
     const int n_uni = info->n_uni, total = info->total_sev;
@@ -516,29 +532,57 @@ __global__ void __launch_bounds__(128) k_surv_gemm(const UniDev* __restrict__ U,
         const int rb = local / ntb, tb = local - rb * ntb;
         const int row0 = rb * 32 + rg * 4;
         const int t0 = tb * 32 + 2 * tg;
-        const double* A = d.coef + row0;
-        const double* Bt = d.KT + t0;
+        const double* Ag = d.coef + rb * 32;  // tile rows [rb*32, rb*32+32) < Rpad
+        const double* Bg = d.KT + tb * 32;    // tile timesteps [tb*32, tb*32+32) < Tpad
+        // chunk ch: terms [ch*KC, min(K, ch*KC+KC)), 16-byte pieces (16 per 32-double row)
+        auto issue = [&](int stage, int k0) {
+            double* As = wsm + stage * (2 * kGemmKC * 32);
+            double* Bs = As + kGemmKC * 32;
+            for (int i = lane; i < kGemmKC * 16; i += 32) {
+                const int kk = i >> 4, pc = (i & 15) * 2;
+                if (k0 + kk < K) {
+                    cp_async16(As + kk * 32 + pc, Ag + (size_t)(k0 + kk) * R + pc);
+                    cp_async16(Bs + kk * 32 + pc, Bg + (size_t)(k0 + kk) * TP + pc);
+                }
+            }
+            cp_async_commit();
+        };
         double acc[4][8];
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
             for (int j = 0; j < 8; j++) acc[i][j] = 0.0;
-#pragma unroll 2
-        for (int k = 0; k < K; k++) {
-            const double2 a01 = __ldg((const double2*)(A + (size_t)k * R));
-            const double2 a23 = __ldg((const double2*)(A + (size_t)k * R + 2));
-            const double av[4] = {a01.x, a01.y, a23.x, a23.y};
-            double bv[8];
-#pragma unroll
-            for (int jj = 0; jj < 4; jj++) {
-                const double2 b2 = __ldg((const double2*)(Bt + (size_t)k * TP + 8 * jj));
-                bv[2 * jj] = b2.x;
-                bv[2 * jj + 1] = b2.y;
+        const int nch = (K + kGemmKC - 1) / kGemmKC;
+        issue(0, 0);
+        for (int ch = 0; ch < nch; ch++) {
+            if (ch + 1 < nch) {
+                issue((ch + 1) & 1, (ch + 1) * kGemmKC);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
             }
+            __syncwarp();
+            const double* As = wsm + (ch & 1) * (2 * kGemmKC * 32) + rg * 4;
+            const double* Bs = wsm + (ch & 1) * (2 * kGemmKC * 32) + kGemmKC * 32 + 2 * tg;
+            const int kn = min(kGemmKC, K - ch * kGemmKC);
+#pragma unroll 4
+            for (int kk = 0; kk < kn; kk++) {
+                const double2 a01 = *(const double2*)(As + kk * 32);
+                const double2 a23 = *(const double2*)(As + kk * 32 + 2);
+                const double av[4] = {a01.x, a01.y, a23.x, a23.y};
+                double bv[8];
 #pragma unroll
-            for (int i = 0; i < 4; i++)
+                for (int jj = 0; jj < 4; jj++) {
+                    const double2 b2 = *(const double2*)(Bs + kk * 32 + 8 * jj);
+                    bv[2 * jj] = b2.x;
+                    bv[2 * jj + 1] = b2.y;
+                }
 #pragma unroll
-                for (int j = 0; j < 8; j++) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int j = 0; j < 8; j++) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+            }
+            __syncwarp();  // the stage is refilled by the issue of chunk ch + 2
         }
         const int nrows = ctl[u].S * dim;
         [[maybe_unused]] const int64_t nspos = (int64_t)d.S_max * T;

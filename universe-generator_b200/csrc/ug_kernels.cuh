@@ -63,6 +63,10 @@ __global__ void k_greedy(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* i
 __global__ void k_commit(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_rehash(const UniDev* __restrict__ U, UniCtl* ctl, int u, int64_t n_slots);
 
+// k_surv_gemm: terms per shared-memory chunk; two stages of A and B per warp.
+constexpr int kGemmKC = 8;
+constexpr size_t kGemmSmem = (size_t)4 * 2 * 2 * kGemmKC * 32 * sizeof(double);  // 4 warps per CTA
+
 // Shared memory of k_surv_gen per warp (bytes), for F <= kMaxF.
 constexpr int kSurvWarps = 4;
 constexpr size_t kSurvSmemPerWarpBase = (size_t)3 * (kMaxF + 1) * 2 * sizeof(double) + 3 * sizeof(double) +
