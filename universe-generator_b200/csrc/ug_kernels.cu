@@ -603,9 +603,12 @@ __global__ void __launch_bounds__(128) k_surv_gemm(const UniDev* __restrict__ U,
     }
 }
 
-// Round hash block of a cell: 2 cells per axis, so the 3 neighbour cells of
-// a point span at most 2 blocks per axis (3 at the seam of an odd gw).
-__device__ __forceinline__ int rblock_gw(const UniDev& d) { return (d.gw + 1) >> 1; }
+// Round hash block of a cell: 2 cells per axis, so the 3 neighbour cells of a
+// point span at most 2 blocks per axis (3 at the seam of an odd gw).  Measured
+// on c3 against 4- and 8-cell blocks (fewer probes, longer chains): 108 ms
+// against 140 and 116 ms of k_conflicts per job.
+constexpr int kRBlockShift = 1;  // cells per round-hash block per axis: 1 << kRBlockShift
+__device__ __forceinline__ int rblock_gw(const UniDev& d) { return (d.gw + (1 << kRBlockShift) - 1) >> kRBlockShift; }
 
 // k_surv_hash: one thread per survivor timestep inserts the point into the
 // round hash (key: epoch, t, block).
@@ -621,7 +624,7 @@ __global__ void __launch_bounds__(256) k_surv_hash(const UniDev* __restrict__ U,
         const int r = local / T, t = local - r * T;
         Pt64* q = d.spos + UG_IDX((int64_t)r * T + t, (int64_t)d.S_max * T);
         int bc[3];
-        for (int ax = 0; ax < d.dim; ax++) bc[ax] = cell_of(q->c[ax], d.cell, d.gw) >> 1;
+        for (int ax = 0; ax < d.dim; ax++) bc[ax] = cell_of(q->c[ax], d.cell, d.gw) >> kRBlockShift;
         for (int ax = d.dim; ax < 3; ax++) q->c[ax] = 0.0;
         const uint64_t key = rkey_of(c.epoch, t, lin_cell(bc, d.dim, rblock_gw(d)));
         const uint64_t h = rhash_claim(d, key);
@@ -835,9 +838,9 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
                 }
                 for (int ax = 0; ax < d.dim; ax++) {
                     const int c0 = cell_of(P.c[ax], d.cell, gw);
-                    const int v0 = (c0 == 0 ? gw - 1 : c0 - 1) >> 1;
-                    const int v1 = c0 >> 1;
-                    const int v2 = (c0 == gw - 1 ? 0 : c0 + 1) >> 1;
+                    const int v0 = (c0 == 0 ? gw - 1 : c0 - 1) >> kRBlockShift;
+                    const int v1 = c0 >> kRBlockShift;
+                    const int v2 = (c0 == gw - 1 ? 0 : c0 + 1) >> kRBlockShift;
                     int n = 0;
                     bl[ax][n++] = v0;
                     if (v1 != v0) bl[ax][n++] = v1;
