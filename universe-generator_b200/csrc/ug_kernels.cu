@@ -894,7 +894,71 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
     int k = 0, stop_at = S_eff;
     int64_t n_unique = c.n_unique, n_sub = c.n_sub;
     bool grow = false, hit_max = false, undecided = false;
-    for (int r = 0; r < S_eff; r++) {
+    // Plain rounds: 32 survivors per step.  Each lane gathers its survivor's
+    // listed contacts -- admitted ones from earlier steps (certain rejection)
+    // and a bit mask of the earlier lanes of this step -- and the warp then
+    // decides the 32 in index order from those masks: the same decisions as the
+    // one-at-a-time loop below, which group rounds use.
+    for (int r0 = 0; !group && r0 < S_eff; r0 += 32) {
+        const int r = r0 + lane, nvalid = min(32, S_eff - r0);
+        uint32_t dep = 0;
+        bool ext = false, over = false;
+        if (lane < nvalid) {
+            const int n_all = d.ccount[UG_IDX(r, d.S_max)];
+            over = n_all > kConflictCap;
+            const int n = over ? kConflictCap : n_all;
+            const int32_t* lst = d.clist + UG_IDX((int64_t)r * kConflictCap, (int64_t)d.S_max * kConflictCap);
+            for (int i = 0; i < n; i++) {
+                const int r2 = lst[i];
+                if (r2 < r0)
+                    ext |= acc_s[UG_IDX(r2, kSmaxCap)] >= 0;
+                else
+                    dep |= 1u << (r2 - r0);
+            }
+        }
+        uint32_t accm = 0;
+        int stop = -1;
+        for (int j = 0; j < nvalid; j++) {
+            if (k + __popc(accm) >= room) {
+                stop = j;
+                grow = true;
+                break;
+            }
+            const uint32_t dj = __shfl_sync(0xffffffffu, dep, j);
+            const bool ej = __shfl_sync(0xffffffffu, ext, j);
+            const bool oj = __shfl_sync(0xffffffffu, over, j);
+            const bool acc = !ej && !(dj & accm);
+            if (acc && oj) {  // an unlisted contact might be admitted: decide next round
+                stop = j;
+                undecided = true;
+                break;
+            }
+            if (acc) {
+                accm |= 1u << j;
+                if (c.phase == 1 && c.max_n > 0 && n_unique + __popc(accm) >= c.max_n) {
+                    stop = j + 1;
+                    hit_max = true;
+                    break;
+                }
+            }
+        }
+        const int lim = stop < 0 ? nvalid : stop;
+        if (lane < lim) {
+            const bool a = (accm >> lane) & 1u;
+            const int rank = k + __popc(accm & ((1u << lane) - 1u));
+            acc_s[UG_IDX(r, kSmaxCap)] = a ? rank : -1;
+            gid_s[UG_IDX(r, kSmaxCap)] = a ? (int32_t)(c.n_slots + rank) : -1;
+        }
+        __syncwarp();
+        const uint32_t taken = accm & (lim >= 32 ? 0xffffffffu : ((1u << lim) - 1u));
+        k += __popc(taken);
+        n_unique += __popc(taken);
+        if (stop >= 0) {
+            stop_at = r0 + stop;
+            break;
+        }
+    }
+    for (int r = 0; group && r < S_eff; r++) {
         if (k >= room) {
             stop_at = r;
             grow = true;
