@@ -316,6 +316,7 @@ struct MixedLaunch {
 
 constexpr int kMxThreads = 512;  // 4 threads per candidate row
 constexpr int kMxParts = kMxThreads / kTile;
+constexpr int kMxCompact = 16;   // live rows of a warp at or below which their tests are spread
 
 // kGroup: the batch holds group-mode universes (group rounds need the join /
 // two-group logic in the neighbour scans; batches without them run without it).
@@ -554,6 +555,45 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                 for (int ax = 0; ax < dim; ax++)
                     tmem_ld8(lane_base + (uint32_t)UG_IDX(ax * nm + c0 + 7, L.ncols) - 7, x[ax]);
                 tmem_wait_ld();
+                // Few live rows: spread their (row, column) tests over all 32 lanes, column
+                // by column, instead of leaving the dead rows' lanes idle.  The staged
+                // positions live in this warp's slice of the (now idle) operand stages.
+                const uint32_t am = dump ? 0u : __ballot_sync(0xffffffffu, valid && !vrej[row]);
+                const int na = __popc(am);
+                if (!dump && na <= kMxCompact) {
+                    if (na == 0) continue;
+                    const int ncol = min(8, T - col0);
+                    float* xs = reinterpret_cast<float*>(sm) + warp * (8 * 3 * 32 + 32);  // [8][3][32] + rho[32]
+#pragma unroll
+                    for (int j = 0; j < 8; j++)
+#pragma unroll
+                        for (int ax = 0; ax < 3; ax++)
+                            if (j < ncol && ax < dim)
+                                xs[(j * 3 + ax) * 32 + lane] = torus_wrapf(fmaf(x[ax][j], inv_sum[ax], a2f[ax]));
+                    xs[8 * 3 * 32 + lane] = rho;
+                    __syncwarp();
+                    const int nitems = na * ncol;
+                    for (int i = lane; i < nitems; i += 32) {
+                        const int j = i / na, src = __fns(am, 0, i - j * na + 1);
+                        const int rrow = (warp & 3) * 32 + src;
+                        if (vrej[rrow]) continue;
+                        const int t = __ldg(d.order + col0 + j);
+                        float X[3];
+                        for (int ax = 0; ax < dim; ax++) X[ax] = xs[(j * 3 + ax) * 32 + src];
+                        const float bnd = fminf(2.f, 2.f * (float)__ldg(d.invsinz + t) * xs[8 * 3 * 32 + src]);
+                        const float mt = (2.f * d.mx_mc1 * bnd + d.mx_mc0) * 1.01f;
+                        nev++;
+                        bool gr = false;
+                        int* gp = (kGroup && group) ? s_grp + rrow : nullptr;
+                        const int dead = (kEuclid && d.euclid)
+                                             ? test32_at<true>(d, t, X, r, mt, inv_cell, cpt, &gr, gp, &nvis)
+                                             : test32_at<false>(d, t, X, r, mt, inv_cell, cpt, &gr, gp, &nvis);
+                        if (dead) vrej[rrow] = 1;
+                        if (gr) vgray[rrow] = 1;
+                    }
+                    __syncwarp();
+                    continue;
+                }
                 for (int j = 0; j < 8; j++) {
                     const int col = col0 + j;
                     if (col >= T) break;
