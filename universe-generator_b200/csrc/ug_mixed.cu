@@ -316,7 +316,7 @@ struct MixedLaunch {
 
 constexpr int kMxThreads = 512;  // 4 threads per candidate row
 constexpr int kMxParts = kMxThreads / kTile;
-constexpr int kMxCompact = 16;   // live rows of a warp at or below which their tests are spread
+constexpr int kMxCompact = 24;   // live rows of a warp at or below which their tests are spread (16, 24, 32 measured)
 
 // kGroup: the batch holds group-mode universes (group rounds need the join /
 // two-group logic in the neighbour scans; batches without them run without it).
