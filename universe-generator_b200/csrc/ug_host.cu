@@ -88,6 +88,7 @@ struct Batch {
     bool any_mixed = false;
     bool any_group = false;   // some universe runs group rounds
     bool any_euclid = false;  // some universe excludes by the L2 ball
+    bool any_knot = false;    // some universe draws from the knot stream
     int64_t launches = 0;  // kernels issued (graph replays count every node)
     int64_t h2d = 0, d2h = 0;  // bytes copied between host and device
     int kernels_per_round = 9;
@@ -402,8 +403,10 @@ static int launch_round(Batch& B, bool timed) {
     k_compact<<<B.n, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
     te(K_COMPACT);
     tb(K_SGEN);
-    k_surv_gen<<<B.nsm * 4, 32 * kSurvWarps, kSurvWarps * kSurvSmemPerWarp, B.st>>>(B.dU, B.dCtl,
-                                                                                     B.dInfo);
+    {
+        const int wb = (int)(B.any_knot ? kSurvSmemPerWarp : kSurvSmemAxis);
+        k_surv_gen<<<B.nsm * 8, 32 * kSurvWarps, kSurvWarps * wb, B.st>>>(B.dU, B.dCtl, B.dInfo, wb);
+    }
     te(K_SGEN);
     tb(K_SGEMM);
     k_surv_gemm<<<B.nsm * 4, 128, kGemmSmem, B.st>>>(B.dU, B.dCtl, B.dInfo);
@@ -605,6 +608,7 @@ int ug_batch_create(const ug_universe_cfg* cfgs, int32_t n, const ug_run_opts* o
         }
         if (cfgs[i].group_mode != UG_GROUP_NONE) B->any_group = true;
         if (cfgs[i].euclid) B->any_euclid = true;
+        if (cfgs[i].rng == UG_RNG_KNOT) B->any_knot = true;
     }
     if (cudaMalloc(&B->dU, sizeof(UniDev) * n) != cudaSuccess ||
         cudaMalloc(&B->dCtl, sizeof(UniCtl) * n) != cudaSuccess ||

@@ -452,10 +452,10 @@ __device__ __forceinline__ void store_coef_rows(const UniDev& d, int r, const do
 // the same operations as the thread-per-candidate prefilter, so identical
 // values) and stores them as rows r * dim + ax of the term-ordered matrix coef.
 __global__ void __launch_bounds__(32 * kSurvWarps) k_surv_gen(const UniDev* __restrict__ U,
-                                                                UniCtl* ctl, RoundInfo* info) {
+                                                                UniCtl* ctl, RoundInfo* info, int warp_bytes) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    unsigned char* my = smem_raw + (size_t)wib * kSurvSmemPerWarp;
+    unsigned char* my = smem_raw + (size_t)wib * warp_bytes;
     double* alpha = (double*)my;
     double* beta = alpha + 3 * (kMaxF + 1);
     double* a2 = beta + 3 * (kMaxF + 1);
@@ -469,6 +469,53 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_surv_gen(const UniDev* __re
         const UniDev& d = U[u];
         const UniCtl& c = ctl[u];
         const uint64_t idx = (uint64_t)(c.round_base + d.surv_off[UG_IDX(r, d.S_max + 1)]);
+        if (d.rng == RNG_PHILOX) {
+            // one axis at a time in a (F+1)-entry buffer pair, rows written as they are
+            // finished: warp_gen64's operations per axis, a quarter of its shared memory
+            const int F = d.F, R = d.Rpad;
+            [[maybe_unused]] const int64_t ncoef = (int64_t)d.K * R;
+            double* al = (double*)my;
+            double* bt = al + (kMaxF + 1);
+            for (int ax = 0; ax < d.dim; ax++) {
+                const int row = r * d.dim + ax;
+                for (int p = lane; 2 * p <= F; p += 32) {
+                    const uint4 o = philox_block(d.seed, idx, ax, p);
+                    if (p == 0) {
+                        d.a2row[UG_IDX(row, R)] = d.pin ? 0.0 : (double)o.x * (1.0 / 2147483648.0) - 1.0;
+                        continue;
+                    }
+                    const int be = 2 * p, bo = 2 * p + 1;
+                    const double Ee = -log(((double)o.x + 0.5) * (1.0 / 4294967296.0));
+                    al[be] = (o.z & 1u) ? -Ee : Ee;
+                    bt[be] = (double)(o.z >> 1) * (1.0 / 2147483648.0) * kPi;
+                    if (bo <= F) {
+                        const double Eo = -log(((double)o.y + 0.5) * (1.0 / 4294967296.0));
+                        al[bo] = (o.w & 1u) ? -Eo : Eo;
+                    }
+                }
+                __syncwarp();
+                double sum = 0.0;
+                if (lane == 0)
+                    for (int b = 2; b <= F; b++) sum += fabs(al[b]);
+                sum = __shfl_sync(0xffffffffu, sum, 0);
+                for (int b = 2 + lane; b <= F; b += 32) {
+                    const double e = al[b];
+                    double amp = fabs(e) / sum / (double)b;
+                    if (e < 0.0) amp = -amp;
+                    const int64_t k = kseq_s(b);
+                    if (b & 1) {
+                        d.coef[UG_IDX(k * R + row, ncoef)] = amp;
+                    } else {
+                        double sf, cf;
+                        sincos(bt[b], &sf, &cf);
+                        d.coef[UG_IDX(k * R + row, ncoef)] = amp * cf;
+                        d.coef[UG_IDX((k + 1) * R + row, ncoef)] = amp * sf;
+                    }
+                }
+                __syncwarp();
+            }
+            continue;
+        }
         warp_gen64(d, idx, alpha, beta, a2, bj, wj, lane);
         store_coef_rows(d, r, alpha, beta, a2, lane);
         __syncwarp();

@@ -52,7 +52,7 @@ __global__ void k_prefilter64(const UniDev* __restrict__ U, UniCtl* ctl, RoundIn
 __global__ void k_gray_compact(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_confirm64w(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_compact(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
-__global__ void k_surv_gen(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
+__global__ void k_surv_gen(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info, int warp_bytes);
 __global__ void k_surv_gemm(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_surv_hash(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_restore_gen(const UniDev* __restrict__ U, int u, const int64_t* __restrict__ idx, int m);
@@ -72,6 +72,8 @@ constexpr int kSurvWarps = 4;
 constexpr size_t kSurvSmemPerWarpBase = (size_t)3 * (kMaxF + 1) * 2 * sizeof(double) + 3 * sizeof(double) +
                                     (size_t)kMaxF * (sizeof(int32_t) + sizeof(double));
 constexpr size_t kSurvSmemPerWarp = kSurvSmemPerWarpBase;
+// k_surv_gen on a batch without knot-stream universes: one axis of alpha / beta
+constexpr size_t kSurvSmemAxis = (size_t)2 * (kMaxF + 1) * sizeof(double);
 // k_confirm64w adds the FP64 trajectory of a 1+1D candidate
 constexpr size_t kConfSmemPerWarp = kSurvSmemPerWarpBase + (size_t)kMaxF * sizeof(double);
 
