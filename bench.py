@@ -143,6 +143,19 @@ def cpu_baseline(us, budget_s: float = 20.0):
                       f"{secs:.1f} s; oracle threaded prefilter + in-order recheck"}
 
 
+def combine_ranks(t_ms: float, cands: int, dist, device: str):
+    """Whole-job numbers of a multi-rank run: the slowest rank's device time and the
+    candidates of all ranks (each rank packs its own universes; no data-path
+    collective, only these two reductions)."""
+    import torch
+
+    t = torch.tensor([float(t_ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([int(cands)], dtype=torch.int64, device=device)
+    dist.all_reduce(c)
+    return float(t.item()), int(c.item())
+
+
 def frames_line(packer):
     """c4's second stage: frame_bake of the packed universe (last timed job), 256 instants
     z_obs in [0.25, 0.75] pi, one path observer, the 'fit' front, a 1024 x 1024 uint32
@@ -322,12 +335,7 @@ def main() -> int:
         sampler.wait()
     t_ms = float(sum(times))
     if dist:
-        t = torch.tensor([t_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
-        c = torch.tensor([float(cands)], device="cuda")
-        dist.all_reduce(c)
-        cands = int(c.item())
+        t_ms, cands = combine_ranks(t_ms, cands, dist, "cuda")
     value = cands / (t_ms / 1000.0)
 
     # end to end through the public API with host buffers
