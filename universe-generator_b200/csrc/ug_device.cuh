@@ -228,14 +228,18 @@ __device__ __forceinline__ bool hit1(double d, double cell, int inclusive) {
 // reference expression bit for bit.
 __device__ __forceinline__ bool pair_hit64(const UniDev& U, const double* P, const double* Q) {
     if (!U.euclid) {
-        for (int ax = 0; ax < U.dim; ax++)
-            if (!hit1(torus_delta(P[ax] - Q[ax]), U.cell, U.inclusive)) return false;
+#pragma unroll
+        for (int ax = 0; ax < 3; ax++)
+            if (ax < U.dim && !hit1(torus_delta(P[ax] - Q[ax]), U.cell, U.inclusive)) return false;
         return true;
     }
     double s = 0.0;
-    for (int ax = 0; ax < U.dim; ax++) {
-        const double d = torus_delta(P[ax] - Q[ax]);
-        s = __dadd_rn(s, __dmul_rn(d, d));
+#pragma unroll
+    for (int ax = 0; ax < 3; ax++) {
+        if (ax < U.dim) {
+            const double d = torus_delta(P[ax] - Q[ax]);
+            s = __dadd_rn(s, __dmul_rn(d, d));
+        }
     }
     const double r2 = __dmul_rn(U.cell, U.cell);
     return U.inclusive ? s <= r2 : s < r2;
@@ -444,9 +448,13 @@ __device__ __forceinline__ uint64_t mix64(uint64_t k) {
     return k;
 }
 
+// Loops over the axes run to the constant 3 (dim <= 3) so that callers' cell
+// arrays stay in registers.
 __device__ __forceinline__ int64_t lin_cell(const int* c, int dim, int gw) {
     int64_t lin = 0;
-    for (int ax = 0; ax < dim; ax++) lin = lin * gw + c[ax];
+#pragma unroll
+    for (int ax = 0; ax < 3; ax++)
+        if (ax < dim) lin = lin * gw + c[ax];
     return lin;
 }
 
@@ -466,7 +474,9 @@ __device__ __forceinline__ int32_t grid_head(const UniDev& U, int t, int64_t lin
 
 __device__ __forceinline__ int64_t cells_per_t(const UniDev& U) {
     int64_t n = 1;
-    for (int ax = 0; ax < U.dim; ax++) n *= U.gw;
+#pragma unroll
+    for (int ax = 0; ax < 3; ax++)
+        if (ax < U.dim) n *= U.gw;
     return n;
 }
 
@@ -484,13 +494,13 @@ __device__ __forceinline__ int64_t occ_bit(const UniDev& U, int t, const int* c)
         const int64_t brick = ((int64_t)(o0 >> 2) * U.occ_nb + (o1 >> 2)) * U.occ_nb + (o2 >> 2);
         return ((int64_t)t * U.occ_per_t + brick) * 64 + ((o0 & 3) << 4 | (o1 & 3) << 2 | (o2 & 3));
     }
-    int64_t lin = 0;
-    for (int ax = 0; ax < U.dim; ax++) lin = lin * U.occ_gw + (c[ax] >> U.occ_shift);
-    return (int64_t)t * U.occ_per_t + lin;
+    return (int64_t)t * U.occ_per_t + (c[0] >> U.occ_shift);  // dim 1
 }
 __device__ __forceinline__ int64_t occ1_bit(const UniDev& U, int t, const int* c) {
     int64_t lin = 0;
-    for (int ax = 0; ax < U.dim; ax++) lin = lin * U.occ1_gw + (c[ax] >> (U.occ_shift + 3));
+#pragma unroll
+    for (int ax = 0; ax < 3; ax++)
+        if (ax < U.dim) lin = lin * U.occ1_gw + (c[ax] >> (U.occ_shift + 3));
     return (int64_t)t * U.occ1_per_t + lin;
 }
 

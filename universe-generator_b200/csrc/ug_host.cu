@@ -415,7 +415,9 @@ static int launch_round(Batch& B, bool timed) {
     k_surv_hash<<<B.nsm * 8, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
     te(K_SHASH);
     tb(K_CONFL);
-    k_conflicts<<<B.nsm * 8, 128, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+    // 16 four-warp CTAs per SM: 48 registers allow 10 resident (40 warps); on c3
+    // 104 ms per job against 108 ms with 8 per SM
+    k_conflicts<<<B.nsm * 16, 128, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
     te(K_CONFL);
     tb(K_GREEDY);
     k_greedy<<<B.n, 32, 2 * kSmaxCap * sizeof(int32_t), B.st>>>(B.dU, B.dCtl, B.dInfo);

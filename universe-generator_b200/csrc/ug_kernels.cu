@@ -655,6 +655,7 @@ __global__ void __launch_bounds__(128) k_surv_gemm(const UniDev* __restrict__ U,
 // on c3 against 4- and 8-cell blocks (fewer probes, longer chains): 108 ms
 // against 140 and 116 ms of k_conflicts per job.
 constexpr int kRBlockShift = 1;  // cells per round-hash block per axis: 1 << kRBlockShift
+static_assert(((2 * kMaxF) >> kRBlockShift) <= 1024, "k_conflicts packs block coordinates in 10 bits");
 __device__ __forceinline__ int rblock_gw(const UniDev& d) { return (d.gw + (1 << kRBlockShift) - 1) >> kRBlockShift; }
 
 // k_surv_hash: one thread per survivor timestep inserts the point into the
@@ -670,9 +671,14 @@ __global__ void __launch_bounds__(256) k_surv_hash(const UniDev* __restrict__ U,
         const int local = w - info->spt_off[u];
         const int r = local / T, t = local - r * T;
         Pt64* q = d.spos + UG_IDX((int64_t)r * T + t, (int64_t)d.S_max * T);
-        int bc[3];
-        for (int ax = 0; ax < d.dim; ax++) bc[ax] = cell_of(q->c[ax], d.cell, d.gw) >> kRBlockShift;
-        for (int ax = d.dim; ax < 3; ax++) q->c[ax] = 0.0;
+        int bc[3] = {0, 0, 0};
+#pragma unroll
+        for (int ax = 0; ax < 3; ax++) {
+            if (ax < d.dim)
+                bc[ax] = cell_of(q->c[ax], d.cell, d.gw) >> kRBlockShift;
+            else
+                q->c[ax] = 0.0;
+        }
         const uint64_t key = rkey_of(c.epoch, t, lin_cell(bc, d.dim, rblock_gw(d)));
         const uint64_t h = rhash_claim(d, key);
         int32_t nxt = -1;
@@ -877,34 +883,39 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
             const int gw = d.gw, gwb = rblock_gw(d);
             for (int t = lane; t < T; t += 32) {
                 const Pt64 P = d.spos[UG_IDX((int64_t)r * T + t, (int64_t)d.S_max * T)];
-                // distinct round-hash blocks of the 3 neighbour cells per axis
-                int bl[3][3], nbk[3];
+                // distinct round-hash blocks of the 3 neighbour cells per axis:
+                // bl[ax] packs up to three 10-bit block coordinates, nbk[ax] counts them
+                // (registers only: every index below is a compile-time constant)
+                uint32_t bl[3] = {0u, 0u, 0u};
+                int nbk[3] = {1, 1, 1};
+#pragma unroll
                 for (int ax = 0; ax < 3; ax++) {
-                    nbk[ax] = 1;
-                    bl[ax][0] = bl[ax][1] = bl[ax][2] = 0;
+                    if (ax < d.dim) {
+                        const int c0 = cell_of(P.c[ax], d.cell, gw);
+                        const uint32_t v0 = (uint32_t)((c0 == 0 ? gw - 1 : c0 - 1) >> kRBlockShift);
+                        const uint32_t v1 = (uint32_t)(c0 >> kRBlockShift);
+                        const uint32_t v2 = (uint32_t)((c0 == gw - 1 ? 0 : c0 + 1) >> kRBlockShift);
+                        uint32_t pk = v0;
+                        int n = 1;
+                        if (v1 != v0) pk |= v1 << (10 * n++);
+                        if (v2 != v0 && v2 != v1) pk |= v2 << (10 * n++);
+                        bl[ax] = pk;
+                        nbk[ax] = n;
+                    }
                 }
-                for (int ax = 0; ax < d.dim; ax++) {
-                    const int c0 = cell_of(P.c[ax], d.cell, gw);
-                    const int v0 = (c0 == 0 ? gw - 1 : c0 - 1) >> kRBlockShift;
-                    const int v1 = c0 >> kRBlockShift;
-                    const int v2 = (c0 == gw - 1 ? 0 : c0 + 1) >> kRBlockShift;
-                    int n = 0;
-                    bl[ax][n++] = v0;
-                    if (v1 != v0) bl[ax][n++] = v1;
-                    if (v2 != v0 && v2 != v1) bl[ax][n++] = v2;
-                    nbk[ax] = n;
+                const int n12 = nbk[1] * nbk[2], nall = nbk[0] * n12;
+                for (int m = 0; m < nall; m++) {
+                    const int i0 = m / n12, rem = m - i0 * n12;
+                    const int i1 = rem / nbk[2], i2 = rem - i1 * nbk[2];
+                    const int bc[3] = {(int)((bl[0] >> (10 * i0)) & 1023u), (int)((bl[1] >> (10 * i1)) & 1023u),
+                                       (int)((bl[2] >> (10 * i2)) & 1023u)};
+                    int32_t r2 = rhash_head(d, rkey_of(c.epoch, t, lin_cell(bc, d.dim, gwb)));
+                    while (r2 >= 0) {
+                        const Pt64* Q = d.spos + UG_IDX((int64_t)r2 * T + t, (int64_t)d.S_max * T);
+                        if (r2 < r && pair_hit64(d, P.c, Q->c)) add(r2);
+                        r2 = Q->next;
+                    }
                 }
-                for (int i0 = 0; i0 < nbk[0]; i0++)
-                    for (int i1 = 0; i1 < nbk[1]; i1++)
-                        for (int i2 = 0; i2 < nbk[2]; i2++) {
-                            const int bc[3] = {bl[0][i0], bl[1][i1], bl[2][i2]};
-                            int32_t r2 = rhash_head(d, rkey_of(c.epoch, t, lin_cell(bc, d.dim, gwb)));
-                            while (r2 >= 0) {
-                                const Pt64* Q = d.spos + UG_IDX((int64_t)r2 * T + t, (int64_t)d.S_max * T);
-                                if (r2 < r && pair_hit64(d, P.c, Q->c)) add(r2);
-                                r2 = Q->next;
-                            }
-                        }
             }
         }
         __syncwarp();
@@ -1214,8 +1225,10 @@ __global__ void __launch_bounds__(256) k_commit(const UniDev* __restrict__ U, Un
             if (k >= 0) {
                 const int64_t slot = UG_IDX(c.n_slots_prev + k, d.slot_cap);
                 Pt64 q = d.spos[UG_IDX((int64_t)r * d.T + t, (int64_t)d.S_max * d.T)];
-                int cc[3];
-                for (int ax = 0; ax < d.dim; ax++) cc[ax] = cell_of(q.c[ax], d.cell, d.gw);
+                int cc[3] = {0, 0, 0};
+#pragma unroll
+                for (int ax = 0; ax < 3; ax++)
+                    if (ax < d.dim) cc[ax] = cell_of(q.c[ax], d.cell, d.gw);
                 int32_t old;
                 grid_insert(d, c, t, lin_cell(cc, d.dim, d.gw), cells_per_t(d), (int32_t)slot, &old, &new_key);
                 new_cell = old < 0;
@@ -1259,8 +1272,10 @@ __global__ void k_rehash(const UniDev* __restrict__ U, UniCtl* ctl, int u, int64
         const int64_t slot = w / d.T;
         const int t = (int)(w % d.T);
         Pt64* q = d.pts + slot * d.T + t;
-        int cc[3];
-        for (int ax = 0; ax < d.dim; ax++) cc[ax] = cell_of(q->c[ax], d.cell, d.gw);
+        int cc[3] = {0, 0, 0};
+#pragma unroll
+        for (int ax = 0; ax < 3; ax++)
+            if (ax < d.dim) cc[ax] = cell_of(q->c[ax], d.cell, d.gw);
         int32_t old;
         bool new_key = false;
         grid_insert(d, c, t, lin_cell(cc, d.dim, d.gw), cells_per_t(d), (int32_t)slot, &old, &new_key);
