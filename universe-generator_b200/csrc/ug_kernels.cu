@@ -974,30 +974,38 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
                     dep |= 1u << (r2 - r0);
             }
         }
-        uint32_t accm = 0;
+        // In-order greedy over the step's lanes: a lane decides once every lane it
+        // depends on has decided (dependencies point to lower lanes only, so the
+        // lowest undecided lane is always ready; one pass per link of the longest
+        // dependency chain, usually one).
+        const uint32_t valid = nvalid >= 32 ? 0xffffffffu : ((1u << nvalid) - 1u);
+        uint32_t und = valid, accm = 0;
+        while (und) {
+            const bool ready = ((und >> lane) & 1u) && !(dep & und);
+            accm |= __ballot_sync(0xffffffffu, ready && !ext && !(dep & accm));
+            und &= ~__ballot_sync(0xffffffffu, ready);
+        }
+        // Where the one-at-a-time scan would stop: at lane j it first checks the
+        // room left (stop before j), then an admitted j with an over-full list
+        // (undecided: stop before j), then the unique cap (stop after j).
+        const int acc_before = __popc(accm & ((1u << lane) - 1u));
+        const bool mine = (accm >> lane) & 1u;
+        const uint32_t b_room = __ballot_sync(0xffffffffu, lane < nvalid && k + acc_before >= room);
+        const uint32_t b_over = __ballot_sync(0xffffffffu, mine && over);
+        const uint32_t b_max = __ballot_sync(
+            0xffffffffu, mine && c.phase == 1 && c.max_n > 0 && n_unique + acc_before + 1 >= c.max_n);
         int stop = -1;
-        for (int j = 0; j < nvalid; j++) {
-            if (k + __popc(accm) >= room) {
+        if (b_room | b_over | b_max) {
+            const int j = __ffs(b_room | b_over | b_max) - 1;
+            if ((b_room >> j) & 1u) {
                 stop = j;
                 grow = true;
-                break;
-            }
-            const uint32_t dj = __shfl_sync(0xffffffffu, dep, j);
-            const bool ej = __shfl_sync(0xffffffffu, ext, j);
-            const bool oj = __shfl_sync(0xffffffffu, over, j);
-            const bool acc = !ej && !(dj & accm);
-            if (acc && oj) {  // an unlisted contact might be admitted: decide next round
+            } else if ((b_over >> j) & 1u) {
                 stop = j;
                 undecided = true;
-                break;
-            }
-            if (acc) {
-                accm |= 1u << j;
-                if (c.phase == 1 && c.max_n > 0 && n_unique + __popc(accm) >= c.max_n) {
-                    stop = j + 1;
-                    hit_max = true;
-                    break;
-                }
+            } else {
+                stop = j + 1;
+                hit_max = true;
             }
         }
         const int lim = stop < 0 ? nvalid : stop;
