@@ -111,8 +111,8 @@ struct UniDev {
     int32_t* surv_off;     // [S_max]  candidate offset within the round
     int32_t* gray_off;     // [B_max]  mixed: offsets of candidates sent to the FP64 retest
     Pt64* spos;            // [S_max * T]
-    uint64_t* rkeys;       // round hash keys [rcap]: epoch<<40 | t<<31 | cell
-    uint64_t* rvals;       // [rcap]: epoch<<32 | head survivor rank
+    ulonglong2* rslot;     // round hash [rcap]: x = key epoch<<40 | t<<31 | block,
+                           // y = epoch<<32 | head survivor rank (one 16-byte sector part)
     uint64_t rmask;
     int32_t* ccount;       // [S_max]
     int32_t* clist;        // [S_max * kConflictCap]

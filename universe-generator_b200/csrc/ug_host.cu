@@ -326,7 +326,7 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
         (rc = dalloc(h, &d.sgid, Sm, 0xff)) || (rc = dalloc(h, &d.acc_rank, Sm, 0xff)))
         return rc;
     const int64_t rcap = pow2_at_least(2LL * Sm * T);
-    if ((rc = dalloc(h, &d.rkeys, rcap, 0xff)) || (rc = dalloc(h, &d.rvals, rcap, 0xff))) return rc;
+    if ((rc = dalloc(h, &d.rslot, rcap, 0xff))) return rc;
     d.rmask = (uint64_t)(rcap - 1);
     return UG_OK;
 }
@@ -941,7 +941,7 @@ int ug_batch_restore(void* h, int32_t u, int64_t n, const int64_t* idx, const in
     }
     CKR(cudaMemsetAsync(d.occ, 0, (size_t)U.occ_words * sizeof(uint32_t), B->st));
     CKR(cudaMemsetAsync(d.occ1, 0, (size_t)U.occ1_words * sizeof(uint32_t), B->st));
-    CKR(cudaMemsetAsync(d.rkeys, 0xff, (size_t)(d.rmask + 1) * sizeof(uint64_t), B->st));
+    CKR(cudaMemsetAsync(d.rslot, 0xff, (size_t)(d.rmask + 1) * sizeof(ulonglong2), B->st));
     // room for the admissions and the next rounds
     if (n + (int64_t)d.S_max * 2 > d.slot_cap) {
         CKR(cudaStreamSynchronize(B->st));
