@@ -83,8 +83,8 @@ struct UniDev {
     // main grid
     int32_t grid_kind;
     int32_t pad1;
-    int32_t* heads;        // dense: [T * gw^dim]; hash: values [hcap]
-    uint64_t* hkeys;       // hash keys [hcap]
+    int32_t* heads;        // dense: chain heads [T * gw^dim]
+    ulonglong2* hslot;     // hash [hcap]: x = key t<<40 | cell, y = head slot (low 32 bits)
     uint64_t hmask;        // hcap - 1
     // occupancy bitmap: one bit per (timestep, coarse cell); a coarse cell is
     // 2^occ_shift cells per axis.  A clear bit proves the cells empty, so
@@ -464,9 +464,9 @@ __device__ __forceinline__ int32_t grid_head(const UniDev& U, int t, int64_t lin
     const uint64_t key = ((uint64_t)t << 40) | (uint64_t)lin;
     uint64_t h = mix64(key) & U.hmask;
     for (uint64_t probe = 0; probe <= U.hmask; probe++) {
-        const uint64_t k = __ldg(U.hkeys + UG_IDX(h, U.hmask + 1));
-        if (k == key) return __ldg(U.heads + UG_IDX(h, U.hmask + 1));
-        if (k == kEmptyKey) return -1;
+        const ulonglong2 s = __ldg(U.hslot + UG_IDX(h, U.hmask + 1));  // key and head in one load
+        if (s.x == key) return (int32_t)(uint32_t)s.y;
+        if (s.x == kEmptyKey) return -1;
         h = (h + 1) & U.hmask;
     }
     return -1;

@@ -172,15 +172,12 @@ static int alloc_points(UniHost& h, int64_t cap) {
     return UG_OK;
 }
 
+// Hash grid of cap slots, all empty (key and head all ones: no key, head -1).
 static int alloc_hash(UniHost& h, int64_t cap) {
-    uint64_t* k = nullptr;
-    int32_t* v = nullptr;
-    CKR(cudaMalloc(&k, (size_t)cap * sizeof(uint64_t)));
-    CKR(cudaMalloc(&v, (size_t)cap * sizeof(int32_t)));
-    CKR(cudaMemset(k, 0xff, (size_t)cap * sizeof(uint64_t)));
-    CKR(cudaMemset(v, 0xff, (size_t)cap * sizeof(int32_t)));
-    h.d.hkeys = k;
-    h.d.heads = v;
+    ulonglong2* s = nullptr;
+    CKR(cudaMalloc(&s, (size_t)cap * sizeof(ulonglong2)));
+    CKR(cudaMemset(s, 0xff, (size_t)cap * sizeof(ulonglong2)));
+    h.d.hslot = s;
     h.d.hmask = (uint64_t)(cap - 1);
     h.hcap = cap;
     return UG_OK;
@@ -499,12 +496,10 @@ static int ensure_capacity(Batch& B, int rounds) {
         if (h.d.grid_kind == GRID_HASH) {
             const int64_t need_keys = k.hash_used + (int64_t)rounds * h.d.S_max * h.cfg.T;
             if (need_keys * 2 > h.hcap) {
-                uint64_t* ok = h.d.hkeys;
-                int32_t* ov = h.d.heads;
+                ulonglong2* os = h.d.hslot;
                 int rc = alloc_hash(h, pow2_at_least(need_keys * 4));
                 if (rc) return rc;
-                cudaFree(ok);
-                cudaFree(ov);
+                cudaFree(os);
                 int64_t zero = 0;
                 k.hash_used = 0;
                 CKR(cudaMemcpyAsync(&B.dCtl[i].hash_used, &zero, sizeof zero, cudaMemcpyHostToDevice, B.st));
@@ -689,8 +684,7 @@ int ug_batch_reset(void* h, const uint64_t* seeds) {
             for (int ax = 0; ax < u.d.dim; ax++) cpt *= u.d.gw;
             CKR(cudaMemsetAsync(u.d.heads, 0xff, (size_t)u.d.T * cpt * sizeof(int32_t), B->st));
         } else {
-            CKR(cudaMemsetAsync(u.d.hkeys, 0xff, (size_t)u.hcap * sizeof(uint64_t), B->st));
-            CKR(cudaMemsetAsync(u.d.heads, 0xff, (size_t)u.hcap * sizeof(int32_t), B->st));
+            CKR(cudaMemsetAsync(u.d.hslot, 0xff, (size_t)u.hcap * sizeof(ulonglong2), B->st));
         }
         CKR(cudaMemsetAsync(u.d.occ, 0, (size_t)u.occ_words * sizeof(uint32_t), B->st));
         CKR(cudaMemsetAsync(u.d.occ1, 0, (size_t)u.occ1_words * sizeof(uint32_t), B->st));
@@ -931,12 +925,10 @@ int ug_batch_restore(void* h, int32_t u, int64_t n, const int64_t* idx, const in
         const int64_t need = std::max<int64_t>(1 << 16, pow2_at_least((n * T + (int64_t)d.S_max * T) * 4));
         if (need > U.hcap) {
             CKR(cudaStreamSynchronize(B->st));
-            cudaFree(d.hkeys);
-            cudaFree(d.heads);
+            cudaFree(d.hslot);
             if ((rc = alloc_hash(U, need))) return rc;
         } else {
-            CKR(cudaMemsetAsync(d.hkeys, 0xff, (size_t)U.hcap * sizeof(uint64_t), B->st));
-            CKR(cudaMemsetAsync(d.heads, 0xff, (size_t)U.hcap * sizeof(int32_t), B->st));
+            CKR(cudaMemsetAsync(d.hslot, 0xff, (size_t)U.hcap * sizeof(ulonglong2), B->st));
         }
     }
     CKR(cudaMemsetAsync(d.occ, 0, (size_t)U.occ_words * sizeof(uint32_t), B->st));
@@ -1064,10 +1056,7 @@ int ug_batch_destroy(void* h) {
     if (B->gexec) cudaGraphExecDestroy(B->gexec);
     for (UniHost& u : B->U) {
         for (void* p : u.owned) cudaFree(p);
-        if (u.d.grid_kind == GRID_HASH) {
-            cudaFree(u.d.hkeys);
-            cudaFree(u.d.heads);
-        }
+        if (u.d.grid_kind == GRID_HASH) cudaFree(u.d.hslot);
         cudaFree(u.d.pts);
         cudaFree(u.d.ptf);
         cudaFree(u.d.acc_idx);

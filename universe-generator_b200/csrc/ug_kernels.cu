@@ -1185,9 +1185,10 @@ __device__ __forceinline__ void grid_insert(const UniDev& d, UniCtl& c, int t, i
     const uint64_t key = ((uint64_t)t << 40) | (uint64_t)lin;
     uint64_t h = mix64(key) & d.hmask;
     for (uint64_t probe = 0; probe <= d.hmask; probe++) {
-        uint64_t k = __ldcg(d.hkeys + h);
+        unsigned long long* kp = &d.hslot[h].x;
+        uint64_t k = __ldcg(kp);
         if (k == kEmptyKey) {
-            const uint64_t prev = atomicCAS((unsigned long long*)(d.hkeys + h), kEmptyKey, key);
+            const uint64_t prev = atomicCAS(kp, kEmptyKey, key);
             if (prev == kEmptyKey) {
                 *new_key = true;
                 k = key;
@@ -1196,7 +1197,7 @@ __device__ __forceinline__ void grid_insert(const UniDev& d, UniCtl& c, int t, i
             }
         }
         if (k == key) {
-            *old_head = atomicExch(d.heads + h, slot);
+            *old_head = (int32_t)(uint32_t)atomicExch(&d.hslot[h].y, (unsigned long long)(uint32_t)slot);
             return;
         }
         h = (h + 1) & d.hmask;
