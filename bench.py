@@ -33,7 +33,7 @@ import numpy as np  # noqa: E402
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes (read + write) per k_prefilter_mixed launch over one complete job of the
 # workload, from the 1-pass ncu capture in profiles/k_prefilter_mixed_c3_dram.md
-PREFILTER_TRAFFIC = {("c3", "mixed"): 1.245e9}
+PREFILTER_TRAFFIC = {("c3", "mixed"): 1.267e9}
 FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
 
 

@@ -342,10 +342,13 @@ __device__ __forceinline__ uint64_t rkey_of(int epoch, int t, int64_t lin) {
     return ((uint64_t)(epoch & 0xFFFFFF) << 40) | ((uint64_t)t << 31) | (uint64_t)lin;
 }
 
+// Home slot of a round-hash key.
+__device__ __forceinline__ uint64_t rhash_home(const UniDev& d, uint64_t key) { return mix64(key) & d.rmask; }
+
 // Round hash slot holding `key` (claiming an empty or stale slot).
 __device__ __forceinline__ uint64_t rhash_claim(const UniDev& d, uint64_t key) {
     const uint64_t ep = key >> 40, mask = d.rmask;
-    uint64_t h = mix64(key) & mask;
+    uint64_t h = rhash_home(d, key);
     for (uint64_t probe = 0; probe <= mask; probe++) {
         unsigned long long* kp = &d.rslot[h].x;
         uint64_t k = __ldcg(kp);
@@ -365,7 +368,7 @@ __device__ __forceinline__ uint64_t rhash_claim(const UniDev& d, uint64_t key) {
 // arrays: k_surv_hash 48 -> 33 ms and k_conflicts 104 -> 96 ms per job.
 __device__ __forceinline__ int32_t rhash_head(const UniDev& d, uint64_t key) {
     const uint64_t ep = key >> 40, mask = d.rmask;
-    uint64_t h = mix64(key) & mask;
+    uint64_t h = rhash_home(d, key);
     for (uint64_t probe = 0; probe <= mask; probe++) {
         const ulonglong2 s = __ldcg(d.rslot + h);
         if (s.x == key) return (s.y >> 32) == (ep & 0xFFFFFF) ? (int32_t)(uint32_t)s.y : -1;
@@ -904,19 +907,19 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
                         nbk[ax] = n;
                     }
                 }
-                const int n12 = nbk[1] * nbk[2], nall = nbk[0] * n12;
-                for (int m = 0; m < nall; m++) {
-                    const int i0 = m / n12, rem = m - i0 * n12;
-                    const int i1 = rem / nbk[2], i2 = rem - i1 * nbk[2];
-                    const int bc[3] = {(int)((bl[0] >> (10 * i0)) & 1023u), (int)((bl[1] >> (10 * i1)) & 1023u),
-                                       (int)((bl[2] >> (10 * i2)) & 1023u)};
-                    int32_t r2 = rhash_head(d, rkey_of(c.epoch, t, lin_cell(bc, d.dim, gwb)));
-                    while (r2 >= 0) {
-                        const Pt64* Q = d.spos + UG_IDX((int64_t)r2 * T + t, (int64_t)d.S_max * T);
-                        if (r2 < r && pair_hit64(d, P.c, Q->c)) add(r2);
-                        r2 = Q->next;
-                    }
-                }
+                for (int i0 = 0; i0 < nbk[0]; i0++)
+                    for (int i1 = 0; i1 < nbk[1]; i1++)
+                        for (int i2 = 0; i2 < nbk[2]; i2++) {
+                            const int bc[3] = {(int)((bl[0] >> (10 * i0)) & 1023u),
+                                               (int)((bl[1] >> (10 * i1)) & 1023u),
+                                               (int)((bl[2] >> (10 * i2)) & 1023u)};
+                            int32_t r2 = rhash_head(d, rkey_of(c.epoch, t, lin_cell(bc, d.dim, gwb)));
+                            while (r2 >= 0) {
+                                const Pt64* Q = d.spos + UG_IDX((int64_t)r2 * T + t, (int64_t)d.S_max * T);
+                                if (r2 < r && pair_hit64(d, P.c, Q->c)) add(r2);
+                                r2 = Q->next;
+                            }
+                        }
             }
         }
         __syncwarp();
