@@ -258,6 +258,25 @@ int ug_frame_bake(const ug_frames_cfg* cfg, int32_t n, int32_t nw, const double*
  * out->hits == NULL only hit counts and densities come back. */
 int ug_batch_frames(void* h, int32_t u, const ug_frames_cfg* cfg, ug_frames_out* out);
 
+/* Observer-view remap of one frame's hits, the viewer's draw-time transform
+ * (braidlab/frames.py:147-188, apparent_positions).  UG_VIEW_STATIC: the stored
+ * offsets and ln_dopp = 0.  UG_VIEW_MOVING: beta is capped at |beta| = 0.995 (and
+ * |beta| <= 1e-6 is static); each hit's unit direction n is boosted into the
+ * observer's rest frame, n' = [n + gamma beta + (gamma - 1)(u.n) u] / [gamma (1 +
+ * beta.n)] with u = beta / |beta|, ln_dopp = ln(gamma (1 + beta.n)), and the image is
+ * put back at its own chi on the Chebyshev shell (cheb != 0) or the Euclidean one;
+ * hits at the pulse centre keep their offsets.  Outputs are n doubles each.  Host
+ * buffers, computed on the GPU; UG_EINVAL for another mode. */
+#define UG_VIEW_STATIC 0
+#define UG_VIEW_MOVING 1
+int ug_apparent_positions(const ug_hit* hits, int64_t n, double beta_x, double beta_y, int32_t mode,
+                          int32_t cheb, double* ax, double* ay, double* ln_dopp);
+/* The same on device buffers (hits as from a frame bake left on the GPU), enqueued
+ * on `stream` (a cudaStream_t; NULL: the legacy default stream). */
+int ug_apparent_positions_async(const ug_hit* d_hits, int64_t n, double beta_x, double beta_y,
+                                int32_t mode, int32_t cheb, double* d_ax, double* d_ay,
+                                double* d_ln_dopp, void* stream);
+
 /* ---- single-universe convenience: a batch of one (the ug_pack_* surface) */
 int ug_pack_create(const ug_universe_cfg* cfg, const ug_run_opts* opts, void** out);
 int ug_pack_run(void* h);

@@ -226,3 +226,48 @@ def parse_knot_dump(text: str, dim: int, nw: int):
                 k += 3
         rows.append({"species": species, "idx": attempt - 1, "b": b, "a": a, "f": f, "a2": a2})
     return rows
+
+
+# ---------------------------------------------------------------------------
+# Observer-view remap of a frame's hits (numpy restatement of the reference's
+# braidlab/frames.py:147-188, apparent_positions).  FP64 throughout, the
+# reference's operations in its order.
+# ---------------------------------------------------------------------------
+
+BETA_CAP = 0.995  # braidlab/frames.py:37
+
+
+def apparent_positions(dx, dy, chi, beta, mode: str = "static", cheb: bool = True):
+    """(ax, ay, ln_dopp) for float32 hit offsets dx, dy and front radii chi seen by
+    an observer of boost beta: frames.py:159-162 (static), 163-174 (boost set-up:
+    cap, static below 1e-6, gamma, unit vector), 175-188 (per-hit aberration,
+    Doppler factor, Chebyshev or Euclidean shell)."""
+    dx = np.asarray(dx, np.float32).astype(np.float64)
+    dy = np.asarray(dy, np.float32).astype(np.float64)
+    if mode == "static":
+        return dx, dy, np.zeros(len(dx))
+    if mode != "moving":
+        raise ValueError(f"mode must be static|moving, got {mode!r}")
+    b = np.array(beta, np.float64).reshape(2)
+    bm = float(np.hypot(b[0], b[1]))
+    if bm > BETA_CAP:
+        b = b * (BETA_CAP / bm)
+        bm = BETA_CAP
+    if bm <= 1e-6:
+        return dx, dy, np.zeros(len(dx))
+    g = 1.0 / np.sqrt(1.0 - bm ** 2)
+    ux, uy = b[0] / bm, b[1] / bm
+    r = np.hypot(dx, dy)
+    ok = r > 0
+    nx = np.where(ok, dx / np.where(ok, r, 1.0), 0.0)
+    ny = np.where(ok, dy / np.where(ok, r, 1.0), 0.0)
+    bn = b[0] * nx + b[1] * ny
+    un = ux * nx + uy * ny
+    dfac = g * (1.0 + bn)
+    px = (nx + g * b[0] + (g - 1.0) * un * ux) / dfac
+    py = (ny + g * b[1] + (g - 1.0) * un * uy) / dfac
+    c = np.asarray(chi, np.float32).astype(np.float64)
+    norm = np.maximum(np.abs(px), np.abs(py)) if cheb else 1.0
+    ax = np.where(ok, px * c / norm, dx)
+    ay = np.where(ok, py * c / norm, dy)
+    return ax, ay, np.where(ok, np.log(dfac), 0.0)

@@ -1,4 +1,6 @@
-"""Reader of baked .frames files (reference braidlab/frames.py:88-144).
+"""Reader of baked .frames files (reference braidlab/frames.py:88-144), the
+observer-view remap of a frame's hits on the GPU (frames.py:147-188) and the per-frame
+measurements beside it (frames.py:191-223).
 
 The BRF1 layout (cuda/frame_bake.cu:29-38):
   header : b"BRF1", u32 n_paths, u32 n_observers, u32 n_instants, u32 front,
@@ -83,3 +85,41 @@ def load_frames(path: str | Path) -> FrameSet:
                                      np.sort(hits, order=["chi", "src"])))
         frames.append(row)
     return FrameSet(n_paths, _FRONTS[front], bool(cheb), speed, z_min, observers, frames)
+
+
+def apparent_positions(frame: ObserverFrame, mode: str = "static", cheb: bool = True):
+    """Apparent sky offsets and Doppler log-factor per hit (reference
+    braidlab/frames.py:147-188): ``static`` returns the stored offsets (ln_dopp 0);
+    ``moving`` boosts each hit's direction into the observer's rest frame by
+    ``frame.beta`` (capped at |beta| = 0.995) and puts it back on its own Chebyshev
+    shell (``cheb``) or Euclidean one.  Runs on the GPU through libug
+    (ug_apparent_positions)."""
+    from ugb200.frames import apparent_positions as _apparent
+
+    if mode not in ("static", "moving"):
+        raise ValueError(f"mode must be static|moving, got {mode!r}")
+    return _apparent(frame.hits, frame.beta, mode, cheb)
+
+
+def counts_vs_redshift(frame: ObserverFrame, edges: np.ndarray):
+    """(histogram, cumulative N(<Z)) of the images binned by cosmological 1+Z
+    (frames.py:191-197)."""
+    hist, _ = np.histogram(frame.redshift, bins=edges)
+    return hist, np.cumsum(hist)
+
+
+def ghost_multiplicity(frame: ObserverFrame) -> np.ndarray:
+    """Images per source worldline: torus wraps and earlier epochs (frames.py:200-202)."""
+    return np.bincount(frame.hits["src"])
+
+
+def load_gids(dump_path: str | Path) -> np.ndarray:
+    """Group id per dump row from a subpath dump's trailing gid column
+    (frames.py:205-223); a dump without one is an error."""
+    import csv
+
+    with open(dump_path) as fh:
+        rd = csv.DictReader(fh)
+        if rd.fieldnames is None or "gid" not in rd.fieldnames:
+            raise ValueError(f"{dump_path}: no gid column (not a subpath dump)")
+        return np.array([int(row["gid"]) for row in rd], dtype=np.int64)

@@ -618,3 +618,121 @@ extern "C" int ug_frame_bake(const ug_frames_cfg* cfg, int32_t n, int32_t nw, co
     }
     return bake_device(cfg, n, nw, bMax, dA2, dA, dB, dF, obs, out);
 }
+
+// ------------------------------------------------------- observer view remap
+
+namespace ug {
+namespace {
+
+// The boost of one observer frame, set up on the host with the reference's
+// operations in its order (braidlab/frames.py:164-174): cap, static threshold,
+// gamma, unit vector, and the two scalar products it forms once.
+struct ViewBoost {
+    int moving, cheb;
+    double bx, by, ux, uy, gamma, gm1, gbx, gby;
+};
+
+constexpr double kBetaCap = 0.995;  // FRAME_BETA_CAP (braidlab/frames.py:37)
+
+ViewBoost view_boost(double beta_x, double beta_y, int mode, int cheb) {
+    ViewBoost v{};
+    v.cheb = cheb != 0;
+    if (mode != UG_VIEW_MOVING) return v;
+    double bx = beta_x, by = beta_y;
+    double bm = std::hypot(bx, by);
+    if (bm > kBetaCap) {
+        const double s = kBetaCap / bm;
+        bx *= s;
+        by *= s;
+        bm = kBetaCap;
+    }
+    if (bm <= 1e-6) return v;
+    v.moving = 1;
+    v.gamma = 1.0 / std::sqrt(1.0 - std::pow(bm, 2.0));
+    v.ux = bx / bm;
+    v.uy = by / bm;
+    v.bx = bx;
+    v.by = by;
+    v.gbx = v.gamma * bx;
+    v.gby = v.gamma * by;
+    v.gm1 = v.gamma - 1.0;
+    return v;
+}
+
+// One thread per hit, FP64, every product and sum rounded on its own (no
+// contraction) in the order of braidlab/frames.py:175-188.
+__global__ void k_apparent(const ug_hit* __restrict__ hits, int64_t n, ViewBoost v, double* __restrict__ ax,
+                           double* __restrict__ ay, double* __restrict__ ld) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const ug_hit h = hits[i];
+        const double dx = h.dx, dy = h.dy;
+        if (!v.moving) {
+            ax[i] = dx;
+            ay[i] = dy;
+            ld[i] = 0.0;
+            continue;
+        }
+        const double eucl = hypot(dx, dy);
+        const bool ok = eucl > 0.0;
+        const double nx = ok ? dx / eucl : 0.0, ny = ok ? dy / eucl : 0.0;
+        const double bdotn = __dadd_rn(__dmul_rn(v.bx, nx), __dmul_rn(v.by, ny));
+        const double udotn = __dadd_rn(__dmul_rn(v.ux, nx), __dmul_rn(v.uy, ny));
+        const double dfac = __dmul_rn(v.gamma, __dadd_rn(1.0, bdotn));
+        const double gu = __dmul_rn(v.gm1, udotn);
+        const double apx = __dadd_rn(__dadd_rn(nx, v.gbx), __dmul_rn(gu, v.ux)) / dfac;
+        const double apy = __dadd_rn(__dadd_rn(ny, v.gby), __dmul_rn(gu, v.uy)) / dfac;
+        const double chi = h.chi;
+        const double norm = v.cheb ? fmax(fabs(apx), fabs(apy)) : 1.0;
+        ax[i] = ok ? __dmul_rn(apx, chi) / norm : dx;
+        ay[i] = ok ? __dmul_rn(apy, chi) / norm : dy;
+        ld[i] = ok ? log(dfac) : 0.0;
+    }
+}
+
+int check_view(int64_t n, int32_t mode) {
+    if (n < 0) return set_error(UG_EINVAL, "apparent_positions: negative hit count");
+    if (mode != UG_VIEW_STATIC && mode != UG_VIEW_MOVING)
+        return set_error(UG_EINVAL, "apparent_positions: mode must be static|moving");
+    return UG_OK;
+}
+
+}  // namespace
+}  // namespace ug
+
+extern "C" int ug_apparent_positions_async(const ug_hit* d_hits, int64_t n, double beta_x, double beta_y,
+                                           int32_t mode, int32_t cheb, double* d_ax, double* d_ay,
+                                           double* d_ln_dopp, void* stream) {
+    int rc = check_view(n, mode);
+    if (rc || n == 0) return rc;
+    if (!d_hits || !d_ax || !d_ay || !d_ln_dopp) return set_error(UG_EINVAL, "apparent_positions: null buffer");
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return set_error(UG_ECUDA, "apparent_positions: no CUDA device");
+    const int64_t blocks = std::min<int64_t>((n + 255) / 256, (int64_t)nsm * 8);
+    k_apparent<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(d_hits, n, view_boost(beta_x, beta_y, mode, cheb),
+                                                                   d_ax, d_ay, d_ln_dopp);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(UG_ECUDA, cudaGetErrorString(e));
+    return UG_OK;
+}
+
+extern "C" int ug_apparent_positions(const ug_hit* hits, int64_t n, double beta_x, double beta_y, int32_t mode,
+                                     int32_t cheb, double* ax, double* ay, double* ln_dopp) {
+    int rc = check_view(n, mode);
+    if (rc || n == 0) return rc;
+    if (!hits || !ax || !ay || !ln_dopp) return set_error(UG_EINVAL, "apparent_positions: null buffer");
+    DevBuf buf;
+    ug_hit* dH = buf.get<ug_hit>((size_t)n);
+    double* dO = buf.get<double>((size_t)n * 3);
+    if (!dH || !dO) return set_error(UG_ENOMEM, "apparent_positions: device allocation failed");
+    if (cudaMemcpy(dH, hits, (size_t)n * sizeof(ug_hit), cudaMemcpyHostToDevice) != cudaSuccess)
+        return set_error(UG_ECUDA, "apparent_positions: hit copy failed");
+    rc = ug_apparent_positions_async(dH, n, beta_x, beta_y, mode, cheb, dO, dO + n, dO + 2 * n, nullptr);
+    if (rc) return rc;
+    if (cudaMemcpy(ax, dO, (size_t)n * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(ay, dO + n, (size_t)n * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(ln_dopp, dO + 2 * n, (size_t)n * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return set_error(UG_ECUDA, "apparent_positions: result copy failed");
+    return UG_OK;
+}

@@ -27,7 +27,7 @@ EXPORTS = (
     "ug_batch_kernel_times", "ug_batch_reset_times", "ug_batch_counters", "ug_batch_mixed_error",
     "ug_batch_destroy", "ug_pack_create", "ug_pack_run", "ug_pack_stats", "ug_pack_destroy",
     "ug_frame_bake", "ug_batch_frames", "ug_state_bytes", "ug_batch_save_state", "ug_batch_restore",
-    "ug_batch_probe",
+    "ug_batch_probe", "ug_apparent_positions", "ug_apparent_positions_async",
 )
 
 
@@ -107,6 +107,8 @@ def load():
     L.ug_batch_save_state.argtypes = [vp, i32, vp]
     L.ug_batch_restore.argtypes = [vp, i32, i64, vp, vp, vp]
     L.ug_batch_probe.argtypes = [vp, i32, C.c_uint64, i64, i32, vp, vp]
+    L.ug_apparent_positions.argtypes = [vp, i64, C.c_double, C.c_double, i32, i32, vp, vp, vp]
+    L.ug_apparent_positions_async.argtypes = [vp, i64, C.c_double, C.c_double, i32, i32, vp, vp, vp, vp]
     for name in EXPORTS:
         f = getattr(L, name)
         if f.restype is None or name != "ug_last_error":

@@ -4,7 +4,8 @@
 on dump arrays and returns per-(instant, observer) hit tables and, optionally,
 bins x bins uint32 density grids of the hit offsets over [-chi_max, chi_max]^2.
 ``write_brf1`` writes the reference's .frames layout (cuda/frame_bake.cu:29-38), which
-braidlab.frames.load_frames reads.
+braidlab.frames.load_frames reads.  ``apparent_positions`` is the observer-view remap of a
+frame's hits (braidlab/frames.py:147-188) on the GPU.
 """
 
 from __future__ import annotations
@@ -137,3 +138,25 @@ def write_brf1(path, bk: Baked) -> None:
                 fh.write(struct.pack("<4d", *bk.obs_meta[fi, o]))
                 fh.write(struct.pack("<Q", len(h)))
                 fh.write(h.astype(HIT_DTYPE).tobytes())
+
+
+VIEW_MODES = {"static": 0, "moving": 1}
+
+
+def apparent_positions(hits: np.ndarray, beta, mode: str = "static", cheb: bool = True):
+    """(ax, ay, ln_dopp) of HIT_DTYPE hits seen by an observer of boost ``beta``
+    (braidlab/frames.py:147-188) through ug_apparent_positions: ``static`` keeps the
+    stored offsets; ``moving`` aberrates each hit's direction into the observer's rest
+    frame (|beta| capped at 0.995) with the Doppler log-factor, on the Chebyshev shell
+    of its chi when ``cheb``."""
+    if mode not in VIEW_MODES:
+        raise ValueError(f"mode must be static|moving, got {mode!r}")
+    h = np.ascontiguousarray(hits, dtype=HIT_DTYPE)
+    n = len(h)
+    out = np.empty((3, n), np.float64)
+    bx, by = (float(v) for v in np.asarray(beta, np.float64).reshape(2))
+    lib = L.load()
+    L.check(lib.ug_apparent_positions(h.ctypes.data if n else None, n, bx, by, VIEW_MODES[mode],
+                                      int(bool(cheb)), out[0].ctypes.data, out[1].ctypes.data,
+                                      out[2].ctypes.data))
+    return out[0], out[1], out[2]
