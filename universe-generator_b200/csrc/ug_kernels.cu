@@ -1211,7 +1211,8 @@ __device__ __forceinline__ void grid_insert(const UniDev& d, UniCtl& c, int t, i
 }
 
 // Sets a bit of an occupancy bitmap; bits are only ever set during a run, so
-// a bit read as set needs no atomic.
+// a bit read as set needs no atomic (most are: an unconditional atomicOr took
+// k_commit from 56 to 63 ms per c3 job).
 __device__ __forceinline__ void occ_set(uint32_t* words, int64_t bit, int64_t nwords) {
     uint32_t* w = words + UG_IDX(bit >> 5, nwords);
     const uint32_t m = 1u << (bit & 31);
