@@ -18,6 +18,7 @@ import argparse
 import json
 import math
 import os
+import tempfile
 import subprocess
 import sys
 import time
@@ -236,6 +237,8 @@ def main() -> int:
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--clocks-dir", default="",
+                    help="where the nvidia-smi samples of the timed region go (default: the temp dir)")
     ap.add_argument("--profile-case", action="store_true",
                     help="run one untimed packing job of the workload and exit (for ncu captures)")
     ap.add_argument("--stride", type=int, default=1,
@@ -302,8 +305,7 @@ def main() -> int:
     torch.cuda.synchronize()
 
     # device-timed steps (inputs resident, L2 flushed between steps)
-    clk_path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "/tmp",
-                            f"clocks_rank{rank}.csv")
+    clk_path = os.path.join(args.clocks_dir or tempfile.gettempdir(), f"clocks_rank{rank}.csv")
     sampler = start_clock_sampler(clk_path)
     times = []
     cands = 0
