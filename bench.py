@@ -340,21 +340,34 @@ def main() -> int:
         t_ms, cands = combine_ranks(t_ms, cands, dist, "cuda")
     value = cands / (t_ms / 1000.0)
 
-    # end to end through the public API with host buffers
-    e2e_t = 0.0
+    # end to end through the public API with host buffers: CUDA events on the packer's
+    # stream around each job (seed upload, rounds, host syncs, accepted lists read back),
+    # ranks started together and combined like `value` (max time, summed candidates)
+    e2e_ms = 0.0
     e2e_c = 0
+    nrep = max(1, args.steps // 2)
     _, h2d0, d2h0 = packer.counters()
-    for s in range(max(1, args.steps // 2)):
-        t0 = time.perf_counter()
+    if dist:
+        dist.barrier()
+    for s in range(nrep):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
         packer.reset(seeds(100 + s)).run()
         acc = [packer.accepted(k)[0] for k in range(len(us))]
-        e2e_t += time.perf_counter() - t0
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
         e2e_c += sum(packer.stats(k).attempts for k in range(len(us)))
         del acc
     _, h2d1, d2h1 = packer.counters()
-    nrep = max(1, args.steps // 2)
-    e2e = {"value": e2e_c / e2e_t, "unit": "candidates/s",
-           "h2d_bytes_per_step": (h2d1 - h2d0) // nrep, "d2h_bytes_per_step": (d2h1 - d2h0) // nrep}
+    h2d_b, d2h_b = (h2d1 - h2d0) // nrep, (d2h1 - d2h0) // nrep
+    if dist:
+        e2e_ms, e2e_c = combine_ranks(e2e_ms, e2e_c, dist, "cuda")
+        _, h2d_b = combine_ranks(0.0, h2d_b, dist, "cuda")
+        _, d2h_b = combine_ranks(0.0, d2h_b, dist, "cuda")
+    e2e = {"value": e2e_c / (e2e_ms / 1000.0), "unit": "candidates/s",
+           "h2d_bytes_per_step": h2d_b, "d2h_bytes_per_step": d2h_b}
 
     packer.close()
     # per-kernel timing pass (events around each launch on the packer's stream)
