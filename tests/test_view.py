@@ -102,3 +102,30 @@ def test_abi_rejects_a_bad_mode_before_device_work(ug):
         from ugb200.frames import apparent_positions
 
         apparent_positions(h, (0.1, 0.0), "sideways")
+
+
+@pytest.mark.parametrize("cheb", [True, False])
+def test_oracle_remap_properties(oracle, cheb):
+    """Images stay on their own shell, centre hits stay put, boosts above the cap act
+    as the cap, boosts under 1e-6 and the static mode return the stored offsets."""
+    rng = np.random.default_rng(7)
+    n = 1 << 14
+    chi = rng.uniform(1e-3, 4.0, n).astype(np.float32)
+    ang = rng.uniform(-np.pi, np.pi, n)
+    dx = (chi * np.cos(ang)).astype(np.float32)
+    dy = (chi * np.sin(ang)).astype(np.float32)
+    dx[::101] = 0.0
+    dy[::101] = 0.0
+    moved = (dx != 0) | (dy != 0)
+    ax, ay, ld = oracle.apparent_positions(dx, dy, chi, (0.5, -0.6), "moving", cheb)
+    r = np.maximum(np.abs(ax), np.abs(ay)) if cheb else np.hypot(ax, ay)
+    np.testing.assert_allclose(r[moved], chi[moved].astype(np.float64), rtol=1e-12)
+    assert np.all(ax[~moved] == 0) and np.all(ld[~moved] == 0)
+    cap = oracle.apparent_positions(dx, dy, chi, (0.995 * 0.6, 0.995 * 0.8), "moving", cheb)
+    over = oracle.apparent_positions(dx, dy, chi, (6.0, 8.0), "moving", cheb)
+    for a, b in zip(cap, over):
+        np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-12)
+    for beta, mode in (((3e-7, 4e-7), "moving"), ((0.5, 0.5), "static")):
+        sx, sy, sl = oracle.apparent_positions(dx, dy, chi, beta, mode, cheb)
+        assert np.array_equal(sx, dx.astype(np.float64)) and np.array_equal(sy, dy.astype(np.float64))
+        assert not sl.any()
