@@ -92,7 +92,22 @@ struct Batch {
     int64_t launches = 0;  // kernels issued (graph replays count every node)
     int64_t h2d = 0, d2h = 0;  // bytes copied between host and device
     int kernels_per_round = 9;
+    // CTAs per SM of grid-stride round kernels sized from the occupancy at creation
+    int res_sgen = 8, res_shash = 8, res_confl = 16;
 };
+
+// CTAs per SM a grid-stride kernel is launched with: at most as many as can be
+// resident, so that its static item striding runs in one wave (a CTA beyond that
+// starts only when a resident one has finished all of its items).
+template <class F>
+static int resident_ctas(F* fn, int threads, size_t smem, int cap) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, smem) != cudaSuccess || nb < 1) {
+        cudaGetLastError();
+        return 1;
+    }
+    return std::min(nb, cap);
+}
 
 static int64_t pow2_at_least(int64_t v) {
     int64_t p = 1;
@@ -402,19 +417,17 @@ static int launch_round(Batch& B, bool timed) {
     tb(K_SGEN);
     {
         const int wb = (int)(B.any_knot ? kSurvSmemPerWarp : kSurvSmemAxis);
-        k_surv_gen<<<B.nsm * 8, 32 * kSurvWarps, kSurvWarps * wb, B.st>>>(B.dU, B.dCtl, B.dInfo, wb);
+        k_surv_gen<<<B.nsm * B.res_sgen, 32 * kSurvWarps, kSurvWarps * wb, B.st>>>(B.dU, B.dCtl, B.dInfo, wb);
     }
     te(K_SGEN);
     tb(K_SGEMM);
     k_surv_gemm<<<B.nsm * 4, 128, kGemmSmem, B.st>>>(B.dU, B.dCtl, B.dInfo);
     te(K_SGEMM);
     tb(K_SHASH);
-    k_surv_hash<<<B.nsm * 8, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+    k_surv_hash<<<B.nsm * B.res_shash, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
     te(K_SHASH);
     tb(K_CONFL);
-    // 16 four-warp CTAs per SM: 48 registers allow 10 resident (40 warps); on c3
-    // 104 ms per job against 108 ms with 8 per SM
-    k_conflicts<<<B.nsm * 16, 128, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+    k_conflicts<<<B.nsm * B.res_confl, 128, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
     te(K_CONFL);
     tb(K_GREEDY);
     k_greedy<<<B.n, 32, 2 * kSmaxCap * sizeof(int32_t), B.st>>>(B.dU, B.dCtl, B.dInfo);
@@ -633,6 +646,14 @@ int ug_batch_create(const ug_universe_cfg* cfgs, int32_t n, const ug_run_opts* o
     if (B->any_mixed && cudaFuncSetAttribute(k_confirm64w, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)(kSurvWarps * kConfSmemPerWarp)) != cudaSuccess)
         return bail(fail(UG_ECUDA, "smem attribute failed"));
+    // one wave per SM, measured on c3 against 8 / 8 / 16 CTAs per SM: k_surv_gen 27.7 ->
+    // 24.5 ms, k_surv_hash 33.5 -> 32.0 ms, k_conflicts 85.5 -> 80.2 ms per job.  k_commit
+    // and k_confirm64w keep 8 and 4 per SM (more than resident): one wave measured slower
+    // for them (56.6 -> 60.0 and 38.2 -> 40.6 ms).
+    B->res_sgen = resident_ctas(k_surv_gen, 32 * kSurvWarps,
+                                kSurvWarps * (B->any_knot ? kSurvSmemPerWarp : kSurvSmemAxis), 8);
+    B->res_shash = resident_ctas(k_surv_hash, 256, 0, 8);
+    B->res_confl = resident_ctas(k_conflicts, 128, 0, 16);
     for (int k = 0; k < 2 * K_NK; k++) cudaEventCreate(&B->ev[k]);
     *out = B;
     return UG_OK;
