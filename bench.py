@@ -16,7 +16,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import tempfile
 import subprocess
@@ -39,38 +38,13 @@ FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1
 
 
 def workloads(name: str, ug, seed0: int):
-    """Universes of one job.  All inputs are generated from seeds."""
-    U = ug.Universe
-    if name == "c0":  # 1+1D, F=T=16, 20k candidates, seed 0
-        return [U(dim=1, T=16, zgrid=1, excl=1, cross1d=1, seed=seed0, attempts=20000,
-                  round_size=4096)], {"dim": 1, "F": 16, "T": 16, "candidates": 20000}
-    if name == "c1":  # 2+1D, F=T=64, 1M candidates, rounds of 16k
-        return [U(dim=2, T=64, zgrid=1, excl=1, seed=seed0, attempts=1_000_000,
-                  round_size=16384)], {"dim": 2, "F": 64, "T": 64, "candidates": 1_000_000,
-                                       "round": 16384}
-    if name == "c2":  # 3+1D, F=T=128, 5M candidates, rounds of 64k
-        return [U(dim=3, T=128, zgrid=1, excl=1, seed=seed0, attempts=5_000_000,
-                  round_size=65536)], {"dim": 3, "F": 128, "T": 128, "candidates": 5_000_000,
-                                       "round": 65536}
-    if name == "c3":  # 256 universes, d in {1,2,3}, F log-uniform [16,256], caps log-uniform [1e4,1e6]
-        rng = np.random.default_rng(12345)
-        us = []
-        for k in range(256):
-            dim = int(rng.integers(1, 4))
-            F = int(round(math.exp(rng.uniform(math.log(16), math.log(256)))))
-            F = max(16, min(256, F))
-            cap = int(round(math.exp(rng.uniform(math.log(1e4), math.log(1e6)))))
-            us.append(U(dim=dim, T=F, zgrid=1, excl=1, cross1d=int(dim == 1),
-                        seed=(seed0 * 1000003 + k) & (2**64 - 1), attempts=cap,
-                        round_size=16384))
-        tot = sum(u.attempts for u in us)
-        return us, {"universes": 256, "dims": [1, 2, 3], "F": "log-uniform[16,256]",
-                    "caps": "log-uniform[1e4,1e6]", "candidates": tot}
-    if name == "c4":  # 2+1D unique-group mode at F=256, 2M candidates
-        return [U(dim=2, T=256, zgrid=1, excl=1, group_mode=2, seed=seed0, attempts=2_000_000,
-                  round_size=16384)], {"dim": 2, "F": 256, "T": 256, "candidates": 2_000_000,
-                                       "mode": "unique-group"}
-    raise SystemExit(f"unknown workload {name}")
+    """Universes of one job (ugb200.workloads: all inputs generated from seeds)."""
+    from ugb200 import workloads as W
+
+    try:
+        return W.workload(name, seed0)
+    except ValueError as e:
+        raise SystemExit(str(e))
 
 
 def peaks():

@@ -116,6 +116,13 @@ int ug_version(void);
 /* Message of the last failure on this thread; returns its length. */
 int ug_last_error(char* buf, size_t len);
 
+/* sizeof of the structs a binding must lay out, in this order: ug_universe_cfg,
+ * ug_run_opts, ug_stats, ug_kernel_times, ug_hit, ug_frames_cfg, ug_frames_out.
+ * Writes min(n, 7) of them and returns 7.  Lets a binding (ctypes, cffi, cgo)
+ * check its struct definitions against the library it loaded; no device work.
+ * No reference counterpart (the engines' interface is argv and files). */
+int ug_struct_sizes(int64_t* sizes, int32_t n);
+
 /* Create a batch of independent universes on one GPU (replaces one engine
  * process per job, braidlab/orchestrator.py:85-147).  The library owns all
  * device memory inside the handle. */
@@ -157,10 +164,10 @@ int ug_batch_params(void* h, int32_t u, double* a2, double* a, int32_t* b, doubl
  * allocating any device memory: the regenerated parameters are staged in a
  * fixed 16 MiB buffer that the library image reserves on every GPU that
  * loads it, then copied to the caller's host buffers.  No counterpart in
- * the reference.  For callers that must not allocate device memory at the
- * time of the call -- code running while another thread captures a CUDA
- * graph in global mode, or a serving loop that reserved its device memory
- * at start-up.  Dumps needing more than 16 MiB (paths x dim x (8 + 20 nw)
+ * the reference.  For callers that cannot call cudaMalloc at the time of the
+ * call -- a serving process that reserved all of its device memory at
+ * start-up, or a host whose allocator policy forbids allocations after
+ * start-up.  Dumps needing more than 16 MiB (paths x dim x (8 + 20 nw)
  * bytes) fail with UG_ECAP.  The first call on a device looks up the
  * buffer's device address; make it before any stream capture.  All calls
  * share the buffer: calls whose work overlaps on the GPU race. */

@@ -49,6 +49,9 @@ class _Run(C.Structure):
         ("nthreads", C.c_int32),
         ("sub_attempts", C.c_int64),
         ("round", C.c_int64),
+        ("accept_rate", C.c_double),
+        ("sub_accept_rate", C.c_double),
+        ("sub_fill_rate", C.c_double),
     ]
 
 
@@ -182,13 +185,18 @@ class PackResult:
 
 def pack(m: Model, attempts: int, *, max_n: int = 0, group_mode: int = GROUP_NONE,
          sub_attempts: int = 0, nthreads: int = 1, round_size: int = 65536,
+         accept_rate: float = 0.0, sub_accept_rate: float = 0.0, sub_fill_rate: float = 0.0,
          cap: int | None = None) -> PackResult:
+    """Sequential RSA over the candidate stream (nthreads > 1: threaded batch
+    prefilter + in-order decisions, same result).  The windowed stops use
+    buckets of win_target / 32 candidates aligned at the phase start."""
     cap = cap or max(1024, attempts + (sub_attempts or (attempts if group_mode == GROUP_SUBPATH else 0)))
     acc = np.zeros(cap, np.int64)
     gid = np.zeros(cap, np.int32)
     res = _Result(cap, acc.ctypes.data_as(C.POINTER(C.c_int64)),
                   gid.ctypes.data_as(C.POINTER(C.c_int32)), 0, 0, 0, 0, 0)
-    run = _Run(attempts, max_n, group_mode, nthreads, sub_attempts, round_size)
+    run = _Run(attempts, max_n, group_mode, nthreads, sub_attempts, round_size,
+               accept_rate, sub_accept_rate, sub_fill_rate)
     mc = m._c()
     rc = lib().ora_pack(C.byref(mc), C.byref(run), C.byref(res))
     if rc:

@@ -485,7 +485,7 @@ static int64_t cell_key(int t, const int* c, int dim, int gw) {
     return ((int64_t)t << 40) | lin;
 }
 
-static int store_add(store_t* s, const double* P /* [dim][T] */, int32_t gid, double cell) {
+static int store_add(store_t* s, const double* P /* [dim][T] */, int32_t gid, double cell, int64_t* new_cells) {
     if (s->n == s->cap) {
         int64_t nc = s->cap * 2;
         double* np = realloc(s->pos, sizeof(double) * nc * s->dim * s->T);
@@ -511,6 +511,7 @@ static int store_add(store_t* s, const double* P /* [dim][T] */, int32_t gid, do
             *k = key;
             s->hval[k - s->hkey] = -1;
             s->hn++;
+            ++*new_cells;
         }
         s->next[p * s->T + t] = s->hval[k - s->hkey];
         s->hval[k - s->hkey] = (int32_t)p;
@@ -661,17 +662,93 @@ static int record(ora_result* res, int64_t idx, int32_t gid) {
     return 0;
 }
 
+/* ---- windowed stops (the --until-accept-rate window of braid_cuda.cu:585-590,
+ * 931-943 and the phase-2 new-volume window of braid_cuda.cu:953-1037).  The
+ * reference keeps a deque of its rounds' (batch, admitted) pairs covering at
+ * least win_target = clamp(30 / threshold, 2e7, 5e9) attempts and stops when
+ * the window's rate falls below the threshold after 1e6 attempts.  Its rounds
+ * are its own adaptive batches; here the window is made of 32 buckets of
+ * q = win_target / 32 candidates aligned at the phase start, so the stop point
+ * is a function of the candidate stream alone: at every bucket boundary (in
+ * phase-relative candidates) the last 32 buckets are summed, and the phase
+ * ends there when 32 buckets exist, more than 1e6 candidates are decided and
+ * sum / (32 q) < threshold.  The packer evaluates the same rule at the same
+ * boundaries (its rounds never straddle one). */
+typedef struct {
+    double thr;
+    int64_t q;
+    int64_t ring[32];
+    int64_t nb, sum, cur;
+} win_t;
+
+static void win_init(win_t* w, double thr) {
+    memset(w, 0, sizeof(*w));
+    w->thr = thr;
+    if (thr > 0) {
+        double t = 30.0 / thr;
+        if (t < 2e7) t = 2e7;
+        if (t > 5e9) t = 5e9;
+        const int64_t W = (int64_t)t;
+        w->q = W / 32 > 0 ? W / 32 : 1;
+    }
+}
+
+/* candidates from phase position in_phase to the next bucket boundary */
+static int64_t win_room(const win_t* w, int64_t in_phase) {
+    return w->q ? w->q - in_phase % w->q : INT64_MAX;
+}
+
+/* Called once candidates [0, in_phase) of the phase are decided; returns 1
+ * when the phase stops at in_phase. */
+static int win_close(win_t* w, int64_t in_phase) {
+    if (!w->q || in_phase <= 0 || in_phase % w->q) return 0;
+    const int slot = (int)(w->nb & 31);
+    if (w->nb >= 32) w->sum -= w->ring[slot];
+    w->ring[slot] = w->cur;
+    w->sum += w->cur;
+    w->cur = 0;
+    w->nb++;
+    return w->nb >= 32 && in_phase > 1000000 && (double)w->sum / (double)(32 * w->q) < w->thr;
+}
+
+/* ---- admission rules.  mode 0: unique packing (any contact rejects);
+ * mode 1: unique-group (no contact founds a group labelled by its slot, one
+ * group joins it, two or more reject); mode 2: subpath phase (exactly one group
+ * joins, braid_cuda.cu:726-750).  The first test against the committed packing
+ * is also the threaded prefilter: a rejection there is final because the
+ * packing only grows and group labels never change. */
+static int decide(cand_eval_t* ce, const store_t* s, int mode, int32_t* gid, int* founded) {
+    int32_t g;
+    if (mode == 0) {
+        if (ce_test(ce, s, 0, &g)) return 0;
+        *gid = (int32_t)s->n;
+        *founded = 1;
+        return 1;
+    }
+    if (ce_test(ce, s, 1, &g)) return 0;
+    if (g < 0) {
+        if (mode == 2) return 0;
+        *gid = (int32_t)s->n;
+        *founded = 1;
+        return 1;
+    }
+    *gid = g;
+    *founded = 0;
+    return 1;
+}
+
 /* ---- threaded form: parallel prefilter of a batch against the committed
- * packing, then serial in-order recheck of the survivors against the
- * round's earlier admissions (the scheme of braid_knot.cu:401-469 with CPU
- * threads in place of the kernel). */
+ * packing, then the serial in-order decision of the survivors against the
+ * packing including the batch's earlier admissions (the scheme of
+ * braid_knot.cu:401-469 with CPU threads in place of the kernel; the decisions
+ * are those of the sequential loop). */
 typedef struct {
     const ora_model* m;
     const tabs_t* tb;
     const store_t* s;
     int64_t base, count;
     uint8_t* surv;
-    int tid, nth;
+    int tid, nth, mode;
 } mt_job_t;
 
 static void* mt_worker(void* arg) {
@@ -686,69 +763,82 @@ static void* mt_worker(void* arg) {
     for (int64_t i = lo; i < hi; i++) {
         int32_t g;
         ce_start(ce, (uint64_t)(j->base + i));
-        j->surv[i] = (uint8_t)!ce_test(ce, j->s, 0, &g);
+        j->surv[i] = (uint8_t)!ce_test(ce, j->s, j->mode != 0, &g);
     }
     free(ce);
     return NULL;
 }
 
-static int pack_threaded(const ora_model* m, const ora_run* run, const tabs_t* tb, store_t* s,
-                         ora_result* res) {
-    const int nth = run->nthreads;
-    const int64_t B = run->round > 0 ? run->round : 65536;
-    uint8_t* surv = malloc((size_t)B);
+/* One phase over candidates [start, start + budget): admissions in index order
+ * under rule `mode`, stopped early by max_n (phase-1 uniques) or a window. */
+static int run_phase(const ora_model* m, const ora_run* run, const tabs_t* tb, store_t* s, ora_result* res,
+                     int mode, int64_t start, int64_t budget, int64_t max_n, double acc_thr, double fill_thr,
+                     int64_t* end_out) {
+    const int nth = run->nthreads > 1 ? run->nthreads : 1;
+    const int64_t B = nth > 1 ? (run->round > 0 ? run->round : 65536) : 1;
+    uint8_t* surv = nth > 1 ? malloc((size_t)B) : NULL;
     pthread_t* th = malloc(sizeof(pthread_t) * nth);
     mt_job_t* jobs = malloc(sizeof(mt_job_t) * nth);
     cand_eval_t* ce = malloc(sizeof(cand_eval_t));
-    double* Pin = NULL; /* positions of this round's admissions */
-    int64_t pin_cap = 0;
     int rc = 0;
-    if (!surv || !th || !jobs || !ce) return -1;
+    if ((nth > 1 && !surv) || !th || !jobs || !ce) {
+        rc = -1;
+        goto done;
+    }
     ce->m = m;
     ce->tb = tb;
-    const int T = m->T, D = m->dim;
-    int64_t idx = 0;
-    while (idx < run->attempts && !(run->max_n && s->n >= run->max_n)) {
-        const int64_t cnt = run->attempts - idx < B ? run->attempts - idx : B;
-        for (int k = 0; k < nth; k++) {
-            jobs[k] = (mt_job_t){m, tb, s, idx, cnt, surv, k, nth};
-            pthread_create(&th[k], NULL, mt_worker, &jobs[k]);
-        }
-        for (int k = 0; k < nth; k++) pthread_join(th[k], NULL);
-        const int64_t n0 = s->n;
-        int64_t consumed = cnt;
-        for (int64_t i = 0; i < cnt; i++) {
-            if (!surv[i]) continue;
-            ce_start(ce, (uint64_t)(idx + i));
-            ce_all(ce);
-            int clash = 0;
-            for (int64_t p = n0; p < s->n && !clash; p++) {
-                const double* Q = &s->pos[p * D * T];
-                if (D == 1 && m->cross1d && crosses(ce->P, Q, T)) clash = 1;
-                for (int t = 0; t < T && !clash; t++) clash = pair_hit(tb, D, ce->P + t, T, Q + t, T);
+    win_t wa, wf;
+    win_init(&wa, acc_thr);
+    win_init(&wf, fill_thr);
+    const int64_t end = start + budget;
+    int64_t idx = start;
+    while (idx < end && !(max_n && res->n_unique >= max_n)) {
+        const int64_t in0 = idx - start;
+        int64_t cnt = end - idx < B ? end - idx : B;
+        if (win_room(&wa, in0) < cnt) cnt = win_room(&wa, in0);
+        if (win_room(&wf, in0) < cnt) cnt = win_room(&wf, in0);
+        if (nth > 1) {
+            for (int k = 0; k < nth; k++) {
+                jobs[k] = (mt_job_t){m, tb, s, idx, cnt, surv, k, nth, mode};
+                pthread_create(&th[k], NULL, mt_worker, &jobs[k]);
             }
-            if (clash) continue;
-            if (store_add(s, ce->P, (int32_t)s->n, tb->cell) || record(res, idx + i, (int32_t)s->n - 1)) {
+            for (int k = 0; k < nth; k++) pthread_join(th[k], NULL);
+        }
+        int64_t consumed = cnt, adm = 0, newc = 0;
+        for (int64_t i = 0; i < cnt; i++) {
+            if (surv && !surv[i]) continue;
+            int32_t gid;
+            int founded;
+            ce_start(ce, (uint64_t)(idx + i));
+            if (!decide(ce, s, mode, &gid, &founded)) continue;
+            ce_all(ce);
+            if (store_add(s, ce->P, gid, tb->cell, &newc) || record(res, idx + i, gid)) {
                 rc = -2;
                 goto done;
             }
-            res->n_unique++;
-            if (run->max_n && s->n >= run->max_n) {
+            adm++;
+            if (founded)
+                res->n_unique++;
+            else
+                res->n_sub++;
+            if (max_n && res->n_unique >= max_n) {
                 consumed = i + 1;
                 break;
             }
         }
         idx += consumed;
+        wa.cur += adm;
+        wf.cur += newc;
+        const int sa = win_close(&wa, idx - start);
+        const int sf = win_close(&wf, idx - start);
+        if (sa || sf) break;
     }
-    res->attempts = idx;
-    res->phase1_end = idx;
+    *end_out = idx;
 done:
     free(surv);
     free(th);
     free(jobs);
     free(ce);
-    free(Pin);
-    (void)pin_cap;
     return rc;
 }
 
@@ -761,63 +851,16 @@ int ora_pack(const ora_model* m, const ora_run* run, ora_result* res) {
     store_t s;
     if (store_init(&s, m->dim, m->T, tb.gw)) return -1;
     res->n_acc = res->n_unique = res->n_sub = res->attempts = res->phase1_end = 0;
-    int rc = 0;
-    if (run->nthreads > 1 && run->group_mode == ORA_GROUP_NONE) {
-        rc = pack_threaded(m, run, &tb, &s, res);
-        store_free(&s);
-        tabs_free(&tb);
-        return rc;
-    }
-    cand_eval_t* ce = malloc(sizeof(cand_eval_t));
-    if (!ce) return -1;
-    ce->m = m;
-    ce->tb = &tb;
     int64_t idx = 0;
-    const int single_phase_groups = run->group_mode == ORA_GROUP_UNIQUE;
     /* phase 1 (or the single unique-group phase) */
-    while (idx < run->attempts && !(run->max_n && res->n_unique >= run->max_n)) {
-        int32_t g;
-        ce_start(ce, (uint64_t)idx);
-        if (!single_phase_groups) {
-            if (!ce_test(ce, &s, 0, &g)) {
-                ce_all(ce);
-                const int32_t gid = (int32_t)s.n;
-                if ((rc = store_add(&s, ce->P, gid, tb.cell)) || (rc = record(res, idx, gid))) goto out;
-                res->n_unique++;
-            }
-        } else {
-            if (!ce_test(ce, &s, 1, &g)) {
-                ce_all(ce);
-                int32_t gid = g;
-                if (g < 0) {
-                    gid = (int32_t)s.n; /* founds a group labelled by its own slot */
-                    res->n_unique++;
-                } else {
-                    res->n_sub++;
-                }
-                if ((rc = store_add(&s, ce->P, gid, tb.cell)) || (rc = record(res, idx, gid))) goto out;
-            }
-        }
-        idx++;
-    }
+    int rc = run_phase(m, run, &tb, &s, res, run->group_mode == ORA_GROUP_UNIQUE ? 1 : 0, 0, run->attempts,
+                       run->max_n, run->accept_rate, 0.0, &idx);
     res->phase1_end = idx;
-    /* phase 2: subpaths (candidate stream continues after phase 1) */
-    if (run->group_mode == ORA_GROUP_SUBPATH) {
-        const int64_t end = idx + (run->sub_attempts > 0 ? run->sub_attempts : run->attempts);
-        while (idx < end) {
-            int32_t g;
-            ce_start(ce, (uint64_t)idx);
-            if (!ce_test(ce, &s, 1, &g) && g >= 0) {
-                ce_all(ce);
-                if ((rc = store_add(&s, ce->P, g, tb.cell)) || (rc = record(res, idx, g))) goto out;
-                res->n_sub++;
-            }
-            idx++;
-        }
-    }
+    /* phase 2: subpaths (the candidate stream continues after phase 1) */
+    if (!rc && run->group_mode == ORA_GROUP_SUBPATH)
+        rc = run_phase(m, run, &tb, &s, res, 2, idx, run->sub_attempts > 0 ? run->sub_attempts : run->attempts, 0,
+                       run->sub_accept_rate, run->sub_fill_rate, &idx);
     res->attempts = idx;
-out:
-    free(ce);
     store_free(&s);
     tabs_free(&tb);
     return rc;

@@ -51,9 +51,12 @@ typedef struct ora_run {
     int64_t attempts;     /* candidate budget of the (first) phase */
     int64_t max_n;        /* stop phase 1 at this many paths (0 = off) */
     int32_t group_mode;   /* ORA_GROUP_* */
-    int32_t nthreads;     /* 0/1 = sequential RSA; >1 = threaded batch + in-order recheck */
+    int32_t nthreads;     /* 0/1 = sequential RSA; >1 = threaded batch prefilter + in-order decisions */
     int64_t sub_attempts; /* subpath-phase budget (ORA_GROUP_SUBPATH) */
     int64_t round;        /* batch size of the threaded form */
+    double accept_rate;     /* phase-1 windowed accept-rate stop (0 = off) */
+    double sub_accept_rate; /* phase-2 windowed accept-rate stop (0 = off) */
+    double sub_fill_rate;   /* phase-2 windowed new-volume stop (0 = off) */
 } ora_run;
 
 typedef struct ora_result {

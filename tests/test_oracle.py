@@ -197,3 +197,30 @@ def test_euclid_exclusion_against_brute_force(oracle, dim, excl):
         assert res.acc_idx.tolist() == acc
     cheb = oracle.pack(oracle.Model(dim=dim, T=10, zgrid=1, excl=excl, seed=17 + dim), n)
     assert len(acc) > len(cheb.acc_idx)  # the ball excludes less than the cube
+
+
+def _win_stop(idx, start, budget, thr):
+    """The windowed stop restated in numpy: buckets of q = clamp(30/thr, 2e7, 5e9) // 32
+    candidates from the phase start; at each boundary b (phase-relative) with 32
+    buckets behind it and b > 1e6, stop when admissions in the last 32 q / (32 q) < thr."""
+    W = int(min(5e9, max(2e7, 30.0 / thr)))
+    q = max(1, W // 32)
+    rel = np.sort(np.asarray(idx, np.int64) - start)
+    for j in range(32, budget // q + 1):
+        b = j * q
+        cnt = np.searchsorted(rel, b) - np.searchsorted(rel, b - 32 * q)
+        if b > 1_000_000 and cnt / (32 * q) < thr:
+            return start + b
+    return start + budget
+
+
+def test_accept_rate_window_stop(oracle):
+    """--until-accept-rate (braid_cuda.cu:931-943) with candidate-aligned buckets: the
+    stop lands on the first bucket boundary where the rule holds, and the run equals a
+    budget-limited run to the same attempt count."""
+    m = oracle.Model(dim=2, T=8, zgrid=1, excl=1, seed=21)
+    full = oracle.pack(m, 40_000_000, nthreads=8, round_size=65536, accept_rate=1e-6)
+    assert 20_000_000 < full.attempts < 40_000_000  # not at the first full window
+    assert full.attempts == _win_stop(full.acc_idx, 0, 40_000_000, 1e-6)
+    cut = oracle.pack(m, full.attempts, nthreads=8, round_size=65536)
+    assert np.array_equal(cut.acc_idx, full.acc_idx)

@@ -175,25 +175,37 @@ struct UniCtl {
     int32_t B_min, B_cap;  // round-size adaptation bounds
     int32_t err_code;
     int32_t pad;
-    // windowed accept-rate stop (braid_cuda.cu:931-943): a ring of buckets of
-    // (attempts, admitted); a bucket closes once it holds win_target/32 attempts
+    // windowed stops (braid_cuda.cu:585-590, 931-943 and the phase-2 new-volume
+    // window of :953-1037).  Each window is 32 buckets of q = win_target / 32
+    // candidates aligned at the phase start (phase_start); rounds never straddle a
+    // bucket boundary, and at each boundary the phase ends when 32 buckets exist,
+    // more than 1e6 candidates are decided and the last 32 buckets' count over
+    // 32 q is below the threshold.  win_*: admissions (accept rate, phase 1 or 2),
+    // fwin_*: newly occupied grid cells (phase 2).
     double accept_rate;     // phase 1 threshold (0 = off)
     double sub_accept_rate; // phase 2 threshold (0 = off)
-    int64_t win_target, win_att, win_adm;
-    int32_t win_head, win_len;
-    int64_t win_b[64];
-    int64_t win_a[64];
-    // occupied (timestep, cell) buckets and the windowed new-volume stop of
-    // phase 2 (braid_cuda.cu:960-1035): newly occupied cells per attempt
+    double win_thr;         // threshold of the running phase
+    int64_t phase_start;    // first candidate of the running phase
+    int64_t win_q, win_nb, win_sum, win_cur;
+    int64_t win_ring[32];
+    // occupied (timestep, cell) buckets of the collision grid
     int64_t filled;         // occupied cells so far
     int64_t round_new;      // cells first occupied by this round's commit
     int64_t last_used;      // candidates decided by the last round
     double sub_fill_rate;   // threshold (0 = off)
-    int64_t fwin_target, fwin_att, fwin_new;
-    int32_t fwin_head, fwin_len;
-    int64_t fwin_b[64];
-    int64_t fwin_n[64];
+    int64_t fwin_q, fwin_nb, fwin_sum, fwin_cur;
+    int64_t fwin_ring[32];
 };
+
+// Bucket size of a window for threshold thr: win_target = clamp(30 / thr, 2e7, 5e9)
+// candidates (braid_cuda.cu:589-590) in 32 buckets; 0 = off.
+__host__ __device__ __forceinline__ int64_t win_bucket(double thr) {
+    if (!(thr > 0)) return 0;
+    double t = 30.0 / thr;
+    t = t < 2e7 ? 2e7 : (t > 5e9 ? 5e9 : t);
+    const int64_t W = (int64_t)t;
+    return W / 32 > 0 ? W / 32 : 1;
+}
 
 // ------------------------------------------------------------------ helpers
 

@@ -363,9 +363,10 @@ static void init_ctl(const ug_universe_cfg& c, const UniDev& d, UniCtl& k) {
     k.round_B = (int)std::min<int64_t>(b0, d.B_max) / kTile * kTile;
     k.accept_rate = c.accept_rate;
     k.sub_accept_rate = c.sub_accept_rate;
-    k.win_target = c.accept_rate > 0 ? (int64_t)std::min(5e9, std::max(2e7, 30.0 / c.accept_rate)) : 0;
+    k.win_thr = c.accept_rate;
+    k.win_q = win_bucket(c.accept_rate);
     k.sub_fill_rate = c.sub_fill_rate;
-    k.fwin_target = 0;  // armed when phase 2 starts
+    k.fwin_q = 0;  // armed when phase 2 starts
 }
 
 static int push_unidev(Batch& B) {
@@ -563,6 +564,14 @@ using namespace ug;
 extern "C" {
 
 int ug_version(void) { return 1; }
+
+int ug_struct_sizes(int64_t* sizes, int32_t n) {
+    const int64_t v[7] = {(int64_t)sizeof(ug_universe_cfg), (int64_t)sizeof(ug_run_opts), (int64_t)sizeof(ug_stats),
+                          (int64_t)sizeof(ug_kernel_times), (int64_t)sizeof(ug_hit), (int64_t)sizeof(ug_frames_cfg),
+                          (int64_t)sizeof(ug_frames_out)};
+    for (int i = 0; sizes && i < n && i < 7; i++) sizes[i] = v[i];
+    return 7;
+}
 
 int ug_last_error(char* buf, size_t len) {
     if (buf && len) {

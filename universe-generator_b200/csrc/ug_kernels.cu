@@ -25,6 +25,21 @@ namespace ug {
 
 // ------------------------------------------------------------------ plan
 
+// Closes the bucket ending at phase position in_phase (a multiple of q) with the
+// count cur; true when the phase stops there: 32 buckets, more than 1e6
+// candidates decided, and the last 32 buckets' count / (32 q) below thr.
+__device__ __forceinline__ bool win_close(int64_t q, int64_t& nb, int64_t& sum, int64_t& cur, int64_t* ring,
+                                          double thr, int64_t in_phase) {
+    if (q <= 0 || in_phase <= 0 || in_phase % q) return false;
+    const int slot = (int)(nb & 31);
+    if (nb >= 32) sum -= ring[slot];
+    ring[slot] = cur;
+    sum += cur;
+    cur = 0;
+    nb++;
+    return nb >= 32 && in_phase > 1000000 && (double)sum / (double)(32 * q) < thr;
+}
+
 __global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info) {
     __shared__ int32_t ntiles[kMaxUni];
     const int n = info->n_uni;
@@ -32,40 +47,20 @@ __global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* inf
         UniCtl& c = ctl[u];
         const UniDev& d = U[u];
         int B = 0;
-        // the last round's newly occupied cells (counted by k_commit); in phase 2
-        // they feed the windowed new-volume stop (braid_cuda.cu:1024-1035)
+        // the last round's admissions (k_greedy) and newly occupied cells (k_commit)
+        // close the windows' buckets; rounds end on bucket boundaries
         {
             const int64_t nc = c.round_new;
             c.round_new = 0;
             c.filled += nc;
-            if (c.phase == 2 && c.fwin_target > 0 && c.last_used > 0 && c.state == ST_ACTIVE) {
-                const int64_t bucket = c.fwin_target / 32 > 0 ? c.fwin_target / 32 : 1;
-                int last = (c.fwin_head + c.fwin_len - 1) & 63;
-                if (c.fwin_len == 0 || c.fwin_b[last] >= bucket) {
-                    if (c.fwin_len == 64) {
-                        c.fwin_att -= c.fwin_b[c.fwin_head];
-                        c.fwin_new -= c.fwin_n[c.fwin_head];
-                        c.fwin_head = (c.fwin_head + 1) & 63;
-                        c.fwin_len--;
-                    }
-                    last = (c.fwin_head + c.fwin_len) & 63;
-                    c.fwin_b[last] = 0;
-                    c.fwin_n[last] = 0;
-                    c.fwin_len++;
-                }
-                c.fwin_b[last] += c.last_used;
-                c.fwin_n[last] += nc;
-                c.fwin_att += c.last_used;
-                c.fwin_new += nc;
-                while (c.fwin_len > 1 && c.fwin_att - c.fwin_b[c.fwin_head] >= c.fwin_target) {
-                    c.fwin_att -= c.fwin_b[c.fwin_head];
-                    c.fwin_new -= c.fwin_n[c.fwin_head];
-                    c.fwin_head = (c.fwin_head + 1) & 63;
-                    c.fwin_len--;
-                }
-                if (c.fwin_att >= c.fwin_target && c.next_cand - c.phase1_end > 1000000 &&
-                    (double)c.fwin_new / (double)c.fwin_att < c.sub_fill_rate)
-                    c.phase_end = c.next_cand;  // stops below
+            if (c.last_used > 0 && c.state == ST_ACTIVE) {
+                const int64_t in_phase = c.next_cand - c.phase_start;
+                c.win_cur += c.accepted_round;
+                c.fwin_cur += nc;
+                const bool sa = win_close(c.win_q, c.win_nb, c.win_sum, c.win_cur, c.win_ring, c.win_thr, in_phase);
+                const bool sf = win_close(c.fwin_q, c.fwin_nb, c.fwin_sum, c.fwin_cur, c.fwin_ring, c.sub_fill_rate,
+                                          in_phase);
+                if (sa || sf) c.phase_end = c.next_cand;  // stops below
             }
             c.last_used = 0;
         }
@@ -77,25 +72,24 @@ __global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* inf
                 if (c.phase == 1 && d.group_mode == GROUP_SUBPATH) {
                     c.phase = 2;
                     c.phase1_end = c.next_cand;
+                    c.phase_start = c.next_cand;
                     c.phase_end = c.next_cand + c.sub_budget;
                     c.round_B = c.B_cap;  // fresh adaptation (braid_cuda.cu:952)
-                    c.win_att = c.win_adm = 0;
-                    c.win_head = c.win_len = 0;
-                    c.win_target = c.sub_accept_rate > 0
-                                       ? (int64_t)fmin(5e9, fmax(2e7, 30.0 / c.sub_accept_rate))
-                                       : 0;
-                    c.fwin_att = c.fwin_new = 0;
-                    c.fwin_head = c.fwin_len = 0;
-                    c.fwin_target = c.sub_fill_rate > 0
-                                        ? (int64_t)fmin(5e9, fmax(2e7, 30.0 / c.sub_fill_rate))
-                                        : 0;
+                    c.win_thr = c.sub_accept_rate;
+                    c.win_q = win_bucket(c.sub_accept_rate);
+                    c.win_nb = c.win_sum = c.win_cur = 0;
+                    c.fwin_q = win_bucket(c.sub_fill_rate);
+                    c.fwin_nb = c.fwin_sum = c.fwin_cur = 0;
                     continue;
                 }
                 c.state = ST_DONE;
                 break;
             }
             if (c.state == ST_ACTIVE) {
-                const int64_t left = c.phase_end - c.next_cand;
+                int64_t left = c.phase_end - c.next_cand;
+                const int64_t in_phase = c.next_cand - c.phase_start;
+                if (c.win_q > 0) left = min(left, c.win_q - in_phase % c.win_q);
+                if (c.fwin_q > 0) left = min(left, c.fwin_q - in_phase % c.fwin_q);
                 const int cap = c.round_B < d.B_max ? c.round_B : d.B_max;  // per-round buffers hold B_max
                 B = (int)(left < (int64_t)cap ? left : (int64_t)cap);
             }
@@ -1140,38 +1134,6 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
         c.round_B = max(c.round_B >> 1, c.B_min);
     else if (c.S_raw < d.S_max / 4 && c.round_B < c.B_cap)
         c.round_B = min(c.round_B << 1, c.B_cap);
-    // windowed accept-rate stop
-    const double thr = c.phase == 1 ? c.accept_rate : c.sub_accept_rate;
-    if (thr > 0 && c.win_target > 0 && used > 0) {
-        const int64_t bucket = c.win_target / 32 > 0 ? c.win_target / 32 : 1;
-        int last = (c.win_head + c.win_len - 1) & 63;
-        if (c.win_len == 0 || c.win_b[last] >= bucket) {
-            if (c.win_len == 64) {  // drop the oldest bucket
-                c.win_att -= c.win_b[c.win_head];
-                c.win_adm -= c.win_a[c.win_head];
-                c.win_head = (c.win_head + 1) & 63;
-                c.win_len--;
-            }
-            last = (c.win_head + c.win_len) & 63;
-            c.win_b[last] = 0;
-            c.win_a[last] = 0;
-            c.win_len++;
-        }
-        c.win_b[last] += used;
-        c.win_a[last] += k;
-        c.win_att += used;
-        c.win_adm += k;
-        while (c.win_len > 1 && c.win_att - c.win_b[c.win_head] >= c.win_target) {
-            c.win_att -= c.win_b[c.win_head];
-            c.win_adm -= c.win_a[c.win_head];
-            c.win_head = (c.win_head + 1) & 63;
-            c.win_len--;
-        }
-        const int64_t in_phase = c.phase == 1 ? next : next - c.phase1_end;
-        if (c.win_att >= c.win_target && in_phase > 1000000 &&
-            (double)c.win_adm / (double)c.win_att < thr)
-            c.phase_end = next;  // ends this phase at the next plan
-    }
 }
 
 // ---------------------------------------------------------------- commit

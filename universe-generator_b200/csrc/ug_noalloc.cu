@@ -1,10 +1,10 @@
 // ug_noalloc.cu -- parameter dump that allocates no device memory.
 //
 // ug_batch_params stages the regenerated worldline parameters in device
-// buffers it allocates for the call.  Some callers cannot allocate device
-// memory at that point: code that runs while another thread captures a CUDA
-// graph in global mode (cudaMalloc is an illegal call there), or a serving
-// loop that reserved all device memory when it started.  For them,
+// buffers it allocates for the call.  Some callers cannot call cudaMalloc at
+// that point: a serving process that reserved all of its device memory when
+// it started and runs with none to spare, or a host whose allocator policy
+// forbids allocations outside start-up.  For them,
 // ug_batch_params_noalloc stages the same kernel's output in one fixed
 // buffer that lives in the library image: a file-scope __device__ array of
 // kStageBytes (16 MiB), present on every GPU that loads the library until
