@@ -10,16 +10,28 @@ A step is one complete packing job of the workload (every universe run from
 an empty packing to its stop rule).  Multi-GPU: one process per GPU under
 torchrun; universes / replicas are independent, so ranks shard them with no
 data-path collective (weak scaling) and time is the max over ranks.
+
+CPU arms.  Both time COMPLETE jobs (empty packing to the attempt cap) of a
+fixed stratified sample of the workload's universes (cpu_sample): for c3, one
+universe per (dim, F tercile) stratum, the one with the largest cap whose job
+on the reference's CPU path fits a few seconds.  `cpu_baseline` is the oracle
+(the repository's C restatement, threaded prefilter + in-order decisions) on
+those jobs with the workload's conventions; `--impl reference` is the
+reference's own braid_knot code compiled from its source (oracle/_ref/knot_host)
+with the reference's conventions, one sample job per step in rotation.  The
+packer's own rate on exactly the sample jobs is reported beside them.
 """
 
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
-import tempfile
+import re
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -31,10 +43,16 @@ for _p in (ROOT, PKG):
 import numpy as np  # noqa: E402
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
-# DRAM bytes (read + write) per k_prefilter_mixed launch over one complete job of the
-# workload, from the 1-pass ncu capture in profiles/k_prefilter_mixed_c3_dram.md
-PREFILTER_TRAFFIC = {("c3", "mixed"): 1.267e9}
+MIXED_SRC = os.path.join(PKG, "csrc", "ug_mixed.cu")
+# DRAM bytes (read + write) per prefilter launch, averaged over the launches of one
+# complete job of the workload, from a 1-pass ncu capture of that job.  Keyed by the
+# SHA-256 of the prefilter source the capture ran, so a changed kernel reports null
+# instead of a stale figure.
+PREFILTER_TRAFFIC: dict[tuple[str, str, str], float] = {}
 FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+# reference-path cost model for picking affordable sample jobs: seconds ~ cap d T^2 / rate
+REF_COST_RATE = 1.8e8
+REF_JOB_BUDGET_S = 8.0
 
 
 def workloads(name: str, ug, seed0: int):
@@ -47,12 +65,44 @@ def workloads(name: str, ug, seed0: int):
         raise SystemExit(str(e))
 
 
+def cpu_sample(us) -> list[int]:
+    """Universes whose complete jobs the CPU arms time: one per (dim, F tercile)
+    stratum, the largest-cap one whose reference-path job fits REF_JOB_BUDGET_S."""
+    if len(us) == 1:
+        return [0]
+    Fs = sorted(u.T for u in us)
+    t1, t2 = Fs[len(Fs) // 3], Fs[2 * len(Fs) // 3]
+    strata: dict[tuple[int, int], list[int]] = {}
+    for k, u in enumerate(us):
+        strata.setdefault((u.dim, 0 if u.T < t1 else (1 if u.T < t2 else 2)), []).append(k)
+    pick = []
+    for key in sorted(strata):
+        ok = [k for k in strata[key]
+              if us[k].attempts * us[k].dim * us[k].T ** 2 / REF_COST_RATE <= REF_JOB_BUDGET_S]
+        if ok:
+            pick.append(max(ok, key=lambda k: (us[k].attempts, -k)))
+    return pick
+
+
+def sample_desc(us, idx) -> str:
+    tot = sum(u.attempts for u in us)
+    n = sum(us[k].attempts for k in idx)
+    return (f"complete jobs of universes {idx} (d/T/cap: "
+            + ", ".join(f"{us[k].dim}/{us[k].T}/{us[k].attempts}" for k in idx)
+            + f"), {n} candidates = {100.0 * n / tot:.1f}% of the workload's {tot}")
+
+
 def peaks():
     try:
         with open(PEAKS_PATH) as f:
             return json.load(f), "measured"
     except Exception:
         return FALLBACK, "fallback"
+
+
+def src_sha() -> str:
+    with open(MIXED_SRC, "rb") as f:
+        return hashlib.sha256(f.read()).hexdigest()[:16]
 
 
 def start_clock_sampler(out_path: str):
@@ -92,30 +142,53 @@ def clocks_summary(path: str):
             "samples": len(sm)}
 
 
-def cpu_baseline(us, budget_s: float = 20.0):
-    """The oracle (plain-C restatement of the reference path), threaded batch
-    prefilter + in-order recheck on all host cores, on a bounded sample: the
-    leading candidates of the workload's first universes."""
+def cpu_baseline(us, idx, budget_s: float = 40.0):
+    """The oracle (plain-C restatement of the reference path), threaded batch prefilter
+    + in-order decisions on all host cores, on complete jobs of the sample universes
+    with the workload's own conventions and seeds."""
     import oracle as O
 
     cores = os.cpu_count() or 1
-    per = 20000
     done, secs, used = 0, 0.0, []
-    for u in us[:16]:
+    for k in idx:
+        u = us[k]
         m = O.Model(dim=u.dim, T=u.T, rng=u.rng, zgrid=u.zgrid, excl=u.excl, cross1d=u.cross1d,
                     pin=u.pin_sin1, seed=u.seed)
-        n = min(u.attempts, per)
         t0 = time.perf_counter()
-        O.pack(m, n, nthreads=cores, round_size=16384)
+        r = O.pack(m, u.attempts, nthreads=cores, round_size=16384, max_n=u.max_n,
+                   group_mode=u.group_mode, sub_attempts=u.sub_attempts, accept_rate=u.accept_rate)
         secs += time.perf_counter() - t0
-        done += n
-        used.append(f"d{u.dim}/T{u.T}")
+        done += r.attempts
+        used.append(k)
         if secs > budget_s:
             break
     return {"value": done / secs, "unit": "candidates/s", "cores": cores, "kind": "port",
-            "sample": f"first {min(per, max(u.attempts for u in us))} candidates of each of "
-                      f"{len(used)} universes ({', '.join(used)}), {done} candidates in "
-                      f"{secs:.1f} s; oracle threaded prefilter + in-order recheck"}
+            "sample": sample_desc(us, used) + f"; {secs:.1f} s; oracle threaded prefilter + "
+                      "in-order decisions, the workload's conventions and seeds",
+            "universes": used}
+
+
+def matched_gpu(ugb200, us, idx, prec, local, stream):
+    """The packer on exactly the CPU arms' sample jobs (same universes and seeds),
+    batched, device-timed: the like-for-like GPU figure beside the CPU rates."""
+    import torch
+
+    sub = [us[k] for k in idx]
+    with ugb200.Packer(sub, precision=prec, device=local, stream=stream.cuda_stream,
+                       rounds_per_sync=8, use_graph=True) as p:
+        p.run()
+        seeds = [u.seed for u in sub]
+        ms, c = 0.0, 0
+        for _ in range(3):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            p.reset(seeds).run()
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            c += sum(p.stats(k).attempts for k in range(len(sub)))
+    return {"value": c / (ms / 1000.0), "unit": "candidates/s", "universes": list(idx)}
 
 
 def combine_ranks(t_ms: float, cands: int, dist, device: str):
@@ -151,51 +224,100 @@ def frames_line(packer):
                       "device-resident paths, densities copied to host"}
 
 
+def precision_report(packer, us, count: int = 2048):
+    """Achieved tensor-core position error against FP64 (first `count` candidates of
+    every universe, all timesteps and axes) and the share of FP64 work."""
+    import ugb200
+
+    err, band, ratio = 0.0, 0.0, 0.0
+    for k, u in enumerate(us):
+        try:
+            e, m, q = packer.mixed_error(k, 0, min(count, u.attempts))
+        except ugb200.UgError:
+            continue  # universe not on the tensor-core path (knot stream)
+        err, band, ratio = max(err, e), max(band, m), max(ratio, q)
+    st = [packer.stats(k) for k in range(len(us))]
+    att = sum(s.attempts for s in st)
+    ev = sum(s.evals for s in st)
+    return {"max_abs_err": err, "widest_band": band, "max_err_to_band": ratio,
+            "gray_frac": sum(s.gray for s in st) / max(att, 1),
+            "evals_fp64_frac": sum(s.evals_fp64 for s in st) / max(ev, 1),
+            "sample": f"first {count} candidates of each universe (all timesteps and axes)"}
+
+
+def reference_gpu(args):
+    """Informational: the reference's own GPU engines (cuda/braid_cuda.cu and
+    cuda/braid_cuda3d.cu, wide builds, compiled unmodified for sm_100a by
+    oracle/Makefile) on this GPU at c1 / c2 shapes with the reference's conventions;
+    attempts / s from their `done:` lines' attempts over the process wall time.  Not
+    bit-comparable (atomicAdd admission order)."""
+    out = {}
+    runs = {"c1": ("braid_cuda_w150", 64, 1_000_000), "c2": ("braid_cuda3d_w150", 128, 1_000_000)}
+    for name, (exe, T, att) in runs.items():
+        path = os.path.join(ROOT, "oracle", "_ref", exe)
+        if not os.path.exists(path):
+            out[name] = {"unavailable": f"oracle/_ref/{exe} not built"}
+            continue
+        cmd = [path, "-t", str(T), "--attempts", str(att), "--terms", str(T), "--maxfreq", str(T),
+               "--seed", "1"]
+        t0 = time.perf_counter()
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+        dt = time.perf_counter() - t0
+        m = re.search(r"done: N=(\d+) in (\d+) attempts", r.stderr)
+        if r.returncode or not m:
+            out[name] = {"unavailable": f"{exe} exit {r.returncode}: {r.stderr.strip()[-200:]}"}
+            continue
+        out[name] = {"value": int(m.group(2)) / dt, "unit": "candidates/s", "N": int(m.group(1)),
+                     "attempts": int(m.group(2)), "wall_s": dt, "cmd": " ".join([exe] + cmd[1:])}
+    return out
+
+
 def reference_arm(args, rank, world):
-    """The reference's own CPU path: reference cuda/braid_knot.cu propose() compiled
-    from the reference source (oracle/_ref/knot_host), all host threads."""
+    """The reference's own CPU path: reference cuda/braid_knot.cu (propose, its
+    eval/collide loop, index-order admission) compiled from the reference source
+    (oracle/_ref/knot_host), all host threads, complete jobs of the sample universes
+    (one per step, in rotation) with the reference's conventions."""
     if rank != 0:
         return 0
     import oracle as O
     import ugb200
 
     us, cfg = workloads(args.workload, ugb200, 0)
-    u = us[0]
     exe = os.path.join(O.REF_DIR, "knot_host")
     if not os.path.exists(exe):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/knot_host not built"}))
         return 0
     cores = os.cpu_count() or 1
-    sample = us[:8]
-    per = 2000  # the reference checks every strand (braid_knot.cu:359-372): O(N) per candidate
-    vals = []
+    idx = cpu_sample(us)
+    done, secs, used = 0, 0.0, []
     for step in range(args.warmup + args.steps):
-        done, secs = 0, 0.0
-        for k, u in enumerate(sample):
-            n = min(u.attempts, per)
-            t0 = time.perf_counter()
-            subprocess.run([exe, "--mode", "pack", "-t", str(u.T), "--dim", str(u.dim),
-                            "--seed", str(1000 * step + k), "--attempts", str(n),
+        k = idx[step % len(idx)]
+        u = us[k]
+        r = subprocess.run([exe, "--mode", "pack", "-t", str(u.T), "--dim", str(u.dim),
+                            "--seed", str(1000 * step + k), "--attempts", str(u.attempts),
                             "--threads", str(cores), "--round", "16384"],
                            capture_output=True, text=True, check=True)
-            secs += time.perf_counter() - t0
-            done += n
-        if step == 0 and secs < 5.0:  # grow the per-universe sample toward ~10 s of CPU work
-            per = int(per * min(8.0, 10.0 / max(secs, 1e-3)))
+        m = re.search(r"in (\d+) attempts \(([0-9.]+) s", r.stderr)
         if step >= args.warmup:
-            vals.append(done / secs)
-    u = sample[0]
-    n = per
-    v = float(np.median(vals)) if vals else 0.0
+            done += int(m.group(1))
+            secs += float(m.group(2))
+            used.append(k)
+    v = done / secs if secs > 0 else 0.0
     line = {"metric": "candidates tested/s", "value": v, "unit": "candidates/s",
             "higher_is_better": True, "impl": "reference", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.workload, **cfg},
+            "same_config": False,
+            "same_config_note": "complete jobs of a stratified sample of the workload's universes "
+                                "(same dim, T, attempt cap); the reference's conventions and "
+                                "candidate stream; the sample is the cheap end of each stratum, "
+                                "so this rate is above the workload's mean for this path",
             "cpu_baseline": {"value": v, "unit": "candidates/s", "cores": cores,
                              "kind": "reference",
-                             "sample": f"up to {n} candidates of each of the first {len(sample)} "
-                                       "universes per step; reference braid_knot.cu propose() + "
-                                       "its eval/collide loop, threaded prefilter + in-order recheck"},
+                             "sample": sample_desc(us, sorted(set(used))) +
+                                       "; one job per step in rotation; reference braid_knot.cu "
+                                       "propose() + its eval/collide loop, threaded prefilter + "
+                                       "in-order recheck, time from its done line"},
             "e2e": {"value": v, "unit": "candidates/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -211,6 +333,9 @@ def main() -> int:
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the FP64 single-universe sweep, the precision report and the "
+                         "reference GPU engines (timing of the workload only)")
     ap.add_argument("--clocks-dir", default="",
                     help="where the nvidia-smi samples of the timed region go (default: the temp dir)")
     ap.add_argument("--profile-case", action="store_true",
@@ -255,18 +380,9 @@ def main() -> int:
                           "evals": sum(s.evals for s in st), "rounds": max(s.rounds for s in st)}))
         return 0
     stream = torch.cuda.Stream()
-    try:
-        packer = ugb200.Packer(us, precision=prec, device=local, stream=stream.cuda_stream,
-                               rounds_per_sync=8, use_graph=True)
-    except ugb200.UgError as e:
-        if prec == ugb200.PREC_MIXED and e.code == ugb200._lib.UG_ENOTSUP:
-            prec = ugb200.PREC_FP64
-            packer = ugb200.Packer(us, precision=prec, device=local, stream=stream.cuda_stream,
-                                   rounds_per_sync=8, use_graph=True)
-        else:
-            raise
+    packer = ugb200.Packer(us, precision=prec, device=local, stream=stream.cuda_stream,
+                           rounds_per_sync=8, use_graph=True)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
-    total_cands = sum(u.attempts for u in us)
 
     base_seeds = [u.seed for u in us]  # reset() writes the new seeds into the universes
 
@@ -302,9 +418,8 @@ def main() -> int:
         cands += sum(packer.stats(k).attempts for k in range(len(us)))
     launches = packer.counters()[0] - launches0
     # accepted sets of the last timed job, for the FP64 single-universe comparison
-    sample = list(range(0, len(us), 8)) if len(us) > 1 else [0]
     last_seeds = seeds(args.warmup + args.steps - 1)
-    acc_batched = {k: packer.accepted(k)[0] for k in sample}
+    acc_batched = [a for a, _ in packer.accepted_all()]
     frames = frames_line(packer) if (args.workload == "c4" and rank == 0) else None
     if sampler:
         sampler.terminate()
@@ -315,8 +430,9 @@ def main() -> int:
     value = cands / (t_ms / 1000.0)
 
     # end to end through the public API with host buffers: CUDA events on the packer's
-    # stream around each job (seed upload, rounds, host syncs, accepted lists read back),
-    # ranks started together and combined like `value` (max time, summed candidates)
+    # stream around each job (seed upload, rounds, host status syncs, and every
+    # universe's accepted indices and group ids read back), ranks started together and
+    # combined like `value` (max time, summed candidates)
     e2e_ms = 0.0
     e2e_c = 0
     nrep = max(1, args.steps // 2)
@@ -328,7 +444,7 @@ def main() -> int:
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         packer.reset(seeds(100 + s)).run()
-        acc = [packer.accepted(k)[0] for k in range(len(us))]
+        acc = packer.accepted_all()
         e1.record(stream)
         e1.synchronize()
         e2e_ms += e0.elapsed_time(e1)
@@ -343,6 +459,9 @@ def main() -> int:
     e2e = {"value": e2e_c / (e2e_ms / 1000.0), "unit": "candidates/s",
            "h2d_bytes_per_step": h2d_b, "d2h_bytes_per_step": d2h_b}
 
+    precision = None
+    if prec == ugb200.PREC_MIXED and not args.no_extras:
+        precision = precision_report(packer, us)
     packer.close()
     # per-kernel timing pass (events around each launch on the packer's stream)
     timer = ugb200.Packer(us, precision=prec, device=local, stream=stream.cuda_stream,
@@ -357,7 +476,7 @@ def main() -> int:
     P, src = peaks()
     pk_s = pk_ms / 1000.0
     avg_s = pk_s / max(pk_n, 1)
-    traffic = PREFILTER_TRAFFIC.get((args.workload, args.precision))
+    traffic = PREFILTER_TRAFFIC.get((args.workload, args.precision, src_sha()))
     # algorithmic units of the prefilter (per launch = job total / launches):
     #  tensor: the contraction 2 d K T per candidate (K = (F-1) + F/2; split-BF16 counted once;
     #          the mixed path evaluates all T timesteps of every candidate)
@@ -384,32 +503,34 @@ def main() -> int:
                 "frac": main["frac"], "traffic": traffic, "tensor": tensor, "hbm": hbm,
                 "launches": pk_n, "avg_launch_ms": pk_ms / max(pk_n, 1),
                 "evals": evals, "visits": sum(s.visits for s in st),
-                "kernel_share": {k: v[0] for k, v in kt.items()}}
+                "kernel_share": {k: v[0] for k, v in kt.items()}, "kernel_src_sha": src_sha()}
 
     # the plain FP64 single-universe form on the same B200 and the same seeds: one
-    # universe per packer, thread-per-candidate FP64 prefilter (the metric's denominator)
-    f_ms, f_c, same = 0.0, 0, True
-    for k in sample:
-        u = us[k]
-        uu = ugb200.Universe(**{**u.__dict__, "seed": last_seeds[k]})
-        with ugb200.Packer([uu], precision=ugb200.PREC_FP64, device=local, stream=stream.cuda_stream,
-                           rounds_per_sync=8, use_graph=True) as p1:
-            p1.run()  # warm-up: builds the CUDA graph of the rounds, as the batched warm-up does
-            p1.reset([last_seeds[k]])
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            p1.run()
-            e1.record(stream)
-            e1.synchronize()
-            f_ms += e0.elapsed_time(e1)
-            f_c += p1.stats(0).attempts
-            same = same and np.array_equal(p1.accepted(0)[0], acc_batched[k])
-    fp64_plain = {"value": f_c / (f_ms / 1000.0), "unit": "candidates/s",
-                  "sample": f"{len(sample)} of the workload's universes (every 8th), each run alone "
-                            f"in FP64 with the seeds of the last timed job, {f_c} candidates",
-                  "same_accepted_set": bool(same)}
-    fp64_plain["mixed_batched_speedup"] = value / fp64_plain["value"]
+    # universe per packer, thread-per-candidate FP64 prefilter (the metric's
+    # denominator), every universe of the workload
+    fp64_plain = None
+    if not args.no_extras:
+        f_ms, f_c, same = 0.0, 0, True
+        for k, u in enumerate(us):
+            uu = ugb200.Universe(**{**u.__dict__, "seed": last_seeds[k]})
+            with ugb200.Packer([uu], precision=ugb200.PREC_FP64, device=local,
+                               stream=stream.cuda_stream, rounds_per_sync=8, use_graph=True) as p1:
+                p1.run()  # warm-up: builds the CUDA graph of the rounds, as the batched warm-up does
+                p1.reset([last_seeds[k]])
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                p1.run()
+                e1.record(stream)
+                e1.synchronize()
+                f_ms += e0.elapsed_time(e1)
+                f_c += p1.stats(0).attempts
+                same = same and np.array_equal(p1.accepted(0)[0], acc_batched[k])
+        fp64_plain = {"value": f_c / (f_ms / 1000.0), "unit": "candidates/s",
+                      "sample": f"all {len(us)} universes of the workload, each run alone in FP64 "
+                                f"with the seeds of the last timed job, {f_c} candidates",
+                      "same_accepted_set": bool(same)}
+        fp64_plain["mixed_batched_speedup"] = value / fp64_plain["value"]
 
     if rank == 0:
         line = {"metric": "candidates tested/s", "value": value, "unit": "candidates/s",
@@ -423,11 +544,17 @@ def main() -> int:
                            "l2": "flushed between steps (256 MiB write)",
                            "parallelism": f"replicas x{world}"},
                 "e2e": e2e, "gpu_launches": launches,
-                "roofline": roofline, "fp64_plain_single_universe": fp64_plain,
+                "roofline": roofline, "precision": precision,
+                "fp64_plain_single_universe": fp64_plain,
                 "frames": frames,
                 "clocks": clocks_summary(clk_path)}
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(us)
+            idx = cpu_sample(us)
+            cb = cpu_baseline(us, idx)
+            cb["matched_gpu"] = matched_gpu(ugb200, us, cb["universes"], prec, local, stream)
+            line["cpu_baseline"] = cb
+        if not args.no_extras:
+            line["reference_gpu"] = reference_gpu(args)
         print(json.dumps(line))
     if dist:
         dist.barrier()

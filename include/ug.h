@@ -149,6 +149,14 @@ int ug_batch_stats(void* h, int32_t u, ug_stats* out);
  * Size query: pass cap = 0 and read *n. */
 int ug_batch_accepted(void* h, int32_t u, int64_t* idx, int32_t* gid, int64_t cap, int64_t* n);
 
+/* Accepted candidate indices and group ids of every universe in one call:
+ * counts[u] (n entries) gets each universe's count, idx / gid (cap entries,
+ * either may be NULL) the lists concatenated in universe order.  A device-side
+ * gather, then one copy per array (the admission logs of all jobs of a
+ * campaign, cuda/braid_knot.cu:449-460, read back at once).  Size query:
+ * cap = 0. */
+int ug_batch_accepted_all(void* h, int64_t* idx, int32_t* gid, int64_t cap, int64_t* counts);
+
 /* Wrapped comoving positions [n][dim][T] of the accepted paths (FP64),
  * the trajectories evalPath fills (braid_cuda.cu:831-862). */
 int ug_batch_positions(void* h, int32_t u, double* pos, int64_t cap_paths);

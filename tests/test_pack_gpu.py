@@ -235,3 +235,23 @@ def test_euclid_exclusion(ug, oracle, dim, T, excl, prec, mode):
     with ug.Packer([cube], precision=prec) as p:
         p.run()
         assert p.stats(0).n < st.n  # the ball excludes less than the cube
+
+
+def test_accepted_all_equals_per_universe(ug):
+    """The bulk read-back (one gather, one copy per array) returns what the
+    per-universe calls return, and the control-block snapshot is reused between
+    reads (no further device-to-host bytes for repeated stats)."""
+    us = [ug.Universe(dim=d, T=T, zgrid=1, excl=1, cross1d=int(d == 1), group_mode=g, seed=s,
+                      attempts=a, round_size=4096)
+          for d, T, g, s, a in [(1, 16, 0, 1, 20000), (2, 24, 2, 2, 30000), (3, 16, 0, 3, 25000),
+                                (2, 32, 0, 4, 40000)]]
+    with ug.Packer(us, precision=1) as p:
+        p.run()
+        per = [p.accepted(k) for k in range(len(us))]
+        bulk = p.accepted_all()
+        for (a, g), (b, h) in zip(per, bulk):
+            assert np.array_equal(a, b) and np.array_equal(g, h)
+        _, _, d0 = p.counters()
+        for k in range(len(us)):
+            p.stats(k)
+        assert p.counters()[2] == d0

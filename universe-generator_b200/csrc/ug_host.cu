@@ -94,6 +94,11 @@ struct Batch {
     int kernels_per_round = 9;
     // CTAs per SM of grid-stride round kernels sized from the occupancy at creation
     int res_sgen = 8, res_shash = 8, res_confl = 16;
+    // bulk read-back staging (ug_batch_accepted_all)
+    int64_t* d_gather_idx = nullptr;
+    int32_t* d_gather_gid = nullptr;
+    int64_t* d_gather_off = nullptr;
+    int64_t gather_cap = 0;
 };
 
 // CTAs per SM a grid-stride kernel is launched with: at most as many as can be
@@ -381,6 +386,7 @@ static int push_unidev(Batch& B) {
 // ---------------------------------------------------------- round launch
 
 static int launch_round(Batch& B, bool timed) {
+    B.synced = false;
     const int g_pre = B.nsm * 8;
     auto tb = [&](int k) {
         if (timed) cudaEventRecord(B.ev[2 * k], B.st);
@@ -461,7 +467,10 @@ static int build_graph(Batch& B, int rounds) {
     return UG_OK;
 }
 
+// Host snapshot of the control blocks.  Work that may change them clears
+// B.synced; reads that find it set use the snapshot without a copy.
 static int pull_ctl(Batch& B) {
+    if (B.synced) return UG_OK;
     CKR(cudaMemcpyAsync(B.hCtl.data(), B.dCtl, sizeof(UniCtl) * B.n, cudaMemcpyDeviceToHost, B.st));
     B.d2h += sizeof(UniCtl) * B.n;
     CKR(cudaStreamSynchronize(B.st));
@@ -520,8 +529,10 @@ static int ensure_capacity(Batch& B, int rounds) {
                 changed = true;
                 int rc2 = push_unidev(B);
                 if (rc2) return rc2;
-                if (k.n_slots > 0)
+                if (k.n_slots > 0) {
+                    B.synced = false;
                     k_rehash<<<B.nsm * 4, 256, 0, B.st>>>(B.dU, B.dCtl, i, k.n_slots);
+                }
                 CKR(cudaGetLastError());
                 CKR(cudaStreamSynchronize(B.st));
             }
@@ -683,6 +694,7 @@ int ug_batch_run(void* h, int64_t max_rounds) {
         if ((rc = ensure_capacity(*B, R))) return rc;
         if (B->opts.use_graph && !B->opts.kernel_timing) {
             if (!B->gexec && (rc = build_graph(*B, R))) return rc;
+            B->synced = false;
             CKR(cudaGraphLaunch(B->gexec, B->st));
         } else {
             for (int r = 0; r < R; r++)
@@ -722,6 +734,7 @@ int ug_batch_reset(void* h, const uint64_t* seeds) {
         init_ctl(u.cfg, u.d, B->hCtl[i]);
         B->hCtl[i].epoch = ep;  // round-hash entries of earlier epochs stay stale
     }
+    B->synced = false;
     CKR(cudaMemcpyAsync(B->dCtl, B->hCtl.data(), sizeof(UniCtl) * B->n, cudaMemcpyHostToDevice, B->st));
     B->h2d += sizeof(UniCtl) * B->n;
     return push_unidev(*B);
@@ -772,8 +785,50 @@ int ug_batch_accepted(void* h, int32_t u, int64_t* idx, int32_t* gid, int64_t ca
         std::vector<Pt64> tmp(N);
         CKR(cudaMemcpy2D(tmp.data(), sizeof(Pt64), d.pts, sizeof(Pt64) * d.T, sizeof(Pt64), N,
                          cudaMemcpyDeviceToHost));
+        B->d2h += N * sizeof(Pt64);
         for (int64_t i = 0; i < N; i++) gid[i] = tmp[i].gid;
     }
+    return UG_OK;
+}
+
+int ug_batch_accepted_all(void* h, int64_t* idx, int32_t* gid, int64_t cap, int64_t* counts) {
+    Batch* B = (Batch*)h;
+    if (!B || !counts) return fail(UG_EINVAL, "bad arguments");
+    int rc = pull_ctl(*B);
+    if (rc) return rc;
+    std::vector<int64_t> off(B->n + 1, 0);
+    for (int u = 0; u < B->n; u++) {
+        counts[u] = B->hCtl[u].n_slots;
+        off[u + 1] = off[u] + counts[u];
+    }
+    const int64_t total = off[B->n];
+    if (cap <= 0 || total == 0) return UG_OK;
+    if (cap < total) return fail(UG_ECAP, "accepted buffer too small (%lld < %lld)", (long long)cap, (long long)total);
+    if (total > B->gather_cap) {
+        cudaFree(B->d_gather_idx);
+        cudaFree(B->d_gather_gid);
+        B->d_gather_idx = nullptr;
+        B->d_gather_gid = nullptr;
+        const int64_t c = pow2_at_least(total);
+        CKR(cudaMalloc(&B->d_gather_idx, (size_t)c * sizeof(int64_t)));
+        CKR(cudaMalloc(&B->d_gather_gid, (size_t)c * sizeof(int32_t)));
+        B->gather_cap = c;
+    }
+    if (!B->d_gather_off) CKR(cudaMalloc(&B->d_gather_off, (size_t)(kMaxUni + 1) * sizeof(int64_t)));
+    CKR(cudaMemcpyAsync(B->d_gather_off, off.data(), off.size() * sizeof(int64_t), cudaMemcpyHostToDevice, B->st));
+    B->h2d += off.size() * sizeof(int64_t);
+    k_gather_accepted<<<B->n, 256, 0, B->st>>>(B->dU, B->d_gather_off, B->d_gather_idx, B->d_gather_gid);
+    CKR(cudaGetLastError());
+    B->launches++;
+    if (idx) {
+        CKR(cudaMemcpyAsync(idx, B->d_gather_idx, (size_t)total * sizeof(int64_t), cudaMemcpyDeviceToHost, B->st));
+        B->d2h += total * sizeof(int64_t);
+    }
+    if (gid) {
+        CKR(cudaMemcpyAsync(gid, B->d_gather_gid, (size_t)total * sizeof(int32_t), cudaMemcpyDeviceToHost, B->st));
+        B->d2h += total * sizeof(int32_t);
+    }
+    CKR(cudaStreamSynchronize(B->st));
     return UG_OK;
 }
 
@@ -975,6 +1030,7 @@ int ug_batch_restore(void* h, int32_t u, int64_t n, const int64_t* idx, const in
     if ((rc = push_unidev(*B))) return rc;
     // rebuild control block: k_commit reads these and accumulates hash keys and cells
     UniCtl k = B->hCtl[u];
+    B->synced = false;
     const int32_t epoch = k.epoch;
     init_ctl(U.cfg, d, k);
     k.epoch = epoch;
@@ -1094,6 +1150,9 @@ int ug_batch_destroy(void* h) {
     }
     cudaFree(B->dU);
     cudaFree(B->dCtl);
+    cudaFree(B->d_gather_idx);
+    cudaFree(B->d_gather_gid);
+    cudaFree(B->d_gather_off);
     cudaFree(B->dInfo);
     for (int k = 0; k < 2 * K_NK; k++)
         if (B->ev[k]) cudaEventDestroy(B->ev[k]);

@@ -1358,4 +1358,20 @@ void launch_params(const UniDev* dU, int u, int64_t n, double* a2, double* a, in
     k_params<<<blocks, 128, 0, st>>>(dU, u, n, a2, a, b, f);
 }
 
+// ------------------------------------------------------------- read-back
+
+// Accepted candidate indices and group labels of every universe into one
+// contiguous pair of arrays (universe u at [off[u], off[u+1])), so that a
+// caller reads all of them back with one copy each.  One CTA per universe.
+__global__ void k_gather_accepted(const UniDev* __restrict__ U, const int64_t* __restrict__ off,
+                                  int64_t* __restrict__ idx, int32_t* __restrict__ gid) {
+    const int u = blockIdx.x;
+    const UniDev& d = U[u];
+    const int64_t o = off[u], n = off[u + 1] - o;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        idx[o + i] = d.acc_idx[UG_IDX(i, d.slot_cap)];
+        gid[o + i] = d.pts[UG_IDX(i * d.T, d.slot_cap * d.T)].gid;
+    }
+}
+
 }  // namespace ug

@@ -62,6 +62,8 @@ __global__ void k_conflicts(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo
 __global__ void k_greedy(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_commit(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_rehash(const UniDev* __restrict__ U, UniCtl* ctl, int u, int64_t n_slots);
+__global__ void k_gather_accepted(const UniDev* __restrict__ U, const int64_t* __restrict__ off,
+                                  int64_t* __restrict__ idx, int32_t* __restrict__ gid);
 
 // k_surv_gemm: terms per shared-memory chunk; two stages of A and B per warp.
 constexpr int kGemmKC = 8;

@@ -22,7 +22,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 
 EXPORTS = (
     "ug_version", "ug_last_error", "ug_struct_sizes", "ug_batch_create", "ug_batch_run", "ug_batch_done",
-    "ug_batch_stats", "ug_batch_accepted", "ug_batch_positions", "ug_batch_params",
+    "ug_batch_stats", "ug_batch_accepted", "ug_batch_accepted_all", "ug_batch_positions", "ug_batch_params",
     "ug_batch_params_noalloc",
     "ug_batch_kernel_times", "ug_batch_reset_times", "ug_batch_counters", "ug_batch_mixed_error",
     "ug_batch_destroy", "ug_pack_create", "ug_pack_run", "ug_pack_stats", "ug_pack_destroy",
@@ -93,6 +93,7 @@ def load():
     L.ug_batch_reset.argtypes = [vp, vp]
     L.ug_batch_stats.argtypes = [vp, i32, C.POINTER(Stats)]
     L.ug_batch_accepted.argtypes = [vp, i32, vp, vp, i64, C.POINTER(i64)]
+    L.ug_batch_accepted_all.argtypes = [vp, vp, vp, i64, vp]
     L.ug_batch_positions.argtypes = [vp, i32, vp, i64]
     L.ug_batch_params.argtypes = [vp, i32, vp, vp, vp, vp, i64]
     L.ug_batch_params_noalloc.argtypes = [vp, i32, vp, vp, vp, vp, i64]

@@ -132,6 +132,22 @@ class Packer:
                                           n.value, C.byref(n)))
         return idx, gid
 
+    def accepted_all(self) -> list[tuple[np.ndarray, np.ndarray]]:
+        """(indices, group ids) of every universe, read back in one gather and one
+        copy per array."""
+        lib = L.load()
+        n = len(self.universes)
+        counts = np.zeros(n, np.int64)
+        L.check(lib.ug_batch_accepted_all(self._h, None, None, 0, counts.ctypes.data))
+        total = int(counts.sum())
+        idx = np.zeros(total, np.int64)
+        gid = np.zeros(total, np.int32)
+        if total:
+            L.check(lib.ug_batch_accepted_all(self._h, idx.ctypes.data, gid.ctypes.data, total,
+                                              counts.ctypes.data))
+        cuts = np.cumsum(counts)[:-1]
+        return list(zip(np.split(idx, cuts), np.split(gid, cuts)))
+
     def positions(self, u: int = 0) -> np.ndarray:
         n = self.stats(u).n
         uni = self.universes[u]
