@@ -123,6 +123,13 @@ int ug_last_error(char* buf, size_t len);
  * No reference counterpart (the engines' interface is argv and files). */
 int ug_struct_sizes(int64_t* sizes, int32_t n);
 
+/* Self-test of the bounded device waits (no reference counterpart): a kernel
+ * waits on an mbarrier that nothing completes, with the wait routine of the
+ * tensor-core prefilter and a limit of limit_ns (at most 10 s); the wait gives
+ * up and the kernel stores UG_ETIMEDOUT in *status and returns, leaving the
+ * context usable.  Returns UG_OK when the kernel ran. */
+int ug_selftest_bounded_wait(int64_t limit_ns, int32_t* status);
+
 /* Create a batch of independent universes on one GPU (replaces one engine
  * process per job, braidlab/orchestrator.py:85-147).  The library owns all
  * device memory inside the handle. */

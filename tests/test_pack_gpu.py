@@ -255,3 +255,20 @@ def test_accepted_all_equals_per_universe(ug):
         for k in range(len(us)):
             p.stats(k)
         assert p.counters()[2] == d0
+
+
+def test_bounded_wait_gives_up_and_context_stays_usable(ug, oracle):
+    """A device wait that nothing completes ends after its limit with UG_ETIMEDOUT
+    (no trap, no hang), and the context keeps working."""
+    import ctypes as C
+    import time
+
+    from ugb200 import _lib
+
+    st = C.c_int32(-1)
+    t0 = time.perf_counter()
+    assert _lib.load().ug_selftest_bounded_wait(50_000_000, C.byref(st)) == 0
+    assert st.value == _lib.UG_ETIMEDOUT
+    assert time.perf_counter() - t0 >= 0.05
+    u = ug.Universe(dim=2, T=16, seed=9, attempts=5000, round_size=1024)
+    _check(ug, oracle, u, precision=1)

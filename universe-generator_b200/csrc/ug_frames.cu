@@ -258,17 +258,46 @@ __global__ void k_fb_refine(FPaths P, FFront F, double ox, double oy, const doub
 // Density scatter: hit offsets binned over the closed square [-chi_max, chi_max]^2.
 // Every hit lies on a front of radius chi <= chi_max, so every hit is counted:
 // an offset that FP32 rounding puts a hair past an edge goes to the edge bin.
-__global__ void k_fb_density(const ug_hit* hits, int64_t n, double chiMax, int bins, uint32_t* grid) {
-    const float inv = (float)(bins / (2.0 * chiMax));
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const ug_hit h = hits[i];
-        int cx = (int)floorf((h.dx + (float)chiMax) * inv);
-        int cy = (int)floorf((h.dy + (float)chiMax) * inv);
-        cx = cx < 0 ? 0 : (cx >= bins ? bins - 1 : cx);
-        cy = cy < 0 ? 0 : (cy >= bins ? bins - 1 : cy);
-        atomicAdd(&grid[(size_t)cy * bins + cx], 1u);
+// Privatised by bands of rows: CTA b owns rows [b rows, (b+1) rows) of the grid in
+// shared memory, streams all hits of the frame (coalesced, L2-resident), counts
+// the ones in its band with shared-memory atomics and writes its band once,
+// coalesced -- no global atomics and no separate clear of the grid.  The hit count
+// is n, or *count (capped at cap) when count is given (read on the device).
+__global__ void k_fb_density(const ug_hit* __restrict__ hits, int64_t n, const unsigned long long* count,
+                             unsigned long long cap, double chiMax, int bins, int rows, uint32_t* grid) {
+    extern __shared__ uint32_t band[];
+    const int r0 = blockIdx.x * rows;
+    const int nr = min(rows, bins - r0);
+    const int cells = nr * bins;
+    for (int i = threadIdx.x; i < cells; i += blockDim.x) band[i] = 0u;
+    __syncthreads();
+    if (count) {
+        const unsigned long long c = *count;
+        n = (int64_t)(c < cap ? c : cap);
     }
+    const float inv = (float)(bins / (2.0 * chiMax));
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const ug_hit h = hits[i];
+        int cy = (int)floorf((h.dy + (float)chiMax) * inv);
+        cy = cy < 0 ? 0 : (cy >= bins ? bins - 1 : cy);
+        if (cy < r0 || cy >= r0 + nr) continue;
+        int cx = (int)floorf((h.dx + (float)chiMax) * inv);
+        cx = cx < 0 ? 0 : (cx >= bins ? bins - 1 : cx);
+        atomicAdd(&band[(cy - r0) * bins + cx], 1u);
+    }
+    __syncthreads();
+    uint32_t* out = grid + (size_t)r0 * bins;
+    for (int i = threadIdx.x; i < cells; i += blockDim.x) out[i] = band[i];
+}
+
+// Rows per density band: bands of at most 48 KB of shared memory.
+inline int density_rows(int bins) { return std::max(1, std::min(bins, 12288 / bins)); }
+
+inline void launch_density(const ug_hit* hits, int64_t n, const unsigned long long* count,
+                           unsigned long long cap, double chiMax, int bins, uint32_t* grid, cudaStream_t st) {
+    const int rows = density_rows(bins);
+    const int bands = (bins + rows - 1) / rows;
+    k_fb_density<<<bands, 512, (size_t)rows * bins * 4, st>>>(hits, n, count, cap, chiMax, bins, rows, grid);
 }
 
 double h_eta(double z) { return log(tan(z / 2.0)); }
@@ -335,22 +364,6 @@ __global__ void k_fb_from_params(int64_t m, const int32_t* bi, double* bd) {
         bd[i] = (double)bi[i];
 }
 
-// Density scatter of one (frame, observer): the hit count is read on the device.
-__global__ void k_fb_density_dev(const ug_hit* hits, const unsigned long long* count, unsigned long long cap,
-                                 double chiMax, int bins, uint32_t* grid) {
-    const unsigned long long c = *count;
-    const int64_t n = (int64_t)(c < cap ? c : cap);
-    const float inv = (float)(bins / (2.0 * chiMax));
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const ug_hit h = hits[i];
-        int cx = (int)floorf((h.dx + (float)chiMax) * inv);
-        int cy = (int)floorf((h.dy + (float)chiMax) * inv);
-        cx = cx < 0 ? 0 : (cx >= bins ? bins - 1 : cx);
-        cy = cy < 0 ? 0 : (cy >= bins ? bins - 1 : cy);
-        atomicAdd(&grid[(size_t)cy * bins + cx], 1u);
-    }
-}
-
 // One observer path's parameters on the host (for its comoving position and velocity).
 struct ObsPath {
     std::vector<double> a2, a, b, f;  // [2], [2][nw] x3
@@ -370,8 +383,12 @@ int check_cfg(const ug_frames_cfg* cfg, ug_frames_out* out, int n) {
 // buffer the hits of every (frame, observer) come back sorted by (chi, src); without
 // one only counts and densities do, and no step waits for the host.
 int bake_device(const ug_frames_cfg* cfg, int n, int nw, int bMax, const double* dA2, const double* dA,
-                const double* dB, const double* dF, const std::vector<ObsPath>& obs, ug_frames_out* out) {
+                const double* dB, const double* dF, const std::vector<ObsPath>& obs, ug_frames_out* out,
+                cudaStream_t st) {
     DevBuf buf;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     // Horner when the band is dense enough that one polynomial beats nw sines
     const int horner = (bMax <= 4 * nw) ? 1 : 0;
     double* dS0 = buf.get<double>((size_t)n * 2);
@@ -394,11 +411,10 @@ int bake_device(const ug_frames_cfg* cfg, int n, int nw, int bMax, const double*
     unsigned long long* dCount = buf.get<unsigned long long>((size_t)NF * NO);
     if (!dS0 || !dC || !dZg || !dChig || !dPx || !dPy || !dHits || !dCross || !dCount || (want_density && !dDen))
         return set_error(UG_ENOMEM, "frame_bake: device allocation failed");
-    if (horner) cudaMemset(dC, 0, (size_t)n * 2 * (bMax + 1) * sizeof(double2));
-    k_fb_prep<<<(int)std::min<int64_t>(((int64_t)n * 2 + 127) / 128, 65536), 128>>>(n, nw, bMax, horner, dA, dB,
-                                                                                     dF, dS0, dC);
-    cudaMemset(dCount, 0, (size_t)NF * NO * sizeof(unsigned long long));
-    if (want_density && !want_hits) cudaMemset(dDen, 0, bins2 * NF * NO * 4);
+    if (horner) cudaMemsetAsync(dC, 0, (size_t)n * 2 * (bMax + 1) * sizeof(double2), st);
+    k_fb_prep<<<(int)std::min<int64_t>(((int64_t)n * 2 + 127) / 128, 65536), 128, 0, st>>>(n, nw, bMax, horner, dA,
+                                                                                           dB, dF, dS0, dC);
+    cudaMemsetAsync(dCount, 0, (size_t)NF * NO * sizeof(unsigned long long), st);
     FPaths P{n, nw, bMax, horner, dA2, dS0, dA, dB, dF, dC};
     const double zMin = std::max(2e-3, cfg->zmin_pi * kPiF);
     // fronts and rewind grids of every frame, uploaded once
@@ -441,8 +457,8 @@ int bake_device(const ug_frames_cfg* cfg, int n, int nw, int bMax, const double*
             out->frame_meta[fi * 3 + 2] = Ks[fi];
         }
     }
-    cudaMemcpy(dZg, zgAll.data(), zgAll.size() * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(dChig, chigAll.data(), chigAll.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpyAsync(dZg, zgAll.data(), zgAll.size() * 8, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dChig, chigAll.data(), chigAll.size() * 8, cudaMemcpyHostToDevice, st);
     int64_t written = 0;
     out->hits_total = 0;
     std::vector<ug_hit> hh;
@@ -453,7 +469,7 @@ int bake_device(const ug_frames_cfg* cfg, int n, int nw, int bMax, const double*
         const double* chig = dChig + (size_t)fi * (Mmax + 1);
         {
             const int64_t tot = (int64_t)n * ((F.M + 1 + 3) / 4);
-            k_fb_grid<<<(int)std::min<int64_t>((tot + 127) / 128, 65536), 128>>>(P, F.M, zg, dPx, dPy);
+            k_fb_grid<<<(int)std::min<int64_t>((tot + 127) / 128, 65536), 128, 0, st>>>(P, F.M, zg, dPx, dPy);
         }
         for (int o = 0; o < NO; o++) {
             double ox, oy, bxv = 0.0, byv = 0.0;
@@ -477,34 +493,34 @@ int bake_device(const ug_frames_cfg* cfg, int n, int nw, int bMax, const double*
             unsigned long long* cnt = dCount + (size_t)fi * NO + o;
             const int side = 2 * K + 1;
             const int64_t tot = (int64_t)n * side * side;
-            k_fb_cross<<<(int)std::min<int64_t>((tot + 127) / 128, 1 << 20), 128>>>(
+            k_fb_cross<<<(int)std::min<int64_t>((tot + 127) / 128, 1 << 20), 128, 0, st>>>(
                 P, F, ox, oy, K, cfg->obs_type[o] == 0 ? cfg->obs_path[o] : -1, chig, dPx, dPy, dCross, cnt, hitCap);
-            k_fb_refine<<<1184, 128>>>(P, F, ox, oy, zg, chig, dCross, cnt, hitCap, dHits);
+            k_fb_refine<<<nsm * 8, 128, 0, st>>>(P, F, ox, oy, zg, chig, dCross, cnt, hitCap, dHits);
             if (!want_hits) {
                 if (want_density)
-                    k_fb_density_dev<<<1184, 256>>>(dHits, cnt, hitCap, F.chiMax, cfg->density_bins,
-                                                    dDen + ((size_t)fi * NO + o) * bins2);
+                    launch_density(dHits, 0, cnt, hitCap, F.chiMax, cfg->density_bins,
+                                   dDen + ((size_t)fi * NO + o) * bins2, st);
                 continue;
             }
             unsigned long long nh = 0;
-            cudaError_t e = cudaMemcpy(&nh, cnt, 8, cudaMemcpyDeviceToHost);
+            cudaError_t e = cudaMemcpyAsync(&nh, cnt, 8, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
             if (e != cudaSuccess) {
                 std::string m = std::string("frame_bake: ") + cudaGetErrorString(e);
                 return set_error(UG_ECUDA, m.c_str());
             }
             if (nh > hitCap) return set_error(UG_ECAP, "frame_bake: hit cap overflow (lower the wraps)");
             if (want_density) {
-                cudaMemset(dDen, 0, bins2 * 4);
-                if (nh)
-                    k_fb_density<<<(int)std::min<unsigned long long>((nh + 255) / 256, 65536), 256>>>(
-                        dHits, (int64_t)nh, F.chiMax, cfg->density_bins, dDen);
-                cudaMemcpy(out->density + ((size_t)fi * NO + o) * bins2, dDen, bins2 * 4, cudaMemcpyDeviceToHost);
+                launch_density(dHits, (int64_t)nh, nullptr, hitCap, F.chiMax, cfg->density_bins, dDen, st);
+                cudaMemcpyAsync(out->density + ((size_t)fi * NO + o) * bins2, dDen, bins2 * 4, cudaMemcpyDeviceToHost,
+                                st);
             }
             if (out->hit_count) out->hit_count[(size_t)fi * NO + o] = (int64_t)nh;
             out->hits_total += (int64_t)nh;
             if (written + (int64_t)nh <= out->hit_cap) {
                 hh.resize(nh);
-                if (nh) cudaMemcpy(hh.data(), dHits, nh * sizeof(ug_hit), cudaMemcpyDeviceToHost);
+                if (nh) cudaMemcpyAsync(hh.data(), dHits, nh * sizeof(ug_hit), cudaMemcpyDeviceToHost, st);
+                if (cudaStreamSynchronize(st) != cudaSuccess) return set_error(UG_ECUDA, "frame_bake: hit copy failed");
                 // device append order is scheduling-dependent: sort by (chi, src)
                 std::sort(hh.begin(), hh.end(), [](const ug_hit& x, const ug_hit& y) {
                     return x.chi < y.chi || (x.chi == y.chi && x.src < y.src);
@@ -514,21 +530,24 @@ int bake_device(const ug_frames_cfg* cfg, int n, int nw, int bMax, const double*
             }
         }
     }
-    const cudaError_t e = cudaDeviceSynchronize();
+    const cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         std::string m = std::string("frame_bake: ") + cudaGetErrorString(e);
         return set_error(UG_ECUDA, m.c_str());
     }
     if (!want_hits) {
         std::vector<unsigned long long> counts((size_t)NF * NO);
-        cudaMemcpy(counts.data(), dCount, counts.size() * 8, cudaMemcpyDeviceToHost);
+        if (cudaMemcpyAsync(counts.data(), dCount, counts.size() * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return set_error(UG_ECUDA, "frame_bake: count copy failed");
         for (size_t i = 0; i < counts.size(); i++) {
             if (counts[i] > hitCap) return set_error(UG_ECAP, "frame_bake: hit cap overflow (lower the wraps)");
             if (out->hit_count) out->hit_count[i] = (int64_t)counts[i];
             out->hits_total += (int64_t)counts[i];
         }
-        if (want_density &&
-            cudaMemcpy(out->density, dDen, bins2 * NF * NO * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        if (want_density && (cudaMemcpyAsync(out->density, dDen, bins2 * NF * NO * 4, cudaMemcpyDeviceToHost, st) !=
+                                 cudaSuccess ||
+                             cudaStreamSynchronize(st) != cudaSuccess))
             return set_error(UG_ECUDA, "frame_bake: density copy failed");
     }
     if (want_hits && out->hits_total > out->hit_cap) return set_error(UG_ECAP, "frame_bake: hit buffer too small");
@@ -545,12 +564,16 @@ __global__ void k_fb_maxb(int64_t m, const int32_t* b, int* out) {
 }
 
 // Largest frequency of device-resident dump parameters.
-int max_b_device(const int32_t* b, int64_t m, int* out) {
+int max_b_device(const int32_t* b, int64_t m, int* out, cudaStream_t st) {
     int* d = nullptr;
     if (cudaMalloc(&d, 4) != cudaSuccess) return set_error(UG_ENOMEM, "frame_bake: device allocation failed");
-    cudaMemset(d, 0, 4);
-    k_fb_maxb<<<592, 256>>>(m, b, d);
-    const cudaError_t e = cudaMemcpy(out, d, 4, cudaMemcpyDeviceToHost);
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaMemsetAsync(d, 0, 4, st);
+    k_fb_maxb<<<nsm * 4, 256, 0, st>>>(m, b, d);
+    cudaError_t e = cudaMemcpyAsync(out, d, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFree(d);
     return e == cudaSuccess ? UG_OK : set_error(UG_ECUDA, "frame_bake: reduction failed");
 }
@@ -558,13 +581,16 @@ int max_b_device(const int32_t* b, int64_t m, int* out) {
 // Frames of the accepted paths of a packer universe, straight from the device
 // (the dump -> frame_bake pipeline without a CSV or host round trip).
 int frames_from_params(const ug_frames_cfg* cfg, int n, int nw, int bMax, const double* dA2, const double* dA,
-                       const int32_t* dBi, const double* dF, ug_frames_out* out) {
+                       const int32_t* dBi, const double* dF, ug_frames_out* out, cudaStream_t st) {
     int rc = check_cfg(cfg, out, n);
     if (rc) return rc;
     DevBuf buf;
     double* dB = buf.get<double>((size_t)n * 2 * nw);
     if (!dB) return set_error(UG_ENOMEM, "frame_bake: device allocation failed");
-    k_fb_from_params<<<1184, 256>>>((int64_t)n * 2 * nw, dBi, dB);
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    k_fb_from_params<<<nsm * 8, 256, 0, st>>>((int64_t)n * 2 * nw, dBi, dB);
     std::vector<ObsPath> obs(cfg->n_obs);
     for (int o = 0; o < cfg->n_obs; o++) {
         if (cfg->obs_type[o] != 0) continue;
@@ -575,14 +601,15 @@ int frames_from_params(const ug_frames_cfg* cfg, int n, int nw, int bMax, const 
         q.b.resize(2 * nw);
         q.f.resize(2 * nw);
         std::vector<int32_t> bi(2 * nw);
-        if (cudaMemcpy(q.a2.data(), dA2 + (size_t)p * 2, 16, cudaMemcpyDeviceToHost) != cudaSuccess ||
-            cudaMemcpy(q.a.data(), dA + (size_t)p * 2 * nw, 16 * nw, cudaMemcpyDeviceToHost) != cudaSuccess ||
-            cudaMemcpy(bi.data(), dBi + (size_t)p * 2 * nw, 8 * nw, cudaMemcpyDeviceToHost) != cudaSuccess ||
-            cudaMemcpy(q.f.data(), dF + (size_t)p * 2 * nw, 16 * nw, cudaMemcpyDeviceToHost) != cudaSuccess)
+        if (cudaMemcpyAsync(q.a2.data(), dA2 + (size_t)p * 2, 16, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaMemcpyAsync(q.a.data(), dA + (size_t)p * 2 * nw, 16 * nw, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaMemcpyAsync(bi.data(), dBi + (size_t)p * 2 * nw, 8 * nw, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaMemcpyAsync(q.f.data(), dF + (size_t)p * 2 * nw, 16 * nw, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
             return set_error(UG_ECUDA, "frame_bake: observer copy failed");
         for (int j = 0; j < 2 * nw; j++) q.b[j] = bi[j];
     }
-    return bake_device(cfg, n, nw, bMax, dA2, dA, dB, dF, obs, out);
+    return bake_device(cfg, n, nw, bMax, dA2, dA, dB, dF, obs, out, st);
 }
 
 }  // namespace ug
@@ -603,10 +630,18 @@ extern "C" int ug_frame_bake(const ug_frames_cfg* cfg, int32_t n, int32_t nw, co
     double* dB = buf.get<double>(m);
     double* dF = buf.get<double>(m);
     if (!dA2 || !dA || !dB || !dF) return set_error(UG_ENOMEM, "frame_bake: device allocation failed");
-    cudaMemcpy(dA2, a2, (size_t)n * 2 * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(dA, a, m * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(dB, b, m * 8, cudaMemcpyHostToDevice);
-    cudaMemcpy(dF, f, m * 8, cudaMemcpyHostToDevice);
+    // the library's own stream for this call (host buffers in, host buffers out)
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+        return set_error(UG_ECUDA, "frame_bake: stream creation failed");
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamDestroy(s); }
+    } guard{st};
+    cudaMemcpyAsync(dA2, a2, (size_t)n * 2 * 8, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dA, a, m * 8, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dB, b, m * 8, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dF, f, m * 8, cudaMemcpyHostToDevice, st);
     std::vector<ObsPath> obs(cfg->n_obs);
     for (int o = 0; o < cfg->n_obs; o++) {
         if (cfg->obs_type[o] != 0) continue;
@@ -616,7 +651,7 @@ extern "C" int ug_frame_bake(const ug_frames_cfg* cfg, int32_t n, int32_t nw, co
         obs[o].b.assign(b + p * 2 * nw, b + (p + 1) * 2 * nw);
         obs[o].f.assign(f + p * 2 * nw, f + (p + 1) * 2 * nw);
     }
-    return bake_device(cfg, n, nw, bMax, dA2, dA, dB, dF, obs, out);
+    return bake_device(cfg, n, nw, bMax, dA2, dA, dB, dF, obs, out, st);
 }
 
 // ------------------------------------------------------- observer view remap

@@ -576,6 +576,12 @@ extern "C" {
 
 int ug_version(void) { return 1; }
 
+int ug_selftest_bounded_wait(int64_t limit_ns, int32_t* status) {
+    if (!status || limit_ns < 0 || limit_ns > 10000000000ll) return fail(UG_EINVAL, "bad arguments");
+    const int rc = wait_selftest(limit_ns, status);
+    return rc ? fail(rc, "bounded-wait self-test: %s", cudaGetErrorString(cudaGetLastError())) : UG_OK;
+}
+
 int ug_struct_sizes(int64_t* sizes, int32_t n) {
     const int64_t v[7] = {(int64_t)sizeof(ug_universe_cfg), (int64_t)sizeof(ug_run_opts), (int64_t)sizeof(ug_stats),
                           (int64_t)sizeof(ug_kernel_times), (int64_t)sizeof(ug_hit), (int64_t)sizeof(ug_frames_cfg),
@@ -903,11 +909,11 @@ int ug_batch_frames(void* h, int32_t u, const ug_frames_cfg* cfg, ug_frames_out*
     }
     launch_params(B->dU, u, N, da2, da, db, df, B->st);
     int bMax = 2;
-    if (cudaStreamSynchronize(B->st) != cudaSuccess || (rc = max_b_device(db, N * 2 * nw, &bMax))) {
+    if (cudaStreamSynchronize(B->st) != cudaSuccess || (rc = max_b_device(db, N * 2 * nw, &bMax, B->st))) {
         release();
         return rc ? rc : fail(UG_ECUDA, "frames: parameter kernel failed");
     }
-    rc = frames_from_params(cfg, (int)N, nw, bMax, da2, da, db, df, out);
+    rc = frames_from_params(cfg, (int)N, nw, bMax, da2, da, db, df, out, B->st);
     release();
     return rc;
 }

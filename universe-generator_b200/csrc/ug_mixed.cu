@@ -63,15 +63,19 @@ __device__ __forceinline__ uint64_t globaltimer() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// Bounded wait: gives up after ~1 s of device time.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait: gives up after limit_ns of device time (or 2^26 polls).
+__device__ __forceinline__ bool mbar_wait_ns(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
     if (mbar_try(bar, parity)) return true;
     const uint64_t t0 = globaltimer();
     for (uint32_t it = 0; it < (1u << 26); it++) {
         if (mbar_try(bar, parity)) return true;
-        if ((it & 255) == 0 && globaltimer() - t0 > 1000000000ull) break;
+        if ((it & 255) == 0 && globaltimer() - t0 > limit_ns) break;
     }
     return false;
+}
+// The prefilter's waits: ~1 s.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    return mbar_wait_ns(bar, parity, 1000000000ull);
 }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
@@ -662,6 +666,30 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
     __syncthreads();
     tc_fence_after();
     if (warp == 0) tmem_dealloc(tmem, L.ncols);
+}
+
+// Self-test of the bounded wait: one thread waits on an mbarrier that nothing
+// arrives on.  The wait gives up after limit_ns and the kernel records
+// UG_ETIMEDOUT in *status and returns, as the prefilter does on a stuck pipeline.
+__global__ void k_wait_selftest(uint64_t limit_ns, int32_t* status) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *status = mbar_wait_ns(&bar, 0, limit_ns) ? UG_OK : UG_ETIMEDOUT;
+}
+
+int wait_selftest(int64_t limit_ns, int32_t* status) {
+    int32_t* d = nullptr;
+    if (cudaMalloc(&d, sizeof(int32_t)) != cudaSuccess) return UG_ENOMEM;
+    cudaMemset(d, 0xff, sizeof(int32_t));
+    k_wait_selftest<<<1, 32>>>((uint64_t)limit_ns, d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(status, d, sizeof(int32_t), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? UG_OK : UG_ECUDA;
 }
 
 // FP64 positions of candidates [first, first+count) (Philox stream) for the

@@ -25,5 +25,7 @@ int mixed_error(const UniDev* dU, int u, const UniDev& d, const MixedTables& mt,
                 int64_t count, double* max_err, double* margin, double* max_ratio, cudaStream_t st);
 void launch_params(const UniDev* dU, int u, int64_t n, double* a2, double* a, int32_t* b, double* f,
                    cudaStream_t st);
+// Runs k_wait_selftest on the current device; *status gets its result.
+int wait_selftest(int64_t limit_ns, int32_t* status);
 
 }  // namespace ug
