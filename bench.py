@@ -25,6 +25,7 @@ packer's own rate on exactly the sample jobs is reported beside them.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import hashlib
 import json
 import os
@@ -333,6 +334,8 @@ def main() -> int:
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="fixed round parameters instead of the autotuned plan (multi-universe workloads)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the FP64 single-universe sweep, the precision report and the "
                          "reference GPU engines (timing of the workload only)")
@@ -380,8 +383,20 @@ def main() -> int:
                           "evals": sum(s.evals for s in st), "rounds": max(s.rounds for s in st)}))
         return 0
     stream = torch.cuda.Stream()
-    packer = ugb200.Packer(us, precision=prec, device=local, stream=stream.cuda_stream,
-                           rounds_per_sync=8, use_graph=True)
+    # round parameters: the autotuned plan for multi-universe workloads (cached per GPU
+    # and workload; tuning time is outside every timed region), else the defaults
+    rps, tuned, tune_info = 8, us, None
+    if len(us) > 1 and not args.no_autotune:
+        from ugb200 import autotune as A
+
+        plan = A.tune(us, precision=prec, device=local, stream=stream.cuda_stream,
+                      log=lambda m: print(m, file=sys.stderr, flush=True))
+        tuned, rps = A.apply(us, plan), int(plan["rounds_per_sync"])
+        tune_info = {"classes": plan["classes"], "rounds_per_sync": rps, "trials": plan["trials"],
+                     "job_ms_tuned": plan["job_s"] * 1e3, "job_ms_default": plan["default_job_s"] * 1e3,
+                     "cached": plan["cached"]}
+    packer = ugb200.Packer(tuned, precision=prec, device=local, stream=stream.cuda_stream,
+                           rounds_per_sync=rps, use_graph=True)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
     base_seeds = [u.seed for u in us]  # reset() writes the new seeds into the universes
@@ -464,8 +479,8 @@ def main() -> int:
         precision = precision_report(packer, us)
     packer.close()
     # per-kernel timing pass (events around each launch on the packer's stream)
-    timer = ugb200.Packer(us, precision=prec, device=local, stream=stream.cuda_stream,
-                          rounds_per_sync=8, use_graph=False, kernel_timing=True)
+    timer = ugb200.Packer(tuned, precision=prec, device=local, stream=stream.cuda_stream,
+                          rounds_per_sync=rps, use_graph=False, kernel_timing=True)
     timer.reset(seeds(args.warmup)).run()
     kt = timer.kernel_times()
     st = [timer.stats(k) for k in range(len(us))]
@@ -542,6 +557,7 @@ def main() -> int:
                 "config": {"workload": args.workload, **cfg,
                            "precision": "mixed" if prec == ugb200.PREC_MIXED else "fp64",
                            "l2": "flushed between steps (256 MiB write)",
+                           "autotune": tune_info or "off (default round parameters)",
                            "parallelism": f"replicas x{world}"},
                 "e2e": e2e, "gpu_launches": launches,
                 "roofline": roofline, "precision": precision,
@@ -551,7 +567,8 @@ def main() -> int:
         if not args.no_cpu_baseline:
             idx = cpu_sample(us)
             cb = cpu_baseline(us, idx)
-            cb["matched_gpu"] = matched_gpu(ugb200, us, cb["universes"], prec, local, stream)
+            same_seeds = [dataclasses.replace(t, seed=u.seed) for t, u in zip(tuned, us)]
+            cb["matched_gpu"] = matched_gpu(ugb200, same_seeds, cb["universes"], prec, local, stream)
             line["cpu_baseline"] = cb
         if not args.no_extras:
             line["reference_gpu"] = reference_gpu(args)

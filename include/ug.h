@@ -70,7 +70,9 @@ typedef struct ug_universe_cfg {
                              grid cells per attempt (0 = off), braid_cuda.cu:960-1035 */
     int32_t euclid;       /* --euclid-collision: exclusion by the L2 ball of radius cell
                              instead of the Chebyshev cube (braid_cuda3d.cu:605-608) */
-    int32_t pad;
+    int32_t surv_cap;     /* survivors resolved per round, at most 8192 (0 = 2^20 / T, 256 for
+                             1+1D); a round is cut at the first survivor beyond it.  Results do
+                             not depend on it */
 } ug_universe_cfg;
 
 typedef struct ug_run_opts {
@@ -122,6 +124,10 @@ int ug_last_error(char* buf, size_t len);
  * check its struct definitions against the library it loaded; no device work.
  * No reference counterpart (the engines' interface is argv and files). */
 int ug_struct_sizes(int64_t* sizes, int32_t n);
+
+/* Name ("<device name> sm_XY") and SM count of a CUDA device (-1: the current
+ * one); the autotuner keys its cache by them.  No reference counterpart. */
+int ug_device_info(int32_t device, char* name, size_t len, int32_t* sms);
 
 /* Self-test of the bounded device waits (no reference counterpart): a kernel
  * waits on an mbarrier that nothing completes, with the wait routine of the

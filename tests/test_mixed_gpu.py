@@ -12,10 +12,11 @@ def _model(O, u):
                    cross1d=u.cross1d, pin=u.pin_sin1, seed=u.seed, euclid=u.euclid)
 
 
-@pytest.mark.parametrize("dim,T,zg,ex", [(2, 16, 0, 0), (2, 64, 1, 1), (3, 128, 1, 1),
-                                         (3, 200, 1, 1), (2, 23, 0, 1), (1, 256, 1, 0)])
-def test_mixed_position_error_within_guard(ug, dim, T, zg, ex):
-    u = ug.Universe(dim=dim, T=T, zgrid=zg, excl=ex, seed=3, attempts=1000, round_size=1024)
+@pytest.mark.parametrize("dim,T,zg,ex,cx", [(2, 16, 0, 0, 0), (2, 64, 1, 1, 0), (3, 128, 1, 1, 0),
+                                            (3, 200, 1, 1, 0), (2, 23, 0, 1, 0), (1, 256, 1, 0, 0),
+                                            (1, 40, 1, 1, 1)])
+def test_mixed_position_error_within_guard(ug, dim, T, zg, ex, cx):
+    u = ug.Universe(dim=dim, T=T, zgrid=zg, excl=ex, cross1d=cx, seed=3, attempts=1000, round_size=1024)
     with ug.Packer([u], precision=ug.PREC_MIXED) as p:
         err, margin, ratio = p.mixed_error(0, 0, 2048)
     print(f"dim={dim} T={T}: max |X_mixed - X_fp64| = {err:.3e}, widest guard {margin:.3e}, "

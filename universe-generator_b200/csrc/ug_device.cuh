@@ -95,11 +95,17 @@ struct UniDev {
     int32_t occ_shift;
     int32_t occ_gw;        // coarse cells per axis
     int64_t occ_per_t;     // coarse cells (2+1, 3+1: bricks) per timestep
-    // second level: one bit per block of 8 (occ cells) per axis, L2-resident
+    // dilated first-level filter: one bit per (timestep, block of 2^occ1_shift
+    // fine cells per axis), set when a committed point lies in a cell within 2
+    // cells (cyclically, every axis) of the block.  Every neighbourhood a test
+    // scans lies within 2 cells of the test point's own cell, so a clear bit of
+    // the own block proves the neighbourhood empty with ONE load.
     uint32_t* occ1;
-    int32_t occ1_gw;
+    int32_t occ1_gw;       // blocks per axis
     int32_t occ_nb;        // 2+1 and 3+1: bricks per axis
     int64_t occ1_per_t;
+    int32_t occ1_shift;
+    int32_t pad_occ1;
     // accepted points
     Pt64* pts;             // [slot_cap * T]
     Pt32* ptf;             // [slot_cap * T]
@@ -508,12 +514,15 @@ __device__ __forceinline__ int64_t occ_bit(const UniDev& U, int t, const int* c)
     }
     return (int64_t)t * U.occ_per_t + (c[0] >> U.occ_shift);  // dim 1
 }
-__device__ __forceinline__ int64_t occ1_bit(const UniDev& U, int t, const int* c) {
+// Dilated filter: true when some committed point may lie within 2 cells of fine
+// cell c at timestep t on every axis (false proves there is none).
+template <int D>
+__device__ __forceinline__ bool occ1_hit(const UniDev& U, int t, const int* c) {
     int64_t lin = 0;
 #pragma unroll
-    for (int ax = 0; ax < 3; ax++)
-        if (ax < U.dim) lin = lin * U.occ1_gw + (c[ax] >> (U.occ_shift + 3));
-    return (int64_t)t * U.occ1_per_t + lin;
+    for (int ax = 0; ax < D; ax++) lin = lin * U.occ1_gw + (c[ax] >> U.occ1_shift);
+    const int64_t b = (int64_t)t * U.occ1_per_t + lin;
+    return (__ldg(U.occ1 + UG_IDX(b >> 5, U.occ1_words)) >> (b & 31)) & 1u;
 }
 
 __device__ __forceinline__ int wrap_cell(int v, int gw) {
@@ -543,56 +552,6 @@ __device__ __forceinline__ void nbhd_make(const UniDev& U, const int* c, const i
 #pragma unroll
         for (int k = 0; k < 4; k++) nb.v[ax][k] = wrap_cell(lo + k, U.gw);
     }
-}
-
-// Second-level occupancy: false proves every cell of the neighbourhood empty.
-// Per axis the range is up to four consecutive cells modulo gw, so its blocks
-// form at most three runs (one wrap); every distinct block is checked.
-template <int D>
-__device__ __forceinline__ bool nbhd_occ1(const UniDev& U, int t, const Nbhd<D>& nb) {
-    const int sh = U.occ_shift + 3;
-    int bl[D][3], nbk[D];
-#pragma unroll
-    for (int ax = 0; ax < D; ax++) {
-        bl[ax][0] = nb.v[ax][0] >> sh;
-        bl[ax][1] = bl[ax][0];
-        bl[ax][2] = bl[ax][0];
-        int cnt = 1;
-#pragma unroll
-        for (int k = 1; k < 4; k++) {
-            if (k >= nb.n[ax]) break;
-            const int bk = nb.v[ax][k] >> sh;
-            const int prev = cnt == 1 ? bl[ax][0] : (cnt == 2 ? bl[ax][1] : bl[ax][2]);
-            if (bk != prev && cnt < 3) {
-                if (cnt == 1)
-                    bl[ax][1] = bk;
-                else
-                    bl[ax][2] = bk;
-                cnt++;
-            }
-        }
-        nbk[ax] = cnt;
-    }
-    const uint32_t* base = U.occ1;
-    const int64_t t0 = (int64_t)t * U.occ1_per_t;
-#pragma unroll
-    for (int i0 = 0; i0 < 3; i0++) {
-        if (i0 >= nbk[0]) break;
-#pragma unroll
-        for (int i1 = 0; i1 < (D > 1 ? 3 : 1); i1++) {
-            if (D > 1 && i1 >= nbk[D > 1 ? 1 : 0]) break;
-#pragma unroll
-            for (int i2 = 0; i2 < (D > 2 ? 3 : 1); i2++) {
-                if (D > 2 && i2 >= nbk[D > 2 ? 2 : 0]) break;
-                int64_t lin = bl[0][i0];
-                if (D > 1) lin = lin * U.occ1_gw + bl[D > 1 ? 1 : 0][i1];
-                if (D > 2) lin = lin * U.occ1_gw + bl[D > 2 ? 2 : 0][i2];
-                const int64_t b = t0 + lin;
-                if ((__ldg(base + UG_IDX(b >> 5, U.occ1_words)) >> (b & 31)) & 1u) return true;
-            }
-        }
-    }
-    return false;
 }
 
 // 4-bit mask x -> bits 4 i (i in x); and -> bits 16 i
@@ -921,9 +880,9 @@ __device__ __forceinline__ bool contacts64_d(const UniDev& U, int t, const doubl
         c[ax] = cell_of(P[ax], U.cell, U.gw);
         z[ax] = 0;
     }
+    if (!occ1_hit<D>(U, t, c)) return false;
     Nbhd<D> nb;
     nbhd_make<D>(U, c, z, z, nb);
-    if (!nbhd_occ1<D>(U, t, nb)) return false;
     return nbhd_scan<D>(U, t, nb, cpt, [&](int32_t p, int32_t& nx) -> bool {
         const Pt64* q = U.pts + UG_IDX((int64_t)p * U.T + t, U.slot_cap * U.T);
         nx = __ldg(&q->next);

@@ -148,6 +148,8 @@ static int validate(const ug_universe_cfg& c) {
     if (c.attempts < 0 || c.max_n < 0 || c.sub_attempts < 0) return fail(UG_EINVAL, "negative budget");
     if (c.round_size < 0 || c.round_size > (1 << 20) || (c.round_size % kTile))
         return fail(UG_EINVAL, "round_size must be a multiple of %d up to 2^20", kTile);
+    if (c.surv_cap < 0 || c.surv_cap > kSmaxCap || (c.surv_cap % 32))
+        return fail(UG_EINVAL, "surv_cap must be a multiple of 32 up to %d", (int)kSmaxCap);
     if (c.cross1d && c.dim != 1) return fail(UG_EINVAL, "cross1d applies to dim 1 only");
     if (c.euclid != 0 && c.euclid != 1) return fail(UG_EINVAL, "bad euclid flag");
     return UG_OK;
@@ -231,6 +233,7 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
     const int T = c.T;
     d.S_max = (int)std::min<int64_t>(kSmaxCap, std::max<int64_t>(256, (1 << 20) / T));
     if (c.dim == 1) d.S_max = 256;  // 1+1D in-round conflicts are found pairwise
+    if (c.surv_cap > 0) d.S_max = c.surv_cap;
     d.S_max = std::min(d.S_max, d.B_max);
     // tables
     std::vector<double> S, Cm, inv;
@@ -319,7 +322,8 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
         h.occ_words = (bits + 31) / 32;
         d.occ_words = h.occ_words;
         if ((rc = dalloc(h, &d.occ, (size_t)h.occ_words, 0))) return rc;
-        d.occ1_gw = (d.occ_gw + 7) >> 3;
+        d.occ1_shift = 2;  // blocks of 4 fine cells per axis
+        d.occ1_gw = (d.gw + 3) >> 2;
         int64_t per1 = 1;
         for (int ax = 0; ax < c.dim; ax++) per1 *= d.occ1_gw;
         d.occ1_per_t = per1;
@@ -575,6 +579,19 @@ using namespace ug;
 extern "C" {
 
 int ug_version(void) { return 1; }
+
+int ug_device_info(int32_t device, char* name, size_t len, int32_t* sms) {
+    int dev = device;
+    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return fail(UG_ECUDA, "no current device");
+    cudaDeviceProp prop;
+    const cudaError_t e = cudaGetDeviceProperties(&prop, dev);
+    if (e != cudaSuccess) return fail(UG_ECUDA, "cudaGetDeviceProperties(%d): %s", dev, cudaGetErrorString(e));
+    if (name && len) {
+        snprintf(name, len, "%s sm_%d%d", prop.name, prop.major, prop.minor);
+    }
+    if (sms) *sms = prop.multiProcessorCount;
+    return UG_OK;
+}
 
 int ug_selftest_bounded_wait(int64_t limit_ns, int32_t* status) {
     if (!status || limit_ns < 0 || limit_ns > 10000000000ll) return fail(UG_EINVAL, "bad arguments");

@@ -1181,6 +1181,55 @@ __device__ __forceinline__ void occ_set(uint32_t* words, int64_t bit, int64_t nw
     if (!(__ldcg(w) & m)) atomicOr(w, m);
 }
 
+__device__ __forceinline__ void occ_set_mask(uint32_t* words, int64_t w, uint32_t m, int64_t nwords) {
+    uint32_t* p = words + UG_IDX(w, nwords);
+    if ((__ldcg(p) & m) != m) atomicOr(p, m);
+}
+
+// Dilated filter: marks every block holding a cell within 2 cells (cyclically)
+// of fine cell c on every axis -- per axis the blocks of c-2 .. c+2 (two, or
+// three across the seam of a partial last block).
+__device__ __forceinline__ void occ1_mark(const UniDev& d, int t, const int* c) {
+    int bk[3][3], nb[3] = {1, 1, 1};
+#pragma unroll
+    for (int ax = 0; ax < 3; ax++) {
+        bk[ax][0] = bk[ax][1] = bk[ax][2] = 0;
+        if (ax >= d.dim) continue;
+        int n = 0;
+#pragma unroll
+        for (int dl = -2; dl <= 2; dl++) {
+            const int b = wrap_cell(c[ax] + dl, d.gw) >> d.occ1_shift;
+            if (n == 0 || (b != bk[ax][n - 1] && b != bk[ax][0])) {
+                if (n < 3) bk[ax][n] = b;
+                n++;
+            }
+        }
+        nb[ax] = n < 3 ? n : 3;
+    }
+    // along the last axis the blocks are neighbouring bits: one masked update per word
+    const int L = d.dim - 1;
+    const int64_t t0 = (int64_t)t * d.occ1_per_t;
+    for (int i0 = 0; i0 < (L > 0 ? nb[0] : 1); i0++)
+        for (int i1 = 0; i1 < (L > 1 ? nb[1] : 1); i1++) {
+            int64_t row = 0;
+            if (L > 0) row = bk[0][i0];
+            if (L > 1) row = row * d.occ1_gw + bk[1][i1];
+            row = t0 + row * d.occ1_gw;
+            int64_t wcur = -1;
+            uint32_t m = 0;
+            for (int i = 0; i < nb[L]; i++) {
+                const int64_t bit = row + bk[L][i];
+                if ((bit >> 5) != wcur) {
+                    if (m) occ_set_mask(d.occ1, wcur, m, d.occ1_words);
+                    wcur = bit >> 5;
+                    m = 0;
+                }
+                m |= 1u << (bit & 31);
+            }
+            occ_set_mask(d.occ1, wcur, m, d.occ1_words);
+        }
+}
+
 __global__ void __launch_bounds__(256) k_commit(const UniDev* __restrict__ U, UniCtl* ctl,
                                                 RoundInfo* info) {
     const int n_uni = info->n_uni, total = info->total_spt;
@@ -1209,7 +1258,7 @@ __global__ void __launch_bounds__(256) k_commit(const UniDev* __restrict__ U, Un
                 grid_insert(d, c, t, lin_cell(cc, d.dim, d.gw), cells_per_t(d), (int32_t)slot, &old, &new_key);
                 new_cell = old < 0;
                 occ_set(d.occ, occ_bit(d, t, cc), d.occ_words);
-                occ_set(d.occ1, occ1_bit(d, t, cc), d.occ1_words);
+                occ1_mark(d, t, cc);
                 q.next = old;
                 q.gid = d.sgid[UG_IDX(r, d.S_max)];
                 d.pts[UG_IDX(slot * d.T + t, d.slot_cap * d.T)] = q;

@@ -236,7 +236,7 @@ __device__ __noinline__ bool group_contact(const UniDev& d, int32_t p, int t, in
 // r + m of X.  Group rounds (grp != nullptr): a certain contact joins the
 // candidate to the contact's group in *grp (shared by the row's threads); a
 // certain contact with a second group rejects.
-template <int D, bool kEuclid>
+template <int D, bool kEuclid, bool kCheckL1 = true>
 __device__ __forceinline__ int test32_d(const UniDev& d, int t, const float* X, float r, float m,
                                         float inv_cell, int64_t cpt, bool* gray, int* grp, int* nvis) {
     // L2 ball: the FP32 distance vector is within sqrt(D) m of the exact one; r 1e-6
@@ -245,19 +245,24 @@ __device__ __forceinline__ int test32_d(const UniDev& d, int t, const float* X, 
     const float mE = kEuclid ? m * (D == 3 ? 1.7320508f : (D == 2 ? 1.4142136f : 1.0f)) * 1.001f + r * 1e-6f : m;
     const float band = mE * inv_cell + 1e-4f;
     int c[D], elo[D], ehi[D];
+    float fr[D];
 #pragma unroll
     for (int ax = 0; ax < D; ax++) {
         const float u = (X[ax] + 1.0f) * inv_cell;
         const float fl = floorf(u);
-        const float fr = u - fl;
+        fr[ax] = u - fl;
         int cc = (int)fl;
         c[ax] = cc >= d.gw ? d.gw - 1 : (cc < 0 ? 0 : cc);
-        elo[ax] = fr < band ? 1 : 0;
-        ehi[ax] = fr > 1.0f - band ? 1 : 0;
+    }
+    // the neighbourhood below lies within 2 cells of c on every axis
+    if (kCheckL1 && !occ1_hit<D>(d, t, c)) return 0;
+#pragma unroll
+    for (int ax = 0; ax < D; ax++) {
+        elo[ax] = fr[ax] < band ? 1 : 0;
+        ehi[ax] = fr[ax] > 1.0f - band ? 1 : 0;
     }
     Nbhd<D> nb;
     nbhd_make<D>(d, c, elo, ehi, nb);
-    if (!nbhd_occ1<D>(d, t, nb)) return 0;
     const float rin = r - mE, rout = r + mE;
     const float rin2 = rin > 0.f ? rin * rin : -1.f, rout2 = rout * rout;
     bool g = false;
@@ -297,12 +302,12 @@ __device__ __forceinline__ int test32_d(const UniDev& d, int t, const float* X, 
     return deep ? 1 : 0;
 }
 
-template <bool kEuclid>
+template <bool kEuclid, bool kCheckL1 = true>
 __device__ __forceinline__ int test32_at(const UniDev& d, int t, const float* X, float r, float m,
                                          float inv_cell, int64_t cpt, bool* gray, int* grp, int* nvis) {
-    if (d.dim == 3) return test32_d<3, kEuclid>(d, t, X, r, m, inv_cell, cpt, gray, grp, nvis);
-    if (d.dim == 2) return test32_d<2, kEuclid>(d, t, X, r, m, inv_cell, cpt, gray, grp, nvis);
-    return test32_d<1, false>(d, t, X, r, m, inv_cell, cpt, gray, grp, nvis);  // 1 axis: ball == cube
+    if (d.dim == 3) return test32_d<3, kEuclid, kCheckL1>(d, t, X, r, m, inv_cell, cpt, gray, grp, nvis);
+    if (d.dim == 2) return test32_d<2, kEuclid, kCheckL1>(d, t, X, r, m, inv_cell, cpt, gray, grp, nvis);
+    return test32_d<1, false, kCheckL1>(d, t, X, r, m, inv_cell, cpt, gray, grp, nvis);  // 1 axis: ball == cube
 }
 
 // --------------------------------------------------------------- kernel
@@ -320,7 +325,11 @@ struct MixedLaunch {
 
 constexpr int kMxThreads = 512;  // 4 threads per candidate row
 constexpr int kMxParts = kMxThreads / kTile;
-constexpr int kMxCompact = 24;   // live rows of a warp at or below which their tests are spread (16, 24, 32 measured)
+constexpr int kXsFloats = 8 * 3 * 32 + 32 + 16;  // per-warp epilogue staging: positions, rho, columns
+constexpr int kMxCompact = 24;
+// the epilogue staging of all warps fits in the smallest pair of operand stages (T <= 16)
+static_assert((kMxThreads / 32) * kXsFloats * 4 <= 2 * (2 * kAImgBytes + 16 * kKC * 2 * 2),
+              "epilogue staging exceeds the operand stages");   // live rows of a warp at or below which their tests are spread (16, 24, 32 measured)
 
 // kGroup: the batch holds group-mode universes (group rounds need the join /
 // two-group logic in the neighbour scans; batches without them run without it).
@@ -406,6 +415,9 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
         const uint32_t idesc = idesc_bf16(128, nm);
         const float r = (float)d.cell, mrg = d.mx_margin, inv_cell = (float)(1.0 / d.cell);
         const int64_t cpt = cells_per_t(d);
+        const uint32_t* __restrict__ occ1 = d.occ1;
+        const int gw = d.gw, occ1_gw = d.occ1_gw, occ1_sh = d.occ1_shift;
+        const int64_t occ1_pt = d.occ1_per_t;
         // group semantics this round (unique-group mode, or phase 2 of the subpath mode)
         const bool group = kGroup && !dump &&
                            (d.group_mode == GROUP_UNIQUE || (d.group_mode == GROUP_SUBPATH && ctl[u].phase == 2));
@@ -423,7 +435,10 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                 double sumE = 0.0, sumEb = 0.0;
                 if (pass == 0 && valid) {
                     const uint4 o = philox_block(d.seed, idx, ax, 0);
-                    a2f[ax] = d.pin ? 0.f : (float)((double)o.x * (1.0 / 2147483648.0) - 1.0);
+                    const float v = d.pin ? 0.f : (float)((double)o.x * (1.0 / 2147483648.0) - 1.0);
+#pragma unroll
+                    for (int k = 0; k < 3; k++)  // selects: a dynamic index would go to local memory
+                        if (k == ax) a2f[k] = v;
                 }
                 for (int ch = 0; ch < nch; ch++, seq++) {
                     const int st = seq & 1;
@@ -478,7 +493,10 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                     __syncthreads();
                     const double tot = ss[0] + ss[2] + ss[4] + ss[6];
                     const double teb = ss[1] + ss[3] + ss[5] + ss[7];
-                    inv_sum[ax] = valid ? (float)(1.0 / tot) : 0.f;
+                    const float iv = valid ? (float)(1.0 / tot) : 0.f;
+#pragma unroll
+                    for (int k = 0; k < 3; k++)
+                        if (k == ax) inv_sum[k] = iv;
                     if (valid) rho = fmaxf(rho, (float)(teb / tot));
                     __syncthreads();
                 }
@@ -520,27 +538,36 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                     float a0 = fabsf(d0);
                     hit = a0 < rin;
                     g = !hit && a0 <= rout;
-                    for (int t = 1; t < T && !hit; t++) {
-                        const float d1 = torus_deltaf(xs[row * pitch + t] - __ldg(&q[t].c[0]));
-                        const float a1 = fabsf(d1);
-                        if (a1 < rin) {
-                            hit = true;
-                            break;
+                    // the path's points 8 timesteps at a time: 8 independent loads in flight
+                    // (the lanes of a warp read the same path: one request serves the warp)
+                    for (int t0 = 1; t0 < T && !hit; t0 += 8) {
+                        float qv[8];
+#pragma unroll
+                        for (int k = 0; k < 8; k++) qv[k] = t0 + k < T ? __ldg(&q[t0 + k].c[0]) : 0.f;
+#pragma unroll
+                        for (int k = 0; k < 8; k++) {
+                            if (hit || t0 + k >= T) break;
+                            const float d1 = torus_deltaf(xs[row * pitch + t0 + k] - qv[k]);
+                            const float a1 = fabsf(d1);
+                            if (a1 < rin) {
+                                hit = true;
+                                break;
+                            }
+                            g = g || a1 <= rout;
+                            // crossing: certain when both signs are certain and the sum is clear of 1
+                            const bool flip = (d0 < 0.f) != (d1 < 0.f);
+                            const bool signs_sure = a0 > mrg && a1 > mrg;
+                            const float sum = a0 + a1;
+                            if (flip && signs_sure && sum < 1.f - 2.f * mrg) {
+                                hit = true;
+                                break;
+                            }
+                            if ((!signs_sure && sum < 1.f + 2.f * mrg) ||
+                                (flip && sum >= 1.f - 2.f * mrg && sum <= 1.f + 2.f * mrg))
+                                g = true;
+                            d0 = d1;
+                            a0 = a1;
                         }
-                        g = g || a1 <= rout;
-                        // crossing: certain when both signs are certain and the sum is clear of 1
-                        const bool flip = (d0 < 0.f) != (d1 < 0.f);
-                        const bool signs_sure = a0 > mrg && a1 > mrg;
-                        const float sum = a0 + a1;
-                        if (flip && signs_sure && sum < 1.f - 2.f * mrg) {
-                            hit = true;
-                            break;
-                        }
-                        if ((!signs_sure && sum < 1.f + 2.f * mrg) ||
-                            (flip && sum >= 1.f - 2.f * mrg && sum <= 1.f + 2.f * mrg))
-                            g = true;
-                        d0 = d1;
-                        a0 = a1;
                     }
                     nev += T;
                     if (hit) vrej[row] = 1;
@@ -556,74 +583,124 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                 if (col0 >= T) break;
                 if (!dump && __all_sync(0xffffffffu, vrej[row] != 0)) break;
                 float x[3][8];
-                for (int ax = 0; ax < dim; ax++)
-                    tmem_ld8(lane_base + (uint32_t)UG_IDX(ax * nm + c0 + 7, L.ncols) - 7, x[ax]);
+#pragma unroll
+                for (int ax = 0; ax < 3; ax++)
+                    if (ax < dim) tmem_ld8(lane_base + (uint32_t)UG_IDX(ax * nm + c0 + 7, L.ncols) - 7, x[ax]);
                 tmem_wait_ld();
-                // Few live rows: spread their (row, column) tests over all 32 lanes, column
-                // by column, instead of leaving the dead rows' lanes idle.  The staged
-                // positions live in this warp's slice of the (now idle) operand stages.
-                const uint32_t am = dump ? 0u : __ballot_sync(0xffffffffu, valid && !vrej[row]);
-                const int na = __popc(am);
-                if (!dump && na <= kMxCompact) {
-                    if (na == 0) continue;
-                    const int ncol = min(8, T - col0);
-                    float* xs = reinterpret_cast<float*>(sm) + warp * (8 * 3 * 32 + 32);  // [8][3][32] + rho[32]
-#pragma unroll
-                    for (int j = 0; j < 8; j++)
-#pragma unroll
-                        for (int ax = 0; ax < 3; ax++)
-                            if (j < ncol && ax < dim)
-                                xs[(j * 3 + ax) * 32 + lane] = torus_wrapf(fmaf(x[ax][j], inv_sum[ax], a2f[ax]));
-                    xs[8 * 3 * 32 + lane] = rho;
-                    __syncwarp();
-                    const int nitems = na * ncol;
-                    for (int i = lane; i < nitems; i += 32) {
-                        const int j = i / na, src = __fns(am, 0, i - j * na + 1);
-                        const int rrow = (warp & 3) * 32 + src;
-                        if (vrej[rrow]) continue;
-                        const int t = __ldg(d.order + col0 + j);
-                        float X[3];
-                        for (int ax = 0; ax < dim; ax++) X[ax] = xs[(j * 3 + ax) * 32 + src];
-                        const float bnd = fminf(2.f, 2.f * (float)__ldg(d.invsinz + t) * xs[8 * 3 * 32 + src]);
+                if (dump) {
+                    for (int j = 0; j < 8; j++) {
+                        const int col = col0 + j;
+                        if (col >= T) break;
+                        // the crossing rule's B image (1+1D) holds the timesteps in natural order
+                        const int t = (dim == 1 && d.cross1d) ? col : __ldg(d.order + col);
+                        // guard band of this timestep (1% over the bound: FP32 evaluation of it)
+                        const float bnd = fminf(2.f, 2.f * (float)__ldg(d.invsinz + t) * rho);
                         const float mt = (2.f * d.mx_mc1 * bnd + d.mx_mc0) * 1.01f;
-                        nev++;
-                        bool gr = false;
-                        int* gp = (kGroup && group) ? s_grp + rrow : nullptr;
-                        const int dead = (kEuclid && d.euclid)
-                                             ? test32_at<true>(d, t, X, r, mt, inv_cell, cpt, &gr, gp, &nvis)
-                                             : test32_at<false>(d, t, X, r, mt, inv_cell, cpt, &gr, gp, &nvis);
-                        if (dead) vrej[rrow] = 1;
-                        if (gr) vgray[rrow] = 1;
-                    }
-                    __syncwarp();
-                    continue;
-                }
-                for (int j = 0; j < 8; j++) {
-                    const int col = col0 + j;
-                    if (col >= T) break;
-                    const int t = __ldg(d.order + col);
-                    float X[3];
-                    for (int ax = 0; ax < dim; ax++) X[ax] = torus_wrapf(fmaf(x[ax][j], inv_sum[ax], a2f[ax]));
-                    // guard band of this timestep (1% over the bound: FP32 evaluation of it)
-                    const float bnd = fminf(2.f, 2.f * (float)__ldg(d.invsinz + t) * rho);
-                    const float mt = (2.f * d.mx_mc1 * bnd + d.mx_mc0) * 1.01f;
-                    if (dump) {
                         if (valid) {
                             for (int ax = 0; ax < dim; ax++)
-                                L.dump[((size_t)off * T + t) * dim + ax] = X[ax];
+                                L.dump[((size_t)off * T + t) * dim + ax] =
+                                    torus_wrapf(fmaf(x[ax][j], inv_sum[ax], a2f[ax]));
                             L.dump_m[(size_t)off * T + t] = mt;
+                        }
+                    }
+                    continue;
+                }
+                const uint32_t am = __ballot_sync(0xffffffffu, valid && !vrej[row]);
+                const int na = __popc(am);
+                if (na == 0) continue;
+                const int ncol = min(8, T - col0);
+                // The block's work is its (live row, column) tests.  Many live rows: each
+                // lane tests its own row's columns.  Few (<= kMxCompact): the tests are
+                // spread over all 32 lanes, column-major, so dead rows leave no lane idle.
+                // Either way a lane first issues the first-level loads of all its tests
+                // together (the dilated occupancy bit of each test point's own cell
+                // block; a clear bit proves the neighbourhood empty), then runs the
+                // exact test only where a bit is set.  The block's positions and column
+                // data are staged in this warp's slice of the (now idle) operand stages.
+                float* xs = reinterpret_cast<float*>(sm) + warp * kXsFloats;  // [8][3][32], rho[32], t[8], isz[8]
+                int* xt = reinterpret_cast<int*>(xs + 8 * 3 * 32 + 32);
+                float* xz = xs + 8 * 3 * 32 + 32 + 8;
+                if (lane < ncol) {
+                    const int t = __ldg(d.order + col0 + lane);
+                    xt[lane] = t;
+                    xz[lane] = (float)__ldg(d.invsinz + t);
+                }
+#pragma unroll
+                for (int j = 0; j < 8; j++)
+#pragma unroll
+                    for (int ax = 0; ax < 3; ax++)
+                        if (j < ncol && ax < dim)
+                            xs[(j * 3 + ax) * 32 + lane] = torus_wrapf(fmaf(x[ax][j], inv_sum[ax], a2f[ax]));
+                xs[8 * 3 * 32 + lane] = rho;
+                __syncwarp();
+                const bool spread = na <= kMxCompact;
+                const int nitems = spread ? na * ncol : (((am >> lane) & 1u) ? ncol : 0);
+                const int rbase = (warp & 3) * 32;
+                uint32_t wv[8];
+                uint64_t bsh = 0;  // bit position of each test's block in its word, 5 bits each
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const int i = spread ? lane + 32 * k : k;
+                    wv[k] = 0u;
+                    if (i < nitems) {
+                        const int j = spread ? i / na : k;
+                        const int src = spread ? (int)__fns(am, 0, i - j * na + 1) : lane;
+                        const int t = xt[j];
+                        int64_t lin = 0;
+#pragma unroll
+                        for (int ax = 0; ax < 3; ax++) {
+                            if (ax >= dim) break;
+                            int cc = (int)floorf((xs[(j * 3 + ax) * 32 + src] + 1.0f) * inv_cell);
+                            cc = cc >= gw ? gw - 1 : (cc < 0 ? 0 : cc);
+                            lin = lin * occ1_gw + (cc >> occ1_sh);
+                        }
+                        const int64_t b = (int64_t)t * occ1_pt + lin;
+                        bsh |= (uint64_t)(b & 31) << (5 * k);
+                        wv[k] = __ldg(occ1 + (b >> 5));
+                    }
+                }
+                uint32_t need = 0;
+#pragma unroll
+                for (int k = 0; k < 8; k++) need |= ((wv[k] >> ((bsh >> (5 * k)) & 31)) & 1u) << k;
+                // tests of this lane (main: the row's columns up to its first certain contact)
+                int tested = spread ? (nitems > lane ? (nitems - lane + 31) / 32 : 0) : nitems;
+                while (need) {
+                    const int k = __ffs(need) - 1;
+                    need &= need - 1;
+                    const int i = spread ? lane + 32 * k : k;
+                    const int j = spread ? i / na : k;
+                    const int src = spread ? (int)__fns(am, 0, i - j * na + 1) : lane;
+                    const int rrow = rbase + src;
+                    if (vrej[rrow]) {
+                        if (!spread) {
+                            tested = k;
+                            break;
                         }
                         continue;
                     }
-                    if (vrej[row]) break;
-                    nev++;
+                    const int t = xt[j];
+                    float X[3];
+#pragma unroll
+                    for (int ax = 0; ax < 3; ax++) X[ax] = ax < dim ? xs[(j * 3 + ax) * 32 + src] : 0.f;
+                    // guard band of this timestep (1% over the bound: FP32 evaluation of it)
+                    const float bnd = fminf(2.f, 2.f * xz[j] * xs[8 * 3 * 32 + src]);
+                    const float mt = (2.f * d.mx_mc1 * bnd + d.mx_mc0) * 1.01f;
                     bool gr = false;
-                    int* gp = (kGroup && group) ? s_grp + row : nullptr;
-                    const int dead = (kEuclid && d.euclid) ? test32_at<true>(d, t, X, r, mt, inv_cell, cpt, &gr, gp, &nvis)
-                                                           : test32_at<false>(d, t, X, r, mt, inv_cell, cpt, &gr, gp, &nvis);
-                    if (dead) vrej[row] = 1;
-                    if (gr) vgray[row] = 1;
+                    int* gp = (kGroup && group) ? s_grp + rrow : nullptr;
+                    const int dead = (kEuclid && d.euclid)
+                                         ? test32_at<true, false>(d, t, X, r, mt, inv_cell, cpt, &gr, gp, &nvis)
+                                         : test32_at<false, false>(d, t, X, r, mt, inv_cell, cpt, &gr, gp, &nvis);
+                    if (gr) vgray[rrow] = 1;
+                    if (dead) {
+                        vrej[rrow] = 1;
+                        if (!spread) {
+                            tested = k + 1;
+                            break;
+                        }
+                    }
                 }
+                nev += tested;
+                __syncwarp();
             }
             tc_fence_before();
             __syncthreads();

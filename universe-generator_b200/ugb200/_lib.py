@@ -21,7 +21,7 @@ GROUP_NONE, GROUP_SUBPATH, GROUP_UNIQUE = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 
 EXPORTS = (
-    "ug_version", "ug_last_error", "ug_struct_sizes", "ug_selftest_bounded_wait", "ug_batch_create", "ug_batch_run", "ug_batch_done",
+    "ug_version", "ug_last_error", "ug_struct_sizes", "ug_device_info", "ug_selftest_bounded_wait", "ug_batch_create", "ug_batch_run", "ug_batch_done",
     "ug_batch_stats", "ug_batch_accepted", "ug_batch_accepted_all", "ug_batch_positions", "ug_batch_params",
     "ug_batch_params_noalloc",
     "ug_batch_kernel_times", "ug_batch_reset_times", "ug_batch_counters", "ug_batch_mixed_error",
@@ -39,7 +39,7 @@ class UniverseCfg(C.Structure):
         ("seed", C.c_uint64), ("attempts", C.c_int64), ("max_n", C.c_int64),
         ("sub_attempts", C.c_int64), ("accept_rate", C.c_double),
         ("sub_accept_rate", C.c_double), ("sub_fill_rate", C.c_double),
-        ("euclid", C.c_int32), ("pad", C.c_int32),
+        ("euclid", C.c_int32), ("surv_cap", C.c_int32),
     ]
 
 
@@ -88,6 +88,7 @@ def load():
     L.ug_last_error.argtypes = [C.c_char_p, C.c_size_t]
     L.ug_struct_sizes.argtypes = [vp, i32]
     L.ug_selftest_bounded_wait.argtypes = [i64, vp]
+    L.ug_device_info.argtypes = [i32, C.c_char_p, C.c_size_t, vp]
     L.ug_batch_create.argtypes = [C.POINTER(UniverseCfg), i32, C.POINTER(RunOpts), C.POINTER(vp)]
     L.ug_batch_run.argtypes = [vp, i64]
     L.ug_batch_done.argtypes = [vp]

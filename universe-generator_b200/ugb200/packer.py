@@ -36,6 +36,7 @@ class Universe:
     sub_accept_rate: float = 0.0
     sub_fill_rate: float = 0.0     # --sub-until-fill-rate (newly occupied cells per attempt)
     euclid: int = 0                # --euclid-collision: L2 ball instead of the Chebyshev cube
+    surv_cap: int = 0              # survivors resolved per round (0 = default); results do not depend on it
 
     @property
     def nw(self) -> int:
@@ -47,7 +48,7 @@ class Universe:
                              self.seed & (2**64 - 1), int(self.attempts), int(self.max_n),
                              int(self.sub_attempts), float(self.accept_rate),
                              float(self.sub_accept_rate), float(self.sub_fill_rate),
-                             int(self.euclid), 0)
+                             int(self.euclid), int(self.surv_cap))
 
 
 @dataclass
