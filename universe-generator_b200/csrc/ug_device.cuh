@@ -96,16 +96,18 @@ struct UniDev {
     int32_t occ_gw;        // coarse cells per axis
     int64_t occ_per_t;     // coarse cells (2+1, 3+1: bricks) per timestep
     // dilated first-level filter: one bit per (timestep, block of 2^occ1_shift
-    // fine cells per axis), set when a committed point lies in a cell within 2
-    // cells (cyclically, every axis) of the block.  Every neighbourhood a test
-    // scans lies within 2 cells of the test point's own cell, so a clear bit of
-    // the own block proves the neighbourhood empty with ONE load.
+    // fine cells per axis), set for every block holding a cell that meets the
+    // cube of half-width occ1_reach (the exclusion radius plus the widest guard
+    // band, plus rounding slack) around a committed point.  A test point within
+    // radius + band of some point therefore has its own cell's block marked: a
+    // clear bit proves that no point is near enough to count, with ONE load.
     uint32_t* occ1;
     int32_t occ1_gw;       // blocks per axis
     int32_t occ_nb;        // 2+1 and 3+1: bricks per axis
     int64_t occ1_per_t;
     int32_t occ1_shift;
     int32_t pad_occ1;
+    double occ1_reach;
     // accepted points
     Pt64* pts;             // [slot_cap * T]
     Pt32* ptf;             // [slot_cap * T]

@@ -322,10 +322,19 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
         h.occ_words = (bits + 31) / 32;
         d.occ_words = h.occ_words;
         if ((rc = dalloc(h, &d.occ, (size_t)h.occ_words, 0))) return rc;
-        d.occ1_shift = 2;  // blocks of 4 fine cells per axis
-        d.occ1_gw = (d.gw + 3) >> 2;
+        // the finest blocks within 16 MiB (2^27 bits): commits mark it at random and
+        // every test reads it, so a small map that stays in L2 pays more than fine
+        // blocks (c3 job: 2^27 bits 513 ms, 2^29 515 ms, 2^32 541 ms).  The FP64
+        // path needs the radius alone (the tensor-core setup widens it by the band)
+        d.occ1_reach = d.cell * 1.001;
         int64_t per1 = 1;
-        for (int ax = 0; ax < c.dim; ax++) per1 *= d.occ1_gw;
+        for (int s1 = 0;; s1++) {
+            d.occ1_shift = s1;
+            d.occ1_gw = (d.gw + (1 << s1) - 1) >> s1;
+            per1 = 1;
+            for (int ax = 0; ax < c.dim; ax++) per1 *= d.occ1_gw;
+            if ((int64_t)T * per1 <= ((int64_t)1 << 27) || s1 >= 6) break;
+        }
         d.occ1_per_t = per1;
         h.occ1_words = ((int64_t)T * per1 + 31) / 32;
         d.occ1_words = h.occ1_words;

@@ -1186,25 +1186,27 @@ __device__ __forceinline__ void occ_set_mask(uint32_t* words, int64_t w, uint32_
     if ((__ldcg(p) & m) != m) atomicOr(p, m);
 }
 
-// Dilated filter: marks every block holding a cell within 2 cells (cyclically)
-// of fine cell c on every axis -- per axis the blocks of c-2 .. c+2 (two, or
-// three across the seam of a partial last block).
-__device__ __forceinline__ void occ1_mark(const UniDev& d, int t, const int* c) {
-    int bk[3][3], nb[3] = {1, 1, 1};
+// Dilated filter: marks every block holding a cell that meets the cube of
+// half-width occ1_reach around the committed point x (cells wrap around the
+// torus; per axis at most 5 cells, so at most 5 blocks).
+__device__ __forceinline__ void occ1_mark(const UniDev& d, int t, const double* x) {
+    int bk[3][5], nb[3] = {1, 1, 1};
 #pragma unroll
     for (int ax = 0; ax < 3; ax++) {
-        bk[ax][0] = bk[ax][1] = bk[ax][2] = 0;
+        bk[ax][0] = 0;
         if (ax >= d.dim) continue;
+        const int c0 = (int)floor((x[ax] - d.occ1_reach + 1.0) / d.cell);
+        const int c1 = (int)floor((x[ax] + d.occ1_reach + 1.0) / d.cell);
         int n = 0;
-#pragma unroll
-        for (int dl = -2; dl <= 2; dl++) {
-            const int b = wrap_cell(c[ax] + dl, d.gw) >> d.occ1_shift;
-            if (n == 0 || (b != bk[ax][n - 1] && b != bk[ax][0])) {
-                if (n < 3) bk[ax][n] = b;
-                n++;
-            }
+        for (int c = c0; c <= c1 && n < 5; c++) {
+            int w = c % d.gw;
+            w += w < 0 ? d.gw : 0;
+            const int b = w >> d.occ1_shift;
+            bool seen = false;
+            for (int k = 0; k < n; k++) seen |= bk[ax][k] == b;
+            if (!seen) bk[ax][n++] = b;
         }
-        nb[ax] = n < 3 ? n : 3;
+        nb[ax] = n;
     }
     // along the last axis the blocks are neighbouring bits: one masked update per word
     const int L = d.dim - 1;
@@ -1258,7 +1260,7 @@ __global__ void __launch_bounds__(256) k_commit(const UniDev* __restrict__ U, Un
                 grid_insert(d, c, t, lin_cell(cc, d.dim, d.gw), cells_per_t(d), (int32_t)slot, &old, &new_key);
                 new_cell = old < 0;
                 occ_set(d.occ, occ_bit(d, t, cc), d.occ_words);
-                occ1_mark(d, t, cc);
+                occ1_mark(d, t, q.c);
                 q.next = old;
                 q.gid = d.sgid[UG_IDX(r, d.S_max)];
                 d.pts[UG_IDX(slot * d.T + t, d.slot_cap * d.T)] = q;

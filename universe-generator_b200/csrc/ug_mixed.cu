@@ -843,6 +843,11 @@ int mixed_setup(const ug_universe_cfg& cfg, UniDev& d, MixedTables& mt) {
     const double mc0 = 2.0 * 2e-6 + 4e-7;
     const double m = 2.0 * mc1 * 2.0 + mc0;
     d.mx_margin = (float)m;
+    // first-level filter reach: radius + the widest band a test applies (1.01 m,
+    // sqrt(d) m + r 1e-6 for the L2 ball), with 2% and 1e-3 cell of slack for the
+    // FP32 cell index of the test point
+    d.occ1_reach = d.cell + 1.02 * m * (cfg.euclid ? std::sqrt((double)dim) * 1.001 : 1.0) +
+                   (cfg.euclid ? d.cell * 1e-6 : 0.0) + d.cell * 1e-3;
     d.mx_mc1 = (float)mc1;
     d.mx_mc0 = (float)mc0;
     mt.margin = m;
