@@ -354,6 +354,10 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
     uint64_t* bar_d = bar + 4;   // all MMAs of the pass finished
     uint32_t* holder = reinterpret_cast<uint32_t*>(bar + 5);
 
+    // tile offsets of the universes, for the per-tile lookup of its universe
+    __shared__ int32_t s_toff[kMaxUni + 1];
+    if (L.dump == nullptr)
+        for (int i = tid; i <= info->n_uni; i += blockDim.x) s_toff[i] = info->tile_off[i];
     if (warp == 0) tmem_alloc(holder, L.ncols);
     if (tid == 0) {
         for (int i = 0; i < 5; i++) mbar_init(&bar[i], 1);
@@ -375,17 +379,21 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
 
     // tiles: the first gridDim.x statically, the rest handed out one at a time
     // (tile costs differ by orders of magnitude across universes)
-    __shared__ int s_next;
+    // The next tile is claimed when a tile starts (its atomic's latency hides
+    // behind the tile's work) into one of two slots read after the tile's last
+    // barrier, so a slow reader never sees the slot overwritten.
+    __shared__ int s_next[2];
+    int npar = 0;
     auto next_tile = [&](int cur) -> int {
         if (dump) return cur + (int)gridDim.x;
-        if (tid == 0) s_next = (int)gridDim.x + atomicAdd(&info->tile_next, 1);
         __syncthreads();
-        const int nt = s_next;
-        __syncthreads();
+        const int nt = s_next[npar];
+        npar ^= 1;
         return nt;
     };
     for (int tile = blockIdx.x; tile < total && !timeout; tile = next_tile(tile)) {
-        const int u = dump ? L.u : find_uni(info->tile_off, n_uni, tile);
+        if (!dump && tid == 0) s_next[npar] = (int)gridDim.x + atomicAdd(&info->tile_next, 1);
+        const int u = dump ? L.u : find_uni(s_toff, n_uni, tile);
         const UniDev& d = U[u];
         const int lt = dump ? tile : tile - info->tile_off[u];
         const int off = lt * kTile + row;
