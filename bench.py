@@ -485,7 +485,7 @@ def main() -> int:
     kt = timer.kernel_times()
     st = [timer.stats(k) for k in range(len(us))]
     timer.close()
-    pk_name = "k_prefilter_mixed" if prec == ugb200.PREC_MIXED else "k_prefilter64"
+    pk_name = "k_prefilter_mixed" if prec == ugb200.PREC_MIXED else "k_prefilter64w"
     pk_ms, pk_n = kt.get(pk_name, (0.0, 0))
     evals = sum(s.evals for s in st)
     P, src = peaks()

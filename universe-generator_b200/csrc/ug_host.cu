@@ -51,7 +51,7 @@ enum KernelId {
     K_PLAN, K_PRE, K_MIXED, K_CONFIRM, K_COMPACT, K_SGEN, K_CONFL, K_GREEDY, K_COMMIT, K_SGEMM, K_SHASH,
     K_NK
 };
-static const char* kKernelNames[12] = {"k_plan",      "k_prefilter64", "k_prefilter_mixed",
+static const char* kKernelNames[12] = {"k_plan",      "k_prefilter64w", "k_prefilter_mixed",
                                        "k_confirm64w", "k_compact",     "k_surv_gen",
                                        "k_conflicts", "k_greedy",      "k_commit",
                                        "k_surv_gemm", "k_surv_hash",   ""};
@@ -400,7 +400,6 @@ static int push_unidev(Batch& B) {
 
 static int launch_round(Batch& B, bool timed) {
     B.synced = false;
-    const int g_pre = B.nsm * 8;
     auto tb = [&](int k) {
         if (timed) cudaEventRecord(B.ev[2 * k], B.st);
     };
@@ -422,13 +421,17 @@ static int launch_round(Batch& B, bool timed) {
         launch_prefilter_mixed(B.dU, B.dCtl, B.dInfo, B.nsm, B.any_group, B.any_euclid, B.st);
         te(K_MIXED);
         tb(K_CONFIRM);
-        k_gray_compact<<<B.n, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+        k_gray_compact<<<B.n, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo, 0);
         k_confirm64w<<<B.nsm * 4, 32 * kSurvWarps, kSurvWarps * kConfSmemPerWarp, B.st>>>(B.dU, B.dCtl,
-                                                                                           B.dInfo);
+                                                                                           B.dInfo, 0);
         te(K_CONFIRM);
     } else {
+        // the FP64 form: every candidate of the round, one warp per candidate
+        // (coefficients in shared memory, lanes over timesteps in endpoint-first order)
         tb(K_PRE);
-        k_prefilter64<<<g_pre, kTile, 0, B.st>>>(B.dU, B.dCtl, B.dInfo);
+        k_gray_compact<<<B.n, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo, 1);
+        k_confirm64w<<<B.nsm * 4, 32 * kSurvWarps, kSurvWarps * kConfSmemPerWarp, B.st>>>(B.dU, B.dCtl,
+                                                                                           B.dInfo, 1);
         te(K_PRE);
     }
     tb(K_COMPACT);
@@ -694,8 +697,9 @@ int ug_batch_create(const ug_universe_cfg* cfgs, int32_t n, const ug_run_opts* o
                              (int)(kSurvWarps * kSurvSmemPerWarp)) != cudaSuccess)
         return bail(fail(UG_ECUDA, "smem attribute failed"));
     if (B->any_mixed && (rc = mixed_init_kernels())) return bail(rc);
-    B->kernels_per_round = B->any_mixed ? 11 : 9;
-    if (B->any_mixed && cudaFuncSetAttribute(k_confirm64w, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    B->kernels_per_round = B->any_mixed ? 11 : 10;
+    // the warp FP64 test serves both forms (all candidates, or the undecided ones)
+    if (cudaFuncSetAttribute(k_confirm64w, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)(kSurvWarps * kConfSmemPerWarp)) != cudaSuccess)
         return bail(fail(UG_ECUDA, "smem attribute failed"));
     // one wave per SM, measured on c3 against 8 / 8 / 16 CTAs per SM: k_surv_gen 27.7 ->

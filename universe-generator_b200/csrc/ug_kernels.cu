@@ -2,8 +2,11 @@
 //
 // One round of every active universe:
 //   k_plan         round sizes, phase transitions, tile decomposition
-//   k_prefilter64  FP64 test of every candidate against the committed packing
-//                  (or k_prefilter_mixed + k_confirm64, ug_mixed.cu)
+//   k_gray_compact + k_confirm64w
+//                  FP64 form: every candidate, warp per candidate (shared-memory
+//                  coefficients, lanes over timesteps) against the committed packing;
+//                  mixed form: k_prefilter_mixed (ug_mixed.cu), then the same warp
+//                  test for the candidates its guard band left undecided
 //   k_compact      survivors in candidate-index order (deterministic)
 //   k_surv_gen     FP64 coefficients of the survivors (term-ordered rows)
 //   k_surv_gemm    their FP64 trajectories as a register-tiled product
@@ -199,61 +202,6 @@ __global__ void __launch_bounds__(kTile) k_probe(const UniDev* __restrict__ U, i
 __device__ __forceinline__ bool group_phase(const UniDev& d, const UniCtl& c) {
     return d.group_mode == GROUP_UNIQUE || (d.group_mode == GROUP_SUBPATH && c.phase == 2);
 }
-
-// Thread-per-candidate FP64 generation + test.  kGrayOnly: only candidates
-// whose gray bit the mixed prefilter set (its FP64 guard-band retest).
-template <bool kGrayOnly>
-__device__ __forceinline__ void prefilter64_tiles(const UniDev* __restrict__ U, UniCtl* ctl,
-                                                  RoundInfo* info) {
-    double alpha[3 * (kMaxF + 1)], beta[3 * (kMaxF + 1)], a2[3];
-    int32_t bj[kMaxF];
-    double wj[kMaxF];
-    const int n_uni = info->n_uni, total = info->total_tiles;
-    const int lane = threadIdx.x & 31;
-    for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
-        const int u = find_uni(info->tile_off, n_uni, tile);
-        const UniDev& d = U[u];
-        const UniCtl& c = ctl[u];
-        const int off = (tile - info->tile_off[u]) * kTile + threadIdx.x;
-        const int B = c.B;
-        bool work = off < B;
-        if (kGrayOnly && work) work = (d.gray_bits[off >> 5] >> (off & 31)) & 1u;
-        bool surv = false;
-        int32_t g = -1;
-        int nev = 0, nvis = 0;
-        if (work) {
-            const uint64_t idx = (uint64_t)(c.round_base + off);
-            const int F1 = d.F + 1;
-            if (d.rng == RNG_KNOT) {
-                gen_knot64(d, idx, alpha, beta, a2, bj, wj, 1);
-            } else {
-                for (int ax = 0; ax < d.dim; ax++)
-                    a2[ax] = gen_philox64(d, idx, ax, alpha + ax * F1, beta + ax * F1, 1);
-            }
-            surv = !test64(d, c.n_slots, alpha, beta, a2, group_phase(d, c), &g, &nev, kGrayOnly ? nullptr : &nvis);
-        }
-        for (int o = 16; o > 0; o >>= 1) nev += __shfl_xor_sync(0xffffffffu, nev, o);
-        for (int o = 16; o > 0; o >>= 1) nvis += __shfl_xor_sync(0xffffffffu, nvis, o);
-        if (lane == 0 && nvis) atomicAdd((unsigned long long*)&ctl[u].visits, (unsigned long long)nvis);
-        if (lane == 0 && nev) {
-            atomicAdd((unsigned long long*)&ctl[u].evals_fp64, (unsigned long long)nev);
-            if (!kGrayOnly) atomicAdd((unsigned long long*)&ctl[u].evals, (unsigned long long)nev);
-        }
-        if (kGrayOnly) {
-            if (work && surv) atomicOr(&d.surv_bits[off >> 5], 1u << (off & 31));
-        } else {
-            const uint32_t bits = __ballot_sync(0xffffffffu, surv);
-            if (lane == 0 && (off & ~31) < d.B_max) d.surv_bits[UG_IDX(off >> 5, d.B_max / 32)] = bits;
-        }
-        if (work && d.group_mode != GROUP_NONE) d.g0[UG_IDX(off, d.B_max)] = g;
-    }
-}
-
-__global__ void __launch_bounds__(kTile) k_prefilter64(const UniDev* __restrict__ U, UniCtl* ctl,
-                                                       RoundInfo* info) {
-    prefilter64_tiles<false>(U, ctl, info);
-}
-
 
 // --------------------------------------------------------------- compact
 
@@ -693,7 +641,7 @@ __global__ void __launch_bounds__(256) k_surv_hash(const UniDev* __restrict__ U,
 // Candidates the mixed prefilter could not decide (guard band, or universes
 // outside the tensor-core path), in index order, per universe.
 __global__ void __launch_bounds__(256) k_gray_compact(const UniDev* __restrict__ U, UniCtl* ctl,
-                                                      RoundInfo* info) {
+                                                      RoundInfo* info, int all) {
     __shared__ int32_t wsum[8];
     __shared__ int32_t s_running;
     __shared__ bool s_last;
@@ -707,7 +655,9 @@ __global__ void __launch_bounds__(256) k_gray_compact(const UniDev* __restrict__
     __syncthreads();
     for (int base = 0; base < nwords; base += 256) {
         const int w = base + tid;
-        uint32_t bits = w < nwords ? d.gray_bits[w] : 0u;
+        // all: the FP64 form, every candidate of the round goes to the warp test
+        uint32_t bits = w < nwords ? (all ? 0xffffffffu : d.gray_bits[w]) : 0u;
+        if (all && w < nwords) d.surv_bits[UG_IDX(w, d.B_max / 32)] = 0u;
         if (w == nwords - 1 && (B & 31)) bits &= (1u << (B & 31)) - 1u;
         const int cnt = __popc(bits);
         int incl = cnt;
@@ -756,7 +706,7 @@ __global__ void __launch_bounds__(256) k_gray_compact(const UniDev* __restrict__
 // against the committed packing, timesteps spread over the lanes (the FP64
 // guard-band retest of the mixed path).
 __global__ void __launch_bounds__(32 * kSurvWarps) k_confirm64w(const UniDev* __restrict__ U,
-                                                                  UniCtl* ctl, RoundInfo* info) {
+                                                                  UniCtl* ctl, RoundInfo* info, int all) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     unsigned char* my = smem_raw + (size_t)wib * kConfSmemPerWarp;
@@ -779,7 +729,7 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_confirm64w(const UniDev* __
         const bool group = group_phase(d, c);
         int32_t g = -1;
         bool hitl = false;
-        int nev = 0;
+        int nev = 0, nvis = 0;
         if (d.dim == 1 && d.cross1d) {
             for (int t = lane; t < T; t += 32) P1[t] = eval64(d, alpha, beta, 1, a2[0], t);
             __syncwarp();
@@ -815,7 +765,7 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_confirm64w(const UniDev* __
                     for (int ax = 0; ax < d.dim; ax++)
                         P[ax] = eval64(d, alpha + ax * F1, beta + ax * F1, 1, a2[ax], t);
                     nev++;
-                    hitl = contacts64(d, t, P, group, &g, cpt);
+                    hitl = contacts64(d, t, P, group, &g, cpt, all ? &nvis : nullptr);
                 }
                 if (__any_sync(0xffffffffu, hitl)) break;
             }
@@ -829,10 +779,13 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_confirm64w(const UniDev* __
         }
         if (group) rej = rej || __any_sync(0xffffffffu, g != -1 && g != first);
         for (int o = 16; o > 0; o >>= 1) nev += __shfl_xor_sync(0xffffffffu, nev, o);
+        for (int o = 16; o > 0; o >>= 1) nvis += __shfl_xor_sync(0xffffffffu, nvis, o);
         if (lane == 0) {
             if (!rej) atomicOr(&d.surv_bits[UG_IDX(off >> 5, d.B_max / 32)], 1u << (off & 31));
             if (d.group_mode != GROUP_NONE) d.g0[UG_IDX(off, d.B_max)] = first;
             if (nev) atomicAdd((unsigned long long*)&c.evals_fp64, (unsigned long long)nev);
+            if (all && nev) atomicAdd((unsigned long long*)&c.evals, (unsigned long long)nev);
+            if (nvis) atomicAdd((unsigned long long*)&c.visits, (unsigned long long)nvis);
         }
         __syncwarp();
     }

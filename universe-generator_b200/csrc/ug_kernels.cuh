@@ -48,9 +48,8 @@ __device__ __forceinline__ int find_uni(const int32_t* off, int n, int item) {
 
 // Kernels (ug_kernels.cu)
 __global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
-__global__ void k_prefilter64(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
-__global__ void k_gray_compact(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
-__global__ void k_confirm64w(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
+__global__ void k_gray_compact(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info, int all);
+__global__ void k_confirm64w(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info, int all);
 __global__ void k_compact(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_surv_gen(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info, int warp_bytes);
 __global__ void k_surv_gemm(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
