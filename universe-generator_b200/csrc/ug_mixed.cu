@@ -549,6 +549,7 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                     // the path's points 8 timesteps at a time: 8 independent loads in flight
                     // (the lanes of a warp read the same path: one request serves the warp)
                     for (int t0 = 1; t0 < T && !hit; t0 += 8) {
+                        if (vrej[row]) break;  // another part of the row found a contact
                         float qv[8];
 #pragma unroll
                         for (int k = 0; k < 8; k++) qv[k] = t0 + k < T ? __ldg(&q[t0 + k].c[0]) : 0.f;
