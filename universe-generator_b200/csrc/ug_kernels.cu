@@ -738,10 +738,18 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_confirm64w(const UniDev* __
                 const Pt64* q = d.pts + UG_IDX(s * T + T - 1, d.slot_cap * T) + 1 - T;
                 double d0 = torus_delta(P1[0] - __ldcg(&q[0].c[0]));
                 bool hit = hit1(d0, d.cell, d.inclusive);
-                for (int t = 1; t < T && !hit; t++) {
-                    const double d1 = torus_delta(P1[t] - __ldcg(&q[t].c[0]));
-                    hit = hit1(d1, d.cell, d.inclusive) || crosses_step(d0, d1);
-                    d0 = d1;
+                // the path's points 4 timesteps at a time (4 independent loads in flight)
+                for (int t0 = 1; t0 < T && !hit; t0 += 4) {
+                    double qv[4];
+#pragma unroll
+                    for (int k = 0; k < 4; k++) qv[k] = t0 + k < T ? __ldcg(&q[t0 + k].c[0]) : 0.0;
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        if (hit || t0 + k >= T) break;
+                        const double d1 = torus_delta(P1[t0 + k] - qv[k]);
+                        hit = hit1(d1, d.cell, d.inclusive) || crosses_step(d0, d1);
+                        d0 = d1;
+                    }
                 }
                 if (hit) {
                     if (!group) {
@@ -823,10 +831,21 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
                 const Pt64* Q = d.spos + UG_IDX((int64_t)r2 * T + T - 1, (int64_t)d.S_max * T) + 1 - T;
                 double d0 = torus_delta(P[0].c[0] - Q[0].c[0]);
                 bool hit = hit1(d0, d.cell, d.inclusive);
-                for (int t = 1; t < T && !hit; t++) {
-                    const double d1 = torus_delta(P[t].c[0] - Q[t].c[0]);
-                    hit = hit1(d1, d.cell, d.inclusive) || crosses_step(d0, d1);
-                    d0 = d1;
+                // both paths' points 4 timesteps at a time (independent loads in flight)
+                for (int t0 = 1; t0 < T && !hit; t0 += 4) {
+                    double pv[4], qv[4];
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        pv[k] = t0 + k < T ? P[t0 + k].c[0] : 0.0;
+                        qv[k] = t0 + k < T ? Q[t0 + k].c[0] : 0.0;
+                    }
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        if (hit || t0 + k >= T) break;
+                        const double d1 = torus_delta(pv[k] - qv[k]);
+                        hit = hit1(d1, d.cell, d.inclusive) || crosses_step(d0, d1);
+                        d0 = d1;
+                    }
                 }
                 if (hit) add(r2);
             }
