@@ -538,8 +538,8 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                 __syncthreads();
                 const int64_t ns = ctl[u].n_slots;
                 const float rin = r - mrg, rout = r + mrg;
-                for (int64_t sl = part; sl < ns; sl += kMxParts) {
-                    if (vrej[row]) break;
+                // walk of one accepted path: every timestep up to the first certain contact
+                auto walk = [&](int64_t sl) {
                     const Pt32* q = d.ptf + UG_IDX(sl * T + T - 1, d.slot_cap * T) + 1 - T;
                     bool hit = false, g = false;
                     float d0 = torus_deltaf(xs[row * pitch] - __ldg(&q[0].c[0]));
@@ -547,7 +547,6 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                     hit = a0 < rin;
                     g = !hit && a0 <= rout;
                     // the path's points 8 timesteps at a time: 8 independent loads in flight
-                    // (the lanes of a warp read the same path: one request serves the warp)
                     for (int t0 = 1; t0 < T && !hit; t0 += 8) {
                         if (vrej[row]) break;  // another part of the row found a contact
                         float qv[8];
@@ -581,6 +580,49 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                     nev += T;
                     if (hit) vrej[row] = 1;
                     else if (g) vgray[row] = 1;
+                };
+                // The paths are walked nearest first: a candidate that meets any path
+                // almost always meets one of the two paths beside it at the first
+                // timestep (those lie between it and every other path) first.  Each
+                // part finds the nearest path below and above among its slots; the
+                // row's four parts combine them through the (idle) partial-sum array.
+                float blo = 4.f, bhi = 4.f;  // distances below / above
+                int slo = -1, shi = -1;
+                if (!vrej[row]) {
+                    const float x0 = xs[row * pitch];
+                    for (int64_t sl = part; sl < ns; sl += kMxParts) {
+                        const float dd = torus_deltaf(x0 - __ldg(&d.ptf[UG_IDX(sl * T, d.slot_cap * T)].c[0]));
+                        if (dd >= 0.f) {
+                            if (dd < blo) blo = dd, slo = (int)sl;
+                        } else if (-dd < bhi) {
+                            bhi = -dd, shi = (int)sl;
+                        }
+                    }
+                }
+                float* nbv = reinterpret_cast<float*>(s_sum);        // [kTile][kMxParts][2]
+                int* nbs = reinterpret_cast<int*>(nbv + kTile * kMxParts * 2);
+                nbv[(row * kMxParts + part) * 2] = blo;
+                nbv[(row * kMxParts + part) * 2 + 1] = bhi;
+                nbs[(row * kMxParts + part) * 2] = slo;
+                nbs[(row * kMxParts + part) * 2 + 1] = shi;
+                __syncthreads();
+                blo = bhi = 4.f;  // same scan in every part: the same pair, ties to the lower part
+                slo = shi = -1;
+#pragma unroll
+                for (int p2 = 0; p2 < kMxParts; p2++) {
+                    const float vl = nbv[(row * kMxParts + p2) * 2], vh = nbv[(row * kMxParts + p2) * 2 + 1];
+                    if (vl < blo) blo = vl, slo = nbs[(row * kMxParts + p2) * 2];
+                    if (vh < bhi) bhi = vh, shi = nbs[(row * kMxParts + p2) * 2 + 1];
+                }
+                // every part now holds the same pair: parts 0 and 1 walk it, then
+                // (rows still alive) all parts walk their own slots but those two
+                if (part == 0 && slo >= 0 && !vrej[row]) walk(slo);
+                if (part == 1 && shi >= 0 && !vrej[row]) walk(shi);
+                __syncthreads();
+                for (int64_t sl = part; sl < ns; sl += kMxParts) {
+                    if (vrej[row]) break;
+                    if (sl == slo || sl == shi) continue;
+                    walk(sl);
                 }
                 __syncthreads();
                 continue;  // single pass for dim 1
