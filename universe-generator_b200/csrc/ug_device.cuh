@@ -179,7 +179,7 @@ struct UniCtl {
     int64_t visits;        // prefilter: accepted points examined by the neighbour tests
     int64_t evals_fp64;    // of which evaluated in FP64 (plain path / guard-band retest)
     int32_t stop_at;       // survivors [0, stop_at) resolved this round
-    int32_t pad2;
+    int32_t tile_ns;       // mixed prefilter: slowest tile of the last round (ns), orders the next round's tiles
     int32_t B_min, B_cap;  // round-size adaptation bounds
     int32_t err_code;
     int32_t pad;
@@ -455,6 +455,43 @@ __device__ __forceinline__ double eval64(const UniDev& U, const double* alpha, c
         acc = fma(beta[b * stride], __ldg(Cm + (size_t)b * T), acc);
     }
     return torus_wrap(fma(acc, __ldg(U.invsinz + t), a2));
+}
+
+// eval64 of D axes at once (coefficient rows ax * F1 of alpha / beta): each
+// axis accumulates in eval64's order, so every coordinate has eval64's bits;
+// the axes' chains are independent and the basis loads are shared.
+template <int D>
+__device__ __forceinline__ void eval64x(const UniDev& U, const double* alpha, const double* beta, const double* a2,
+                                        int t, double* P) {
+    const int T = U.T, F = U.F, F1 = F + 1;
+    const double* S = U.S + t;
+    const double* Cm = U.Cm + t;
+    double acc[D];
+#pragma unroll
+    for (int ax = 0; ax < D; ax++) acc[ax] = 0.0;
+    int b = 2;
+#pragma unroll 2
+    for (; b + 1 <= F; b += 2) {
+        const double s0 = __ldg(S + (size_t)b * T), c0 = __ldg(Cm + (size_t)b * T);
+        const double s1 = __ldg(S + (size_t)(b + 1) * T);
+#pragma unroll
+        for (int ax = 0; ax < D; ax++) {
+            acc[ax] = fma(alpha[ax * F1 + b], s0, acc[ax]);
+            acc[ax] = fma(beta[ax * F1 + b], c0, acc[ax]);
+            acc[ax] = fma(alpha[ax * F1 + b + 1], s1, acc[ax]);
+        }
+    }
+    if (b <= F) {
+        const double s0 = __ldg(S + (size_t)b * T), c0 = __ldg(Cm + (size_t)b * T);
+#pragma unroll
+        for (int ax = 0; ax < D; ax++) {
+            acc[ax] = fma(alpha[ax * F1 + b], s0, acc[ax]);
+            acc[ax] = fma(beta[ax * F1 + b], c0, acc[ax]);
+        }
+    }
+    const double iz = __ldg(U.invsinz + t);
+#pragma unroll
+    for (int ax = 0; ax < D; ax++) P[ax] = torus_wrap(fma(acc[ax], iz, a2[ax]));
 }
 
 // ------------------------------------------------------------ grid access

@@ -45,11 +45,17 @@ __device__ __forceinline__ bool win_close(int64_t q, int64_t& nb, int64_t& sum, 
 
 __global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info) {
     __shared__ int32_t ntiles[kMaxUni];
+    __shared__ int32_t cost[kMaxUni];
+    __shared__ int32_t order[kMaxUni];
     const int n = info->n_uni;
     for (int u = threadIdx.x; u < n; u += blockDim.x) {
         UniCtl& c = ctl[u];
         const UniDev& d = U[u];
         int B = 0;
+        // tile cost: the last round's slowest prefilter tile; before any is timed,
+        // dim * T stands in (all universes start together, so one round uses one kind)
+        cost[u] = c.tile_ns > 0 ? c.tile_ns : d.dim * d.T;
+        c.tile_ns = 0;
         // the last round's admissions (k_greedy) and newly occupied cells (k_commit)
         // close the windows' buckets; rounds end on bucket boundaries
         {
@@ -105,10 +111,24 @@ __global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* inf
         ntiles[u] = (B + kTile - 1) / kTile;
     }
     __syncthreads();
+    // Tiles are handed out costliest universe first, so the long tiles start in
+    // the first wave instead of trailing the round (order does not change results).
+    for (int u = threadIdx.x; u < n; u += blockDim.x) {
+        const int cu = ntiles[u] > 0 ? cost[u] : -1;
+        int rank = 0;
+        for (int v = 0; v < n; v++) {
+            const int cv = ntiles[v] > 0 ? cost[v] : -1;
+            rank += cv > cu || (cv == cu && v < u);
+        }
+        order[rank] = u;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
         int acc = 0, act = 0;
-        for (int u = 0; u < n; u++) {
-            info->tile_off[u] = acc;
+        for (int i = 0; i < n; i++) {
+            const int u = order[i];
+            info->tile_off[i] = acc;
+            info->tile_uni[i] = u;
             acc += ntiles[u];
             act |= ntiles[u] > 0;
         }
@@ -320,56 +340,62 @@ __device__ __forceinline__ int32_t rhash_head(const UniDev& d, uint64_t key) {
     return -1;
 }
 
-// Warp-cooperative FP64 regeneration of candidate idx into shared memory:
-// Philox blocks are spread over the lanes, the normalisation sum runs in
-// ascending b on lane 0 -- the same operations, in the same order, as the
-// thread-per-candidate gen_philox64, so the coefficients are identical.
+// Warp-cooperative FP64 regeneration of axis ax of candidate idx (Philox
+// stream) into shared memory: Philox blocks are spread over the lanes, the
+// normalisation sum runs in ascending b on lane 0 -- the same operations, in
+// the same order, as the thread-per-candidate gen_philox64, so the
+// coefficients are identical.
+__device__ __forceinline__ void warp_gen64_axis(const UniDev& d, uint64_t idx, int ax, double* alpha, double* beta,
+                                                double* a2, int lane) {
+    const int F = d.F, F1 = F + 1;
+    double* al = alpha + ax * F1;
+    double* bt = beta + ax * F1;
+    for (int p = lane; 2 * p <= F; p += 32) {
+        const uint4 o = philox_block(d.seed, idx, ax, p);
+        if (p == 0) {
+            a2[ax] = d.pin ? 0.0 : (double)o.x * (1.0 / 2147483648.0) - 1.0;
+            continue;
+        }
+        const int be = 2 * p, bo = 2 * p + 1;
+        const double Ee = -log(((double)o.x + 0.5) * (1.0 / 4294967296.0));
+        al[be] = (o.z & 1u) ? -Ee : Ee;
+        bt[be] = (double)(o.z >> 1) * (1.0 / 2147483648.0) * kPi;
+        if (bo <= F) {
+            const double Eo = -log(((double)o.y + 0.5) * (1.0 / 4294967296.0));
+            al[bo] = (o.w & 1u) ? -Eo : Eo;
+        }
+    }
+    __syncwarp();
+    double sum = 0.0;
+    if (lane == 0)
+        for (int b = 2; b <= F; b++) sum += fabs(al[b]);
+    sum = __shfl_sync(0xffffffffu, sum, 0);
+    for (int b = 2 + lane; b <= F; b += 32) {
+        const double e = al[b];
+        double amp = fabs(e) / sum / (double)b;
+        if (e < 0.0) amp = -amp;
+        if (b & 1) {
+            al[b] = amp;
+            bt[b] = 0.0;
+        } else {
+            double sf, cf;
+            sincos(bt[b], &sf, &cf);
+            al[b] = amp * cf;
+            bt[b] = amp * sf;
+        }
+    }
+    __syncwarp();
+}
+
+// All axes of candidate idx by one warp (the knot stream is sequential: lane 0
+// replays it).
 __device__ __forceinline__ void warp_gen64(const UniDev& d, uint64_t idx, double* alpha, double* beta,
                                        double* a2, int32_t* bj, double* wj, int lane) {
-    const int F = d.F, F1 = F + 1;
     if (d.rng == RNG_KNOT) {
         if (lane == 0) gen_knot64(d, idx, alpha, beta, a2, bj, wj, 1);
         __syncwarp();
     } else {
-        for (int ax = 0; ax < d.dim; ax++) {
-            double* al = alpha + ax * F1;
-            double* bt = beta + ax * F1;
-            for (int p = lane; 2 * p <= F; p += 32) {
-                const uint4 o = philox_block(d.seed, idx, ax, p);
-                if (p == 0) {
-                    a2[ax] = d.pin ? 0.0 : (double)o.x * (1.0 / 2147483648.0) - 1.0;
-                    continue;
-                }
-                const int be = 2 * p, bo = 2 * p + 1;
-                const double Ee = -log(((double)o.x + 0.5) * (1.0 / 4294967296.0));
-                al[be] = (o.z & 1u) ? -Ee : Ee;
-                bt[be] = (double)(o.z >> 1) * (1.0 / 2147483648.0) * kPi;
-                if (bo <= F) {
-                    const double Eo = -log(((double)o.y + 0.5) * (1.0 / 4294967296.0));
-                    al[bo] = (o.w & 1u) ? -Eo : Eo;
-                }
-            }
-            __syncwarp();
-            double sum = 0.0;
-            if (lane == 0)
-                for (int b = 2; b <= F; b++) sum += fabs(al[b]);
-            sum = __shfl_sync(0xffffffffu, sum, 0);
-            for (int b = 2 + lane; b <= F; b += 32) {
-                const double e = al[b];
-                double amp = fabs(e) / sum / (double)b;
-                if (e < 0.0) amp = -amp;
-                if (b & 1) {
-                    al[b] = amp;
-                    bt[b] = 0.0;
-                } else {
-                    double sf, cf;
-                    sincos(bt[b], &sf, &cf);
-                    al[b] = amp * cf;
-                    bt[b] = amp * sf;
-                }
-            }
-            __syncwarp();
-        }
+        for (int ax = 0; ax < d.dim; ax++) warp_gen64_axis(d, idx, ax, alpha, beta, a2, lane);
     }
 }
 
@@ -702,39 +728,66 @@ __global__ void __launch_bounds__(256) k_gray_compact(const UniDev* __restrict__
     }
 }
 
-// One warp per undecided candidate: FP64 regeneration and the exact test
-// against the committed packing, timesteps spread over the lanes (the FP64
-// guard-band retest of the mixed path).
+// FP64 test of one candidate per group of WPI warps: FP64 regeneration and the
+// exact test against the committed packing, timesteps (1+1D: paths) spread
+// over the group's lanes.  WPI = 1 serves the FP64 form (every candidate of the
+// round: many items, throughput); WPI = kSurvWarps the guard-band retest of the
+// mixed form (few items per round, each of which would otherwise bound the
+// launch by one warp's latency): the axes are generated by separate warps and
+// four times the lanes share the timesteps.
+template <int WPI>
+__device__ __forceinline__ void group_sync() {
+    if (WPI == 1)
+        __syncwarp();
+    else
+        __syncthreads();
+}
+
+template <int WPI>
 __global__ void __launch_bounds__(32 * kSurvWarps) k_confirm64w(const UniDev* __restrict__ U,
                                                                   UniCtl* ctl, RoundInfo* info, int all) {
+    static_assert(WPI == 1 || WPI == kSurvWarps, "a group is one warp or the whole block");
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int kG = kSurvWarps / WPI;  // groups per block
+    constexpr int kGT = 32 * WPI;         // threads per group
+    __shared__ int32_t s_hit[kG];
+    __shared__ int32_t s_first[kSurvWarps], s_rej[kSurvWarps];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    unsigned char* my = smem_raw + (size_t)wib * kConfSmemPerWarp;
+    const int grp = wib / WPI, wig = wib % WPI, gt = wig * 32 + lane;
+    unsigned char* my = smem_raw + (size_t)grp * kConfSmemPerWarp;
     double* alpha = (double*)my;
     double* beta = alpha + 3 * (kMaxF + 1);
     double* a2 = beta + 3 * (kMaxF + 1);
     double* wj = a2 + 3;
     int32_t* bj = (int32_t*)(wj + kMaxF);
     double* P1 = (double*)(my + kSurvSmemPerWarpBase);
+    volatile int32_t* vhit = &s_hit[grp];
     const int n_uni = info->n_uni, total = info->total_gray;
-    const int gwarp = blockIdx.x * kSurvWarps + wib, nwarps = gridDim.x * kSurvWarps;
-    for (int item = gwarp; item < total; item += nwarps) {
+    const int ggrp = blockIdx.x * kG + grp, ngrp = gridDim.x * kG;
+    for (int item = ggrp; item < total; item += ngrp) {
         const int u = find_uni(info->gray_pref, n_uni, item);
         const UniDev& d = U[u];
         UniCtl& c = ctl[u];
         const int off = d.gray_off[UG_IDX(item - info->gray_pref[u], d.B_max)];
         const uint64_t idx = (uint64_t)(c.round_base + off);
-        const int F1 = d.F + 1, T = d.T;
-        warp_gen64(d, idx, alpha, beta, a2, bj, wj, lane);
+        const int T = d.T;
+        if (d.rng == RNG_KNOT || WPI == 1) {
+            if (wig == 0) warp_gen64(d, idx, alpha, beta, a2, bj, wj, lane);
+        } else if (wig < d.dim) {
+            warp_gen64_axis(d, idx, wig, alpha, beta, a2, lane);
+        }
+        if (gt == 0) *vhit = 0;
+        group_sync<WPI>();
         const bool group = group_phase(d, c);
         int32_t g = -1;
         bool hitl = false;
         int nev = 0, nvis = 0;
         if (d.dim == 1 && d.cross1d) {
-            for (int t = lane; t < T; t += 32) P1[t] = eval64(d, alpha, beta, 1, a2[0], t);
-            __syncwarp();
-            nev = lane == 0 ? T : 0;
-            for (int64_t s = lane; s < c.n_slots && !(hitl && !group); s += 32) {
+            for (int t = gt; t < T; t += kGT) P1[t] = eval64(d, alpha, beta, 1, a2[0], t);
+            group_sync<WPI>();
+            nev = gt == 0 ? T : 0;
+            for (int64_t s = gt; s < c.n_slots && !(hitl && !group); s += kGT) {
+                if (!group && *vhit) break;  // another lane of the group found a contact
                 const Pt64* q = d.pts + UG_IDX(s * T + T - 1, d.slot_cap * T) + 1 - T;
                 double d0 = torus_delta(P1[0] - __ldcg(&q[0].c[0]));
                 bool hit = hit1(d0, d.cell, d.inclusive);
@@ -754,6 +807,7 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_confirm64w(const UniDev* __
                 if (hit) {
                     if (!group) {
                         hitl = true;
+                        *vhit = 1;
                     } else {
                         const int32_t gq = __ldcg(&q[0].gid);
                         if (g == -1)
@@ -765,20 +819,29 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_confirm64w(const UniDev* __
             }
         } else {
             const int64_t cpt = cells_per_t(d);
-            for (int oi0 = 0; oi0 < T; oi0 += 32) {
-                const int oi = oi0 + lane;
+            for (int oi0 = 0; oi0 < T; oi0 += kGT) {
+                const int oi = oi0 + gt;
                 if (oi < T && !hitl) {
                     const int t = __ldg(d.order + oi);
                     double P[3];
-                    for (int ax = 0; ax < d.dim; ax++)
-                        P[ax] = eval64(d, alpha + ax * F1, beta + ax * F1, 1, a2[ax], t);
+                    if (d.dim == 3)
+                        eval64x<3>(d, alpha, beta, a2, t, P);
+                    else if (d.dim == 2)
+                        eval64x<2>(d, alpha, beta, a2, t, P);
+                    else
+                        eval64x<1>(d, alpha, beta, a2, t, P);
                     nev++;
                     hitl = contacts64(d, t, P, group, &g, cpt, all ? &nvis : nullptr);
                 }
-                if (__any_sync(0xffffffffu, hitl)) break;
+                if (__any_sync(0xffffffffu, hitl)) {
+                    if (lane == 0) *vhit = 1;
+                    break;
+                }
+                if (WPI > 1 && *vhit) break;
             }
         }
-        // merge the lanes: any rejection, or (group) two distinct groups
+        // merge the lanes of each warp, then the warps of the group: any rejection,
+        // or (group rounds) two distinct groups touched
         bool rej = __any_sync(0xffffffffu, hitl);
         int32_t first = -1;
         for (int o = 0; o < 32; o++) {
@@ -789,15 +852,33 @@ __global__ void __launch_bounds__(32 * kSurvWarps) k_confirm64w(const UniDev* __
         for (int o = 16; o > 0; o >>= 1) nev += __shfl_xor_sync(0xffffffffu, nev, o);
         for (int o = 16; o > 0; o >>= 1) nvis += __shfl_xor_sync(0xffffffffu, nvis, o);
         if (lane == 0) {
-            if (!rej) atomicOr(&d.surv_bits[UG_IDX(off >> 5, d.B_max / 32)], 1u << (off & 31));
-            if (d.group_mode != GROUP_NONE) d.g0[UG_IDX(off, d.B_max)] = first;
             if (nev) atomicAdd((unsigned long long*)&c.evals_fp64, (unsigned long long)nev);
             if (all && nev) atomicAdd((unsigned long long*)&c.evals, (unsigned long long)nev);
             if (nvis) atomicAdd((unsigned long long*)&c.visits, (unsigned long long)nvis);
         }
-        __syncwarp();
+        if (WPI > 1) {
+            if (lane == 0) {
+                s_first[wib] = first;
+                s_rej[wib] = rej ? 1 : 0;
+            }
+            __syncthreads();
+            first = -1;
+            rej = false;
+            for (int w = 0; w < WPI; w++) {
+                const int32_t v = s_first[grp * WPI + w];
+                rej = rej || s_rej[grp * WPI + w] != 0 || (v != -1 && first != -1 && v != first);
+                if (first == -1) first = v;
+            }
+        }
+        if (gt == 0) {
+            if (!rej) atomicOr(&d.surv_bits[UG_IDX(off >> 5, d.B_max / 32)], 1u << (off & 31));
+            if (d.group_mode != GROUP_NONE) d.g0[UG_IDX(off, d.B_max)] = first;
+        }
+        group_sync<WPI>();
     }
 }
+template __global__ void k_confirm64w<1>(const UniDev* __restrict__, UniCtl*, RoundInfo*, int);
+template __global__ void k_confirm64w<kSurvWarps>(const UniDev* __restrict__, UniCtl*, RoundInfo*, int);
 
 // One warp per survivor r: the set of earlier survivors r' < r that it
 // touches (Chebyshev contact at any timestep; plus crossings in 1+1D).

@@ -22,7 +22,8 @@ struct RoundInfo {
     int32_t pad_ti;
     int32_t total_sev;     // k_surv_gemm warp tiles (32 rows x 32 timesteps)
     int32_t total_spt;     // survivor timesteps (k_surv_hash / k_commit items)
-    int32_t tile_off[kMaxUni + 1];
+    int32_t tile_off[kMaxUni + 1];   // prefilter tiles: first tile of the i-th universe in tile order
+    int32_t tile_uni[kMaxUni];       // the universe at position i of the tile order
     int32_t surv_off[kMaxUni + 1];
     int32_t gray_pref[kMaxUni + 1];
     int32_t sev_off[kMaxUni + 1];
@@ -49,6 +50,7 @@ __device__ __forceinline__ int find_uni(const int32_t* off, int n, int item) {
 // Kernels (ug_kernels.cu)
 __global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_gray_compact(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info, int all);
+template <int WPI>
 __global__ void k_confirm64w(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info, int all);
 __global__ void k_compact(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_surv_gen(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info, int warp_bytes);

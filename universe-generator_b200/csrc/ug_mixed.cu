@@ -393,9 +393,11 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
     };
     for (int tile = blockIdx.x; tile < total && !timeout; tile = next_tile(tile)) {
         if (!dump && tid == 0) s_next[npar] = (int)gridDim.x + atomicAdd(&info->tile_next, 1);
-        const int u = dump ? L.u : find_uni(s_toff, n_uni, tile);
+        const int pos = dump ? 0 : find_uni(s_toff, n_uni, tile);
+        const int u = dump ? L.u : info->tile_uni[pos];
         const UniDev& d = U[u];
-        const int lt = dump ? tile : tile - info->tile_off[u];
+        const int lt = dump ? tile : tile - s_toff[pos];
+        const uint64_t tile_t0 = tid == 0 ? globaltimer() : 0;
         const int off = lt * kTile + row;
         int64_t base;
         int B;
@@ -774,6 +776,10 @@ __global__ void __launch_bounds__(kMxThreads, 1) k_prefilter_mixed(const UniDev*
                     const int ng = __popc(gb);
                     if (ng) atomicAdd((unsigned long long*)&ctl[u].gray_total, (unsigned long long)ng);
                 }
+            }
+            if (tid == 0) {  // this tile's time orders the next round's tiles
+                const uint64_t dt = globaltimer() - tile_t0;
+                atomicMax(&ctl[u].tile_ns, (int)(dt < 0x7fffffffull ? dt : 0x7fffffffull));
             }
             __syncthreads();
         }
