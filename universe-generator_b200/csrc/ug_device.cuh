@@ -82,7 +82,7 @@ struct UniDev {
     const int32_t* order;  // [T] endpoint-first
     // main grid
     int32_t grid_kind;
-    int32_t pad1;
+    int32_t rblock_shift;  // round hash: blocks of 2^rblock_shift cells per axis
     int32_t* heads;        // dense: chain heads [T * gw^dim]
     ulonglong2* hslot;     // hash [hcap]: x = key t<<40 | cell, y = head slot (low 32 bits)
     uint64_t hmask;        // hcap - 1

@@ -233,6 +233,24 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
     const int T = c.T;
     d.S_max = (int)std::min<int64_t>(kSmaxCap, std::max<int64_t>(256, (1 << 20) / T));
     if (c.dim == 1) d.S_max = 256;  // 1+1D in-round conflicts are found pairwise
+    // Round-hash block of 2^s cells per axis: a survivor timestep probes the blocks
+    // of its 3-cell window (2 per axis at s = 1, 1 + 2 / 2^s on average above) and
+    // walks their chains (2^(s dim) cells of at most S_max / gw^dim points each).
+    // The block minimising probes * (1 + 2 * expected chain points) is taken:
+    // sparse universes (large F) get large blocks, crowded ones 2 cells.
+    {
+        const double rho = (double)d.S_max / std::pow((double)d.gw, (double)c.dim);
+        double best = 1e300;
+        for (int sh = 1; sh <= 4; sh++) {
+            const double w = (double)(1 << sh);
+            const double probes = std::pow(sh == 1 ? 2.0 : 1.0 + 2.0 / w, (double)c.dim);
+            const double cost = probes * (1.0 + 2.0 * std::pow(w, (double)c.dim) * rho);
+            if (cost < best) {
+                best = cost;
+                d.rblock_shift = sh;
+            }
+        }
+    }
     if (c.surv_cap > 0) d.S_max = c.surv_cap;
     d.S_max = std::min(d.S_max, d.B_max);
     // tables

@@ -622,13 +622,13 @@ __global__ void __launch_bounds__(128) k_surv_gemm(const UniDev* __restrict__ U,
     }
 }
 
-// Round hash block of a cell: 2 cells per axis, so the 3 neighbour cells of a
-// point span at most 2 blocks per axis (3 at the seam of an odd gw).  Measured
-// on c3 against 4- and 8-cell blocks (fewer probes, longer chains): 108 ms
-// against 140 and 116 ms of k_conflicts per job.
-constexpr int kRBlockShift = 1;  // cells per round-hash block per axis: 1 << kRBlockShift
-static_assert(((2 * kMaxF) >> kRBlockShift) <= 1024, "k_conflicts packs block coordinates in 10 bits");
-__device__ __forceinline__ int rblock_gw(const UniDev& d) { return (d.gw + (1 << kRBlockShift) - 1) >> kRBlockShift; }
+// Round hash block of a cell: 2^rblock_shift cells per axis (host-chosen per
+// universe, at least 2), so the 3 neighbour cells of a point span at most 2
+// blocks per axis (3 only at the seam of a partial last block).
+static_assert(2 * kMaxF <= 1024, "k_conflicts packs block coordinates in 10 bits");
+__device__ __forceinline__ int rblock_gw(const UniDev& d) {
+    return (d.gw + (1 << d.rblock_shift) - 1) >> d.rblock_shift;
+}
 
 // k_surv_hash: one thread per survivor timestep inserts the point into the
 // round hash (key: epoch, t, block).
@@ -647,7 +647,7 @@ __global__ void __launch_bounds__(256) k_surv_hash(const UniDev* __restrict__ U,
 #pragma unroll
         for (int ax = 0; ax < 3; ax++) {
             if (ax < d.dim)
-                bc[ax] = cell_of(q->c[ax], d.cell, d.gw) >> kRBlockShift;
+                bc[ax] = cell_of(q->c[ax], d.cell, d.gw) >> d.rblock_shift;
             else
                 q->c[ax] = 0.0;
         }
@@ -931,7 +931,7 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
                 if (hit) add(r2);
             }
         } else {
-            const int gw = d.gw, gwb = rblock_gw(d);
+            const int gw = d.gw, gwb = rblock_gw(d), rbs = d.rblock_shift;
             for (int t = lane; t < T; t += 32) {
                 const Pt64 P = d.spos[UG_IDX((int64_t)r * T + t, (int64_t)d.S_max * T)];
                 // distinct round-hash blocks of the 3 neighbour cells per axis:
@@ -943,9 +943,9 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
                 for (int ax = 0; ax < 3; ax++) {
                     if (ax < d.dim) {
                         const int c0 = cell_of(P.c[ax], d.cell, gw);
-                        const uint32_t v0 = (uint32_t)((c0 == 0 ? gw - 1 : c0 - 1) >> kRBlockShift);
-                        const uint32_t v1 = (uint32_t)(c0 >> kRBlockShift);
-                        const uint32_t v2 = (uint32_t)((c0 == gw - 1 ? 0 : c0 + 1) >> kRBlockShift);
+                        const uint32_t v0 = (uint32_t)((c0 == 0 ? gw - 1 : c0 - 1) >> rbs);
+                        const uint32_t v1 = (uint32_t)(c0 >> rbs);
+                        const uint32_t v2 = (uint32_t)((c0 == gw - 1 ? 0 : c0 + 1) >> rbs);
                         uint32_t pk = v0;
                         int n = 1;
                         if (v1 != v0) pk |= v1 << (10 * n++);
