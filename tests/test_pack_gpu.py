@@ -185,7 +185,9 @@ def test_seam_blocks_when_cells_are_not_a_multiple_of_eight(ug, oracle, precisio
 
 @pytest.mark.parametrize("dim,T,excl,mode,prec,hashed", [(2, 16, 0, 0, 0, False), (2, 24, 1, 1, 1, False),
                                                          (3, 20, 1, 0, 1, True), (3, 32, 0, 2, 0, True),
-                                                         (1, 40, 1, 0, 1, False)])
+                                                         (1, 40, 1, 0, 1, False),
+                                                         # coarsened bitmaps: the hash keys coarse cells
+                                                         (3, 160, 1, 0, 1, True), (3, 200, 1, 1, 0, True)])
 def test_filled_cells_count(ug, dim, T, excl, mode, prec, hashed):
     """The device count of occupied (timestep, cell) buckets equals the count from the
     accepted trajectories (the `filled` of braid_cuda.cu:695, 865-879)."""

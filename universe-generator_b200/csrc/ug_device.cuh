@@ -106,7 +106,10 @@ struct UniDev {
     int32_t occ_nb;        // 2+1 and 3+1: bricks per axis
     int64_t occ1_per_t;
     int32_t occ1_shift;
-    int32_t pad_occ1;
+    // main hash keyed by coarse cells of 2^gkey_shift cells per axis (those of the
+    // occupancy bitmap; 0 = cells).  A coarse key's slot carries the complement of
+    // its cells' occupancy mask in the high half of y.
+    int32_t gkey_shift;
     double occ1_reach;
     // accepted points
     Pt64* pts;             // [slot_cap * T]
@@ -529,6 +532,44 @@ __device__ __forceinline__ int32_t grid_head(const UniDev& U, int t, int64_t lin
     return -1;
 }
 
+// Key of cell cc in the main grid and (coarse keys) the cell's bit in the slot's
+// occupancy mask (0 for cell keys).
+__device__ __forceinline__ int64_t grid_lin(const UniDev& U, const int* cc, uint32_t* fbit) {
+    const int s = U.gkey_shift;
+    if (s == 0) {
+        *fbit = 0u;
+        return lin_cell(cc, U.dim, U.gw);
+    }
+    int cs[3] = {0, 0, 0};
+    uint32_t fi = 0;
+#pragma unroll
+    for (int ax = 0; ax < 3; ax++)
+        if (ax < U.dim) {
+            cs[ax] = cc[ax] >> s;
+            fi = (fi << s) | (uint32_t)(cc[ax] & ((1 << s) - 1));
+        }
+    *fbit = 1u << fi;
+    return lin_cell(cs, U.dim, U.occ_gw);
+}
+
+// Coarse-keyed grid: head of the chain of coarse cell `lin` at t and the mask of
+// its occupied cells (0: no point).
+__device__ __forceinline__ int32_t grid_head_mask(const UniDev& U, int t, int64_t lin, uint32_t* mask) {
+    const uint64_t key = ((uint64_t)t << 40) | (uint64_t)lin;
+    uint64_t h = mix64(key) & U.hmask;
+    for (uint64_t probe = 0; probe <= U.hmask; probe++) {
+        const ulonglong2 s = __ldg(U.hslot + UG_IDX(h, U.hmask + 1));
+        if (s.x == key) {
+            *mask = ~(uint32_t)(s.y >> 32);
+            return (int32_t)(uint32_t)s.y;
+        }
+        if (s.x == kEmptyKey) break;
+        h = (h + 1) & U.hmask;
+    }
+    *mask = 0u;
+    return -1;
+}
+
 __device__ __forceinline__ int64_t cells_per_t(const UniDev& U) {
     int64_t n = 1;
 #pragma unroll
@@ -614,6 +655,28 @@ __device__ __forceinline__ bool brick_cell_visit(const UniDev& U, int t, const N
                                               int o1, int o2, Visit& visit) {
     const int sh = U.occ_shift, gw = U.gw, w = 1 << sh;
     const int f0e = min(gw, (o0 + 1) * w), f1e = min(gw, (o1 + 1) * w), f2e = min(gw, (o2 + 1) * w);
+    if (U.gkey_shift > 0) {  // one chain per coarse cell: walk it when a window cell is occupied
+        uint32_t wm = 0u;
+        for (int f0 = o0 * w; f0 < f0e; f0++) {
+            if (cyc_dist(f0, nb.v[0][0], gw) >= nb.n[0]) continue;
+            for (int f1 = o1 * w; f1 < f1e; f1++) {
+                if (cyc_dist(f1, nb.v[1][0], gw) >= nb.n[1]) continue;
+                for (int f2 = o2 * w; f2 < f2e; f2++)
+                    if (cyc_dist(f2, nb.v[2][0], gw) < nb.n[2])
+                        wm |= 1u << ((((f0 - o0 * w) << sh | (f1 - o1 * w)) << sh) | (f2 - o2 * w));
+            }
+        }
+        uint32_t occm;
+        const int oc[3] = {o0, o1, o2};
+        int32_t p = grid_head_mask(U, t, lin_cell(oc, 3, U.occ_gw), &occm);
+        if (!(occm & wm)) return false;
+        while (p >= 0) {
+            int32_t nx;
+            if (visit(p, nx)) return true;
+            p = nx;
+        }
+        return false;
+    }
     for (int f0 = o0 * w; f0 < f0e; f0++) {
         if (cyc_dist(f0, nb.v[0][0], gw) >= nb.n[0]) continue;
         for (int f1 = o1 * w; f1 < f1e; f1++) {
@@ -798,6 +861,24 @@ __device__ __forceinline__ bool brick_cell_visit2(const UniDev& U, int t, const 
                                                   int o1, Visit& visit) {
     const int sh = U.occ_shift, gw = U.gw, w = 1 << sh;
     const int f0e = min(gw, (o0 + 1) * w), f1e = min(gw, (o1 + 1) * w);
+    if (U.gkey_shift > 0) {  // one chain per coarse cell: walk it when a window cell is occupied
+        uint32_t wm = 0u;
+        for (int f0 = o0 * w; f0 < f0e; f0++) {
+            if (cyc_dist(f0, nb.v[0][0], gw) >= nb.n[0]) continue;
+            for (int f1 = o1 * w; f1 < f1e; f1++)
+                if (cyc_dist(f1, nb.v[1][0], gw) < nb.n[1]) wm |= 1u << ((f0 - o0 * w) << sh | (f1 - o1 * w));
+        }
+        uint32_t occm;
+        const int oc[2] = {o0, o1};
+        int32_t p = grid_head_mask(U, t, lin_cell(oc, 2, U.occ_gw), &occm);
+        if (!(occm & wm)) return false;
+        while (p >= 0) {
+            int32_t nx;
+            if (visit(p, nx)) return true;
+            p = nx;
+        }
+        return false;
+    }
     for (int f0 = o0 * w; f0 < f0e; f0++) {
         if (cyc_dist(f0, nb.v[0][0], gw) >= nb.n[0]) continue;
         for (int f1 = o1 * w; f1 < f1e; f1++) {
@@ -929,6 +1010,11 @@ __device__ __forceinline__ bool contacts64_d(const UniDev& U, int t, const doubl
         double Q[3];
 #pragma unroll
         for (int ax = 0; ax < D; ax++) Q[ax] = __ldg(&q->c[ax]);
+        if (U.gkey_shift > 0) {  // coarse chains: only the points of the 3^D window cells count
+#pragma unroll
+            for (int ax = 0; ax < D; ax++)
+                if (cyc_dist(cell_of(Q[ax], U.cell, U.gw), nb.v[ax][0], U.gw) >= nb.n[ax]) return false;
+        }
         if (!pair_hit64(U, P, Q)) return false;
         if (!group) return true;
         const int32_t gq = __ldg(&q->gid);

@@ -339,6 +339,10 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
         }
         h.occ_words = (bits + 31) / 32;
         d.occ_words = h.occ_words;
+        // A coarsened bitmap leaves several cells per occupied bit; the hash grid then
+        // keys the coarse cells too (one probe per occupied coarse cell instead of
+        // one per window cell in it), with the cells' occupancy mask in the slot.
+        d.gkey_shift = (d.grid_kind == GRID_HASH && c.dim >= 2 && sh * c.dim <= 5) ? sh : 0;
         if ((rc = dalloc(h, &d.occ, (size_t)h.occ_words, 0))) return rc;
         // the finest blocks within 16 MiB (2^27 bits): commits mark it at random and
         // every test reads it, so a small map that stays in L2 pays more than fine

@@ -743,8 +743,10 @@ __device__ __forceinline__ void group_sync() {
         __syncthreads();
 }
 
+// (a register cap instead of launch bounds: with launch bounds alone ptxas keeps
+// the WPI = 1 form at 64 registers and spills)
 template <int WPI>
-__global__ void __launch_bounds__(32 * kSurvWarps) k_confirm64w(const UniDev* __restrict__ U,
+__global__ void __maxnreg__(128) k_confirm64w(const UniDev* __restrict__ U,
                                                                   UniCtl* ctl, RoundInfo* info, int all) {
     static_assert(WPI == 1 || WPI == kSurvWarps, "a group is one warp or the whole block");
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1194,17 +1196,20 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
 // Appends slot to the chain of cell lin at timestep t; *old_head gets the
 // previous head.  *new_key is set when the insert claimed a new hash key (the
 // caller counts them into UniCtl::hash_used).
-__device__ __forceinline__ void grid_insert(const UniDev& d, UniCtl& c, int t, int64_t lin,
-                                            int64_t cpt, int32_t slot, int32_t* old_head, bool* new_key) {
+__device__ __forceinline__ void grid_insert(const UniDev& d, UniCtl& c, int t, int64_t lin, uint32_t fbit,
+                                            int64_t cpt, int32_t slot, int32_t* old_head, bool* new_key,
+                                            bool* new_cell) {
     if (d.grid_kind == GRID_DENSE) {
         *old_head = atomicExch(d.heads + UG_IDX((int64_t)t * cpt + lin, d.dense_cells), slot);
+        *new_cell = *old_head < 0;
         return;
     }
     const uint64_t key = ((uint64_t)t << 40) | (uint64_t)lin;
     uint64_t h = mix64(key) & d.hmask;
     for (uint64_t probe = 0; probe <= d.hmask; probe++) {
         unsigned long long* kp = &d.hslot[h].x;
-        uint64_t k = __ldcg(kp);
+        const ulonglong2 sv = __ldcg(&d.hslot[h]);  // key and y in one load
+        uint64_t k = sv.x;
         if (k == kEmptyKey) {
             const uint64_t prev = atomicCAS(kp, kEmptyKey, key);
             if (prev == kEmptyKey) {
@@ -1215,13 +1220,33 @@ __device__ __forceinline__ void grid_insert(const UniDev& d, UniCtl& c, int t, i
             }
         }
         if (k == key) {
-            *old_head = (int32_t)(uint32_t)atomicExch(&d.hslot[h].y, (unsigned long long)(uint32_t)slot);
-            return;
+            // y: chain head (low half), complemented cell mask of a coarse key (high half)
+            if (!fbit) {
+                *old_head = (int32_t)atomicExch(reinterpret_cast<unsigned int*>(&d.hslot[h].y), (unsigned int)slot);
+                *new_cell = *old_head < 0;
+                return;
+            }
+            // coarse key: the new head and the cell's bit in one compare-and-swap of y
+            // (a failed swap means another insert into this coarse cell went first)
+            unsigned long long* yp = &d.hslot[h].y;
+            unsigned long long cur = sv.y;
+            for (int it = 0; it < (1 << 20); it++) {
+                const unsigned long long nv = (((cur >> 32) & ~(unsigned long long)fbit) << 32) | (uint32_t)slot;
+                const unsigned long long prev = atomicCAS(yp, cur, nv);
+                if (prev == cur) {
+                    *old_head = (int32_t)(uint32_t)cur;
+                    *new_cell = ((cur >> 32) & fbit) != 0ull;
+                    return;
+                }
+                cur = prev;
+            }
+            break;
         }
         h = (h + 1) & d.hmask;
     }
     *old_head = -1;
-    c.err_code = 3;  // hash full (host keeps the load factor below 1/2)
+    *new_cell = false;
+    c.err_code = 3;  // hash full (host keeps the load factor below 1/2), or no progress
     c.state = ST_ERROR;
 }
 
@@ -1310,8 +1335,9 @@ __global__ void __launch_bounds__(256) k_commit(const UniDev* __restrict__ U, Un
                 for (int ax = 0; ax < 3; ax++)
                     if (ax < d.dim) cc[ax] = cell_of(q.c[ax], d.cell, d.gw);
                 int32_t old;
-                grid_insert(d, c, t, lin_cell(cc, d.dim, d.gw), cells_per_t(d), (int32_t)slot, &old, &new_key);
-                new_cell = old < 0;
+                uint32_t fbit;
+                const int64_t lin = grid_lin(d, cc, &fbit);
+                grid_insert(d, c, t, lin, fbit, cells_per_t(d), (int32_t)slot, &old, &new_key, &new_cell);
                 occ_set(d.occ, occ_bit(d, t, cc), d.occ_words);
                 occ1_mark(d, t, q.c);
                 q.next = old;
@@ -1357,8 +1383,10 @@ __global__ void k_rehash(const UniDev* __restrict__ U, UniCtl* ctl, int u, int64
         for (int ax = 0; ax < 3; ax++)
             if (ax < d.dim) cc[ax] = cell_of(q->c[ax], d.cell, d.gw);
         int32_t old;
-        bool new_key = false;
-        grid_insert(d, c, t, lin_cell(cc, d.dim, d.gw), cells_per_t(d), (int32_t)slot, &old, &new_key);
+        bool new_key = false, new_cell = false;
+        uint32_t fbit;
+        const int64_t lin = grid_lin(d, cc, &fbit);
+        grid_insert(d, c, t, lin, fbit, cells_per_t(d), (int32_t)slot, &old, &new_key, &new_cell);
         if (new_key) atomicAdd((unsigned long long*)&c.hash_used, 1ull);
         q->next = old;
         d.ptf[slot * d.T + t].next = old;
