@@ -138,6 +138,7 @@ __global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* inf
         info->total_surv = 0;
         info->compact_done = 0;
         info->tile_next = 0;
+        info->confl_next = 0;
     }
 }
 
@@ -225,6 +226,27 @@ __device__ __forceinline__ bool group_phase(const UniDev& d, const UniCtl& c) {
 
 // --------------------------------------------------------------- compact
 
+// Exclusive prefix of v over the 256 threads of the block; *total gets the sum.
+// Every thread of the block must call it (it synchronises the block).
+__device__ __forceinline__ int block_excl_scan256(int v, int* wsum, int* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int x = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += x;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    int wpre = 0, tot = 0;
+    for (int k = 0; k < 8; k++) {
+        if (k < warp) wpre += wsum[k];
+        tot += wsum[k];
+    }
+    __syncthreads();  // wsum is reused by the next call
+    *total = tot;
+    return wpre + incl - v;
+}
+
 __global__ void __launch_bounds__(256) k_compact(const UniDev* __restrict__ U, UniCtl* ctl,
                                                  RoundInfo* info) {
     __shared__ int32_t wsum[8];
@@ -277,24 +299,45 @@ __global__ void __launch_bounds__(256) k_compact(const UniDev* __restrict__ U, U
         s_last = atomicAdd(&info->compact_done, 1) == info->n_uni - 1;
     }
     __syncthreads();
-    if (s_last && tid == 0) {
+    if (s_last) {  // the last block: work offsets of every universe, as block scans
         __threadfence();
-        int acc = 0, sev = 0, spt = 0;
-        for (int v = 0; v < info->n_uni; v++) {
-            const int Sv = *(volatile int32_t*)&ctl[v].S;
-            info->surv_off[v] = acc;
-            info->sev_off[v] = sev;
-            info->spt_off[v] = spt;
-            acc += Sv;
-            sev += ((Sv * U[v].dim + 31) >> 5) * ((U[v].T + 31) >> 5);
-            spt += Sv * U[v].T;
+        const int n = info->n_uni;
+        int acc = 0, sev = 0, spt = 0, acc_o = 0;
+        for (int b0 = 0; b0 < n; b0 += 256) {
+            const int v = b0 + tid;
+            int Sv = 0, sevv = 0, sptv = 0, So = 0;
+            if (v < n) {
+                Sv = *(volatile int32_t*)&ctl[v].S;
+                sevv = ((Sv * U[v].dim + 31) >> 5) * ((U[v].T + 31) >> 5);
+                sptv = Sv * U[v].T;
+                // the same survivors, universes in tile order (costliest first)
+                So = *(volatile int32_t*)&ctl[info->tile_uni[v]].S;
+            }
+            int t1, t2, t3, t4;
+            const int p1 = block_excl_scan256(Sv, wsum, &t1);
+            const int p2 = block_excl_scan256(sevv, wsum, &t2);
+            const int p3 = block_excl_scan256(sptv, wsum, &t3);
+            const int p4 = block_excl_scan256(So, wsum, &t4);
+            if (v < n) {
+                info->surv_off[v] = acc + p1;
+                info->sev_off[v] = sev + p2;
+                info->spt_off[v] = spt + p3;
+                info->surv_off_o[v] = acc_o + p4;
+            }
+            acc += t1;
+            sev += t2;
+            spt += t3;
+            acc_o += t4;
         }
-        info->surv_off[info->n_uni] = acc;
-        info->sev_off[info->n_uni] = sev;
-        info->spt_off[info->n_uni] = spt;
-        info->total_surv = acc;
-        info->total_sev = sev;
-        info->total_spt = spt;
+        if (tid == 0) {
+            info->surv_off[n] = acc;
+            info->sev_off[n] = sev;
+            info->spt_off[n] = spt;
+            info->surv_off_o[n] = acc_o;
+            info->total_surv = acc;
+            info->total_sev = sev;
+            info->total_spt = spt;
+        }
     }
 }
 
@@ -715,16 +758,23 @@ __global__ void __launch_bounds__(256) k_gray_compact(const UniDev* __restrict__
         s_last = atomicAdd(&info->gray_done, 1) == info->n_uni - 1;
     }
     __syncthreads();
-    if (s_last && tid == 0) {
+    if (s_last) {  // the last block: offsets of every universe's undecided candidates
         __threadfence();
+        const int n = info->n_uni;
         int acc = 0;
-        for (int v = 0; v < info->n_uni; v++) {
-            info->gray_pref[v] = acc;
-            acc += *(volatile int32_t*)&ctl[v].n_gray;
+        for (int b0 = 0; b0 < n; b0 += 256) {
+            const int v = b0 + tid;
+            const int g = v < n ? *(volatile int32_t*)&ctl[v].n_gray : 0;
+            int tot;
+            const int p = block_excl_scan256(g, wsum, &tot);
+            if (v < n) info->gray_pref[v] = acc + p;
+            acc += tot;
         }
-        info->gray_pref[info->n_uni] = acc;
-        info->total_gray = acc;
-        info->gray_done = 0;
+        if (tid == 0) {
+            info->gray_pref[n] = acc;
+            info->total_gray = acc;
+            info->gray_done = 0;
+        }
     }
 }
 
@@ -890,12 +940,20 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
     __shared__ int32_t s_list[4][kConflictCap];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int n_uni = info->n_uni, total = info->total_surv;
-    const int gwarp = blockIdx.x * 4 + wib, nwarps = gridDim.x * 4;
     volatile int32_t* cnt = &s_cnt[wib];
     volatile int32_t* lst = s_list[wib];
-    for (int item = gwarp; item < total; item += nwarps) {
-        const int u = find_uni(info->surv_off, n_uni, item);
-        const int r = item - info->surv_off[u];
+    // Survivors are handed out one at a time, costliest universes first (their cost
+    // differs by the timesteps and dimension); the next one is claimed when an item
+    // starts so the atomic's latency hides behind the item.
+    int item = 0;
+    if (lane == 0) item = atomicAdd(&info->confl_next, 1);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    while (item < total) {
+        int next = 0;
+        if (lane == 0) next = atomicAdd(&info->confl_next, 1);
+        const int pos = find_uni(info->surv_off_o, n_uni, item);
+        const int u = info->tile_uni[pos];
+        const int r = item - info->surv_off_o[pos];
         const UniDev& d = U[u];
         UniCtl& c = ctl[u];
         const int T = d.T;
@@ -980,6 +1038,7 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
         for (int i = lane; i < ns; i += 32) d.clist[UG_IDX((int64_t)r * kConflictCap + i, (int64_t)d.S_max * kConflictCap)] = lst[i];
         if (lane == 0) d.ccount[UG_IDX(r, d.S_max)] = n;
         __syncwarp();
+        item = __shfl_sync(0xffffffffu, next, 0);
     }
 }
 

@@ -19,12 +19,13 @@ struct RoundInfo {
     int32_t total_gray;
     int32_t gray_done;
     int32_t tile_next;     // mixed prefilter: tiles handed out beyond the first gridDim.x
-    int32_t pad_ti;
+    int32_t confl_next;    // k_conflicts: survivors handed out so far
     int32_t total_sev;     // k_surv_gemm warp tiles (32 rows x 32 timesteps)
     int32_t total_spt;     // survivor timesteps (k_surv_hash / k_commit items)
     int32_t tile_off[kMaxUni + 1];   // prefilter tiles: first tile of the i-th universe in tile order
     int32_t tile_uni[kMaxUni];       // the universe at position i of the tile order
     int32_t surv_off[kMaxUni + 1];
+    int32_t surv_off_o[kMaxUni + 1];  // survivor offsets of the universes in tile order
     int32_t gray_pref[kMaxUni + 1];
     int32_t sev_off[kMaxUni + 1];
     int32_t spt_off[kMaxUni + 1];
