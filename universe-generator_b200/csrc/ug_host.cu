@@ -1115,7 +1115,9 @@ int ug_batch_restore(void* h, int32_t u, int64_t n, const int64_t* idx, const in
             const bool past = v > u;
             ri->surv_off[v] = past ? m : 0;
             ri->sev_off[v] = past ? sev : 0;
+            ri->sev_off_o[v] = past ? sev : 0;
             ri->spt_off[v] = past ? m * T : 0;
+            if (v < B->n) ri->tile_uni[v] = v;  // tile order = universe order here
         }
         ri->total_surv = m;
         ri->total_sev = sev;

@@ -43,6 +43,27 @@ __device__ __forceinline__ bool win_close(int64_t q, int64_t& nb, int64_t& sum, 
     return nb >= 32 && in_phase > 1000000 && (double)sum / (double)(32 * q) < thr;
 }
 
+// Exclusive prefix of v over the 256 threads of the block; *total gets the sum.
+// Every thread of the block must call it (it synchronises the block).
+__device__ __forceinline__ int block_excl_scan256(int v, int* wsum, int* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int x = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += x;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    int wpre = 0, tot = 0;
+    for (int k = 0; k < 8; k++) {
+        if (k < warp) wpre += wsum[k];
+        tot += wsum[k];
+    }
+    __syncthreads();  // wsum is reused by the next call
+    *total = tot;
+    return wpre + incl - v;
+}
+
 __global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info) {
     __shared__ int32_t ntiles[kMaxUni];
     __shared__ int32_t cost[kMaxUni];
@@ -123,22 +144,28 @@ __global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* inf
         order[rank] = u;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        int acc = 0, act = 0;
-        for (int i = 0; i < n; i++) {
-            const int u = order[i];
-            info->tile_off[i] = acc;
-            info->tile_uni[i] = u;
-            acc += ntiles[u];
-            act |= ntiles[u] > 0;
+    __shared__ int32_t wsum[8];
+    int acc = 0;
+    for (int b0 = 0; b0 < n; b0 += 256) {  // k_plan runs as one block of 256 threads
+        const int i = b0 + threadIdx.x;
+        const int nt = i < n ? ntiles[order[i]] : 0;
+        int tot;
+        const int p = block_excl_scan256(nt, wsum, &tot);
+        if (i < n) {
+            info->tile_off[i] = acc + p;
+            info->tile_uni[i] = order[i];
         }
+        acc += tot;
+    }
+    if (threadIdx.x == 0) {
         info->tile_off[n] = acc;
         info->total_tiles = acc;
-        info->any_active = act;
+        info->any_active = acc > 0;
         info->total_surv = 0;
         info->compact_done = 0;
         info->tile_next = 0;
         info->confl_next = 0;
+        info->gemm_next = 0;
     }
 }
 
@@ -226,26 +253,6 @@ __device__ __forceinline__ bool group_phase(const UniDev& d, const UniCtl& c) {
 
 // --------------------------------------------------------------- compact
 
-// Exclusive prefix of v over the 256 threads of the block; *total gets the sum.
-// Every thread of the block must call it (it synchronises the block).
-__device__ __forceinline__ int block_excl_scan256(int v, int* wsum, int* total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int incl = v;
-    for (int o = 1; o < 32; o <<= 1) {
-        const int x = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += x;
-    }
-    if (lane == 31) wsum[warp] = incl;
-    __syncthreads();
-    int wpre = 0, tot = 0;
-    for (int k = 0; k < 8; k++) {
-        if (k < warp) wpre += wsum[k];
-        tot += wsum[k];
-    }
-    __syncthreads();  // wsum is reused by the next call
-    *total = tot;
-    return wpre + incl - v;
-}
 
 __global__ void __launch_bounds__(256) k_compact(const UniDev* __restrict__ U, UniCtl* ctl,
                                                  RoundInfo* info) {
@@ -302,38 +309,44 @@ __global__ void __launch_bounds__(256) k_compact(const UniDev* __restrict__ U, U
     if (s_last) {  // the last block: work offsets of every universe, as block scans
         __threadfence();
         const int n = info->n_uni;
-        int acc = 0, sev = 0, spt = 0, acc_o = 0;
+        int acc = 0, sev = 0, spt = 0, acc_o = 0, sev_o = 0;
         for (int b0 = 0; b0 < n; b0 += 256) {
             const int v = b0 + tid;
-            int Sv = 0, sevv = 0, sptv = 0, So = 0;
+            int Sv = 0, sevv = 0, sptv = 0, So = 0, sevo = 0;
             if (v < n) {
                 Sv = *(volatile int32_t*)&ctl[v].S;
                 sevv = ((Sv * U[v].dim + 31) >> 5) * ((U[v].T + 31) >> 5);
                 sptv = Sv * U[v].T;
-                // the same survivors, universes in tile order (costliest first)
-                So = *(volatile int32_t*)&ctl[info->tile_uni[v]].S;
+                // the same survivors and product tiles, universes in tile order (costliest first)
+                const int uo = info->tile_uni[v];
+                So = *(volatile int32_t*)&ctl[uo].S;
+                sevo = ((So * U[uo].dim + 31) >> 5) * ((U[uo].T + 31) >> 5);
             }
-            int t1, t2, t3, t4;
+            int t1, t2, t3, t4, t5;
             const int p1 = block_excl_scan256(Sv, wsum, &t1);
             const int p2 = block_excl_scan256(sevv, wsum, &t2);
             const int p3 = block_excl_scan256(sptv, wsum, &t3);
             const int p4 = block_excl_scan256(So, wsum, &t4);
+            const int p5 = block_excl_scan256(sevo, wsum, &t5);
             if (v < n) {
                 info->surv_off[v] = acc + p1;
                 info->sev_off[v] = sev + p2;
                 info->spt_off[v] = spt + p3;
                 info->surv_off_o[v] = acc_o + p4;
+                info->sev_off_o[v] = sev_o + p5;
             }
             acc += t1;
             sev += t2;
             spt += t3;
             acc_o += t4;
+            sev_o += t5;
         }
         if (tid == 0) {
             info->surv_off[n] = acc;
             info->sev_off[n] = sev;
             info->spt_off[n] = spt;
             info->surv_off_o[n] = acc_o;
+            info->sev_off_o[n] = sev_o;
             info->total_surv = acc;
             info->total_sev = sev;
             info->total_spt = spt;
@@ -581,13 +594,18 @@ __global__ void __launch_bounds__(128) k_surv_gemm(const UniDev* __restrict__ U,
     extern __shared__ __align__(16) double gemm_smem[];  // [warp][stage][A | B][kGemmKC][32]
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     double* wsm = gemm_smem + (size_t)wib * (2 * 2 * kGemmKC * 32);
-    const int gwarp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
     const int n_uni = info->n_uni, total = info->total_sev;
     const int rg = lane >> 2, tg = lane & 3;
-    for (int item = gwarp; item < total; item += nwarps) {
-        const int u = find_uni(info->sev_off, n_uni, item);
-        const int local = item - info->sev_off[u];
+    // tiles handed out one at a time, costliest universes first (a tile's cost is
+    // its universe's term count K, 24 to 384); the next claimed when one starts
+    int item = 0, next = 0;
+    if (lane == 0) item = atomicAdd(&info->gemm_next, 1);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    for (; item < total; item = __shfl_sync(0xffffffffu, next, 0)) {
+        if (lane == 0) next = atomicAdd(&info->gemm_next, 1);
+        const int pos = find_uni(info->sev_off_o, n_uni, item);
+        const int u = info->tile_uni[pos];
+        const int local = item - info->sev_off_o[pos];
         const UniDev& d = U[u];
         const int T = d.T, dim = d.dim, K = d.K, R = d.Rpad, TP = d.Tpad;
         const int ntb = (T + 31) >> 5;

@@ -15,7 +15,8 @@ struct RoundInfo {
     int32_t compact_done;
     int32_t any_active;
     int32_t mixed_ok;      // universes in the mixed prefilter this round
-    int32_t pad[2];
+    int32_t gemm_next;     // k_surv_gemm: product tiles handed out so far
+    int32_t pad1;
     int32_t total_gray;
     int32_t gray_done;
     int32_t tile_next;     // mixed prefilter: tiles handed out beyond the first gridDim.x
@@ -28,6 +29,7 @@ struct RoundInfo {
     int32_t surv_off_o[kMaxUni + 1];  // survivor offsets of the universes in tile order
     int32_t gray_pref[kMaxUni + 1];
     int32_t sev_off[kMaxUni + 1];
+    int32_t sev_off_o[kMaxUni + 1];   // product tile offsets of the universes in tile order
     int32_t spt_off[kMaxUni + 1];
 };
 
