@@ -45,11 +45,14 @@ import numpy as np  # noqa: E402
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 MIXED_SRC = os.path.join(PKG, "csrc", "ug_mixed.cu")
-# DRAM bytes (read + write) per prefilter launch, averaged over the launches of one
-# complete job of the workload, from a 1-pass ncu capture of that job.  Keyed by the
-# SHA-256 of the prefilter source the capture ran, so a changed kernel reports null
-# instead of a stale figure.
-PREFILTER_TRAFFIC: dict[tuple[str, str, str], float] = {}
+# DRAM bytes (read + write) of the prefilter over one complete job of the workload,
+# from a 1-pass ncu capture of that job (dram__bytes_read.sum + dram__bytes_write.sum
+# summed over its launches); the line reports it per launch (÷ the timed job's launch
+# count).  Keyed by the SHA-256 of the prefilter source the capture ran, so a changed
+# kernel reports null instead of a stale figure.
+PREFILTER_TRAFFIC: dict[tuple[str, str, str], float] = {
+    ("c3", "mixed", "7dce91ac1985d3ac"): 65.933716e9 + 2.547354e9,
+}
 FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
 # reference-path cost model for picking affordable sample jobs: seconds ~ cap d T^2 / rate
 REF_COST_RATE = 1.8e8
@@ -339,6 +342,8 @@ def main() -> int:
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the FP64 single-universe sweep, the precision report and the "
                          "reference GPU engines (timing of the workload only)")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the reference's own GPU engines (informational field)")
     ap.add_argument("--clocks-dir", default="",
                     help="where the nvidia-smi samples of the timed region go (default: the temp dir)")
     ap.add_argument("--profile-case", action="store_true",
@@ -491,7 +496,8 @@ def main() -> int:
     P, src = peaks()
     pk_s = pk_ms / 1000.0
     avg_s = pk_s / max(pk_n, 1)
-    traffic = PREFILTER_TRAFFIC.get((args.workload, args.precision, src_sha()))
+    job_traffic = PREFILTER_TRAFFIC.get((args.workload, args.precision, src_sha()))
+    traffic = job_traffic / max(pk_n, 1) if job_traffic else None
     # algorithmic units of the prefilter (per launch = job total / launches):
     #  tensor: the contraction 2 d K T per candidate (K = (F-1) + F/2; split-BF16 counted once;
     #          the mixed path evaluates all T timesteps of every candidate)
@@ -570,7 +576,7 @@ def main() -> int:
             same_seeds = [dataclasses.replace(t, seed=u.seed) for t, u in zip(tuned, us)]
             cb["matched_gpu"] = matched_gpu(ugb200, same_seeds, cb["universes"], prec, local, stream)
             line["cpu_baseline"] = cb
-        if not args.no_extras:
+        if not args.no_extras and not args.no_reference_gpu:
             line["reference_gpu"] = reference_gpu(args)
         print(json.dumps(line))
     if dist:
