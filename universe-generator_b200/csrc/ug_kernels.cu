@@ -1154,34 +1154,54 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
             break;
         }
     }
+    // Group rounds, one survivor at a time.  The per-survivor data comes in ahead of its
+    // step: contact counts and pre-round groups of 32 survivors at once (lane i holds
+    // survivor r0 + i), and the next survivor's list while this one is decided.
+    int w_cnt = 0;
+    int32_t w_g0 = -1, nx0 = -1, nx1 = -1;
+    auto load_window = [&](int rb) {
+        const int rr = rb + lane;
+        w_cnt = 0;
+        w_g0 = -1;
+        if (rr < S_eff) {
+            w_cnt = d.ccount[UG_IDX(rr, d.S_max)];
+            w_g0 = d.g0[UG_IDX(d.surv_off[UG_IDX(rr, d.S_max + 1)], d.B_max)];
+        }
+    };
+    auto load_list = [&](int rr, int nn) {
+        const int32_t* l = d.clist + UG_IDX((int64_t)rr * kConflictCap, (int64_t)d.S_max * kConflictCap);
+        nx0 = lane < nn ? l[lane] : -1;
+        nx1 = lane + 32 < nn ? l[lane + 32] : -1;
+    };
+    if (group && S_eff > 0) {
+        load_window(0);
+        load_list(0, min(__shfl_sync(0xffffffffu, w_cnt, 0), kConflictCap));
+    }
     for (int r = 0; group && r < S_eff; r++) {
         if (k >= room) {
             stop_at = r;
             grow = true;
             break;
         }
-        const int n_all = d.ccount[UG_IDX(r, d.S_max)];
+        const int n_all = __shfl_sync(0xffffffffu, w_cnt, r & 31);
+        const int32_t g0 = __shfl_sync(0xffffffffu, w_g0, r & 31);
         const bool over = n_all > kConflictCap;  // the list holds only kConflictCap contacts
         const int n = over ? kConflictCap : n_all;
-        const int32_t* lst = d.clist + UG_IDX((int64_t)r * kConflictCap, (int64_t)d.S_max * kConflictCap);
+        const int32_t e0 = nx0, e1 = nx1;  // this survivor's list entries lane, lane + 32
+        if (r + 1 < S_eff) {
+            if (((r + 1) & 31) == 0) load_window(r + 1);
+            load_list(r + 1, min(__shfl_sync(0xffffffffu, w_cnt, (r + 1) & 31), kConflictCap));
+        }
         bool accept;
         int32_t gid;
-        if (!group) {
-            bool any = false;
-            for (int i = lane; i < n; i += 32) any |= acc_s[UG_IDX(lst[i], kSmaxCap)] >= 0;
-            accept = !__any_sync(0xffffffffu, any);
-            if (accept && over) {  // an unlisted contact might be admitted: decide next round
-                stop_at = r;
-                undecided = true;
-                break;
-            }
-            gid = (int32_t)(c.n_slots + k);
-        } else {
-            // union of the pre-round group and the groups of admitted earlier survivors
-            int32_t mine = -1;
-            bool two = false;
-            for (int i = lane; i < n; i += 32) {
-                const int r2 = (int)UG_IDX(lst[i], kSmaxCap);
+        // union of the pre-round group and the groups of admitted earlier survivors
+        int32_t mine = -1;
+        bool two = false;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int32_t e = h ? e1 : e0;
+            if (lane + 32 * h < n) {
+                const int r2 = (int)UG_IDX(e, kSmaxCap);
                 if (acc_s[r2] >= 0) {
                     const int32_t g2 = gid_s[r2];
                     if (mine == -1)
@@ -1190,29 +1210,27 @@ __global__ void __launch_bounds__(32) k_greedy(const UniDev* __restrict__ U, Uni
                         two = true;
                 }
             }
-            const int32_t g0 = d.g0[d.surv_off[r]];
-            int32_t first = g0;
-            for (int o = 0; o < 32; o++) {
-                const int32_t v = __shfl_sync(0xffffffffu, mine, o);
-                if (first == -1) first = v;
-            }
-            two = two || (mine != -1 && mine != first);
-            two = __any_sync(0xffffffffu, two);
-            if (!two && over) {  // unlisted contacts might add a group: decide next round
-                stop_at = r;
-                undecided = true;
-                break;
-            }
-            if (two) {
-                accept = false;
-                gid = -1;
-            } else if (first == -1) {
-                accept = unique_group;  // touches nothing: founds a group, or (subpath) rejected
-                gid = (int32_t)(c.n_slots + k);
-            } else {
-                accept = true;
-                gid = first;
-            }
+        }
+        // the first group in list order: the pre-round one, else the lowest lane's
+        const uint32_t hasg = __ballot_sync(0xffffffffu, mine != -1);
+        int32_t first = g0;  // g0 and hasg are the same in every lane
+        if (first == -1 && hasg) first = __shfl_sync(0xffffffffu, mine, __ffs(hasg) - 1);
+        two = two || (mine != -1 && mine != first);
+        two = __any_sync(0xffffffffu, two);
+        if (!two && over) {  // unlisted contacts might add a group: decide next round
+            stop_at = r;
+            undecided = true;
+            break;
+        }
+        if (two) {
+            accept = false;
+            gid = -1;
+        } else if (first == -1) {
+            accept = unique_group;  // touches nothing: founds a group, or (subpath) rejected
+            gid = (int32_t)(c.n_slots + k);
+        } else {
+            accept = true;
+            gid = first;
         }
         if (lane == 0) {
             acc_s[UG_IDX(r, kSmaxCap)] = accept ? k : -1;
