@@ -377,7 +377,10 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
         (rc = dalloc(h, &d.clist, (size_t)Sm * kConflictCap, 0)) ||
         (rc = dalloc(h, &d.sgid, Sm, 0xff)) || (rc = dalloc(h, &d.acc_rank, Sm, 0xff)))
         return rc;
-    const int64_t rcap = pow2_at_least(2LL * Sm * T);
+    // Round hash at a load of at most 1/8..1/4 (a round puts at most S_max * T keys in
+    // it): most lookups miss, and a miss walks the probe run.  c3: k_surv_hash 31.7 ->
+    // 26.1 ms and k_conflicts 49.0 -> 45.0 ms against 1/4..1/2; 1/2..1 was 134 ms slower.
+    const int64_t rcap = pow2_at_least(4LL * Sm * T);
     if ((rc = dalloc(h, &d.rslot, rcap, 0xff))) return rc;
     d.rmask = (uint64_t)(rcap - 1);
     return UG_OK;

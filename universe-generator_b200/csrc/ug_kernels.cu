@@ -378,7 +378,7 @@ __device__ __forceinline__ uint64_t rhash_claim(const UniDev& d, uint64_t key) {
         if (k == key) return h;
         h = (h + 1) & mask;
     }
-    return ~0ull;  // table full: cannot happen with rcap >= 2 * S_max * T
+    return ~0ull;  // table full: cannot happen with rcap >= 4 * S_max * T
 }
 
 // Head survivor of the chain of `key` (after k_surv_hash: key and value are read
