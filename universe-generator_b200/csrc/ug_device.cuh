@@ -122,9 +122,9 @@ struct UniDev {
     int32_t* surv_off;     // [S_max]  candidate offset within the round
     int32_t* gray_off;     // [B_max]  mixed: offsets of candidates sent to the FP64 retest
     Pt64* spos;            // [S_max * T]
-    ulonglong2* rslot;     // round hash [rcap]: x = key epoch<<40 | t<<31 | block,
-                           // y = epoch<<32 | head survivor rank (one 16-byte sector part)
-    uint64_t rmask;
+    uint64_t* rhead;       // round table [T * rblocks]: epoch<<32 | head survivor rank of
+                           // each (timestep, block); entries of other epochs are empty
+    int64_t rblocks;       // blocks per timestep (rblock_gw^dim)
     int32_t* ccount;       // [S_max]
     int32_t* clist;        // [S_max * kConflictCap]
     int32_t* sgid;         // [S_max]  resolved group / -1 rejected, -2 unresolved

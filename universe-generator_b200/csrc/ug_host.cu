@@ -377,12 +377,15 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
         (rc = dalloc(h, &d.clist, (size_t)Sm * kConflictCap, 0)) ||
         (rc = dalloc(h, &d.sgid, Sm, 0xff)) || (rc = dalloc(h, &d.acc_rank, Sm, 0xff)))
         return rc;
-    // Round hash at a load of at most 1/8..1/4 (a round puts at most S_max * T keys in
-    // it): most lookups miss, and a miss walks the probe run.  c3: k_surv_hash 31.7 ->
-    // 26.1 ms and k_conflicts 49.0 -> 45.0 ms against 1/4..1/2; 1/2..1 was 134 ms slower.
-    const int64_t rcap = pow2_at_least(4LL * Sm * T);
-    if ((rc = dalloc(h, &d.rslot, rcap, 0xff))) return rc;
-    d.rmask = (uint64_t)(rcap - 1);
+    // Round table: one 8-byte head per (timestep, block), at most 2^25 entries (the
+    // block grows past the cost model's choice if needed).
+    for (;; d.rblock_shift++) {
+        const int64_t g = (d.gw + (1 << d.rblock_shift) - 1) >> d.rblock_shift;
+        d.rblocks = 1;
+        for (int ax = 0; ax < c.dim; ax++) d.rblocks *= g;
+        if ((int64_t)T * d.rblocks <= ((int64_t)1 << 25) || d.rblock_shift >= 6) break;
+    }
+    if ((rc = dalloc(h, &d.rhead, (size_t)T * d.rblocks, 0xff))) return rc;
     return UG_OK;
 }
 
@@ -1082,7 +1085,7 @@ int ug_batch_restore(void* h, int32_t u, int64_t n, const int64_t* idx, const in
     }
     CKR(cudaMemsetAsync(d.occ, 0, (size_t)U.occ_words * sizeof(uint32_t), B->st));
     CKR(cudaMemsetAsync(d.occ1, 0, (size_t)U.occ1_words * sizeof(uint32_t), B->st));
-    CKR(cudaMemsetAsync(d.rslot, 0xff, (size_t)(d.rmask + 1) * sizeof(ulonglong2), B->st));
+    CKR(cudaMemsetAsync(d.rhead, 0xff, (size_t)T * d.rblocks * sizeof(uint64_t), B->st));
     // room for the admissions and the next rounds
     if (n + (int64_t)d.S_max * 2 > d.slot_cap) {
         CKR(cudaStreamSynchronize(B->st));

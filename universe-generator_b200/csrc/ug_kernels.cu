@@ -356,44 +356,17 @@ __global__ void __launch_bounds__(256) k_compact(const UniDev* __restrict__ U, U
 
 // ------------------------------------------------------------ survivors
 
-__device__ __forceinline__ uint64_t rkey_of(int epoch, int t, int64_t lin) {
-    return ((uint64_t)(epoch & 0xFFFFFF) << 40) | ((uint64_t)t << 31) | (uint64_t)lin;
+// Round table entry of (timestep t, block lin): one 8-byte word per (t, block),
+// epoch in the high half so no table is ever cleared.  A direct table replaced an
+// open-addressing hash keyed by (epoch, t, block): one exchange per insert instead of
+// a probe, a compare-and-swap and an exchange, and a quarter of the memory.
+__device__ __forceinline__ uint64_t* rentry(const UniDev& d, int t, int64_t lin) {
+    return d.rhead + UG_IDX((int64_t)t * d.rblocks + lin, (int64_t)d.T * d.rblocks);
 }
-
-// Home slot of a round-hash key.
-__device__ __forceinline__ uint64_t rhash_home(const UniDev& d, uint64_t key) { return mix64(key) & d.rmask; }
-
-// Round hash slot holding `key` (claiming an empty or stale slot).
-__device__ __forceinline__ uint64_t rhash_claim(const UniDev& d, uint64_t key) {
-    const uint64_t ep = key >> 40, mask = d.rmask;
-    uint64_t h = rhash_home(d, key);
-    for (uint64_t probe = 0; probe <= mask; probe++) {
-        unsigned long long* kp = &d.rslot[h].x;
-        uint64_t k = __ldcg(kp);
-        while (k != key && (k == kEmptyKey || (k >> 40) != ep)) {
-            const uint64_t prev = atomicCAS(kp, k, key);
-            if (prev == k) return h;
-            k = prev;
-        }
-        if (k == key) return h;
-        h = (h + 1) & mask;
-    }
-    return ~0ull;  // table full: cannot happen with rcap >= 4 * S_max * T
-}
-
-// Head survivor of the chain of `key` (after k_surv_hash: key and value are read
-// together in one 16-byte load).  Measured on c3 against separate key and value
-// arrays: k_surv_hash 48 -> 33 ms and k_conflicts 104 -> 96 ms per job.
-__device__ __forceinline__ int32_t rhash_head(const UniDev& d, uint64_t key) {
-    const uint64_t ep = key >> 40, mask = d.rmask;
-    uint64_t h = rhash_home(d, key);
-    for (uint64_t probe = 0; probe <= mask; probe++) {
-        const ulonglong2 s = __ldcg(d.rslot + h);
-        if (s.x == key) return (s.y >> 32) == (ep & 0xFFFFFF) ? (int32_t)(uint32_t)s.y : -1;
-        if (s.x == kEmptyKey || (s.x >> 40) != ep) return -1;
-        h = (h + 1) & mask;
-    }
-    return -1;
+// Head survivor of the chain of (t, block) this round (-1 none).
+__device__ __forceinline__ int32_t rtab_head(const UniDev& d, int epoch, int t, int64_t lin) {
+    const uint64_t v = __ldcg(rentry(d, t, lin));
+    return (v >> 32) == (uint64_t)(uint32_t)epoch ? (int32_t)(uint32_t)v : -1;
 }
 
 // Warp-cooperative FP64 regeneration of axis ax of candidate idx (Philox
@@ -712,15 +685,10 @@ __global__ void __launch_bounds__(256) k_surv_hash(const UniDev* __restrict__ U,
             else
                 q->c[ax] = 0.0;
         }
-        const uint64_t key = rkey_of(c.epoch, t, lin_cell(bc, d.dim, rblock_gw(d)));
-        const uint64_t h = rhash_claim(d, key);
-        int32_t nxt = -1;
-        if (h != ~0ull) {
-            const uint64_t old = atomicExch(&d.rslot[h].y,
-                                            ((uint64_t)(c.epoch & 0xFFFFFF) << 32) | (uint32_t)r);
-            if ((old >> 32) == (uint64_t)(c.epoch & 0xFFFFFF)) nxt = (int32_t)(uint32_t)old;
-        }
-        q->next = nxt;
+        const uint64_t ep = (uint64_t)(uint32_t)c.epoch;
+        const uint64_t old = atomicExch((unsigned long long*)rentry(d, t, lin_cell(bc, d.dim, rblock_gw(d))),
+                                        (unsigned long long)((ep << 32) | (uint32_t)r));
+        q->next = (old >> 32) == ep ? (int32_t)(uint32_t)old : -1;
         q->gid = -1;
     }
 }
@@ -1038,7 +1006,7 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
                             const int bc[3] = {(int)((bl[0] >> (10 * i0)) & 1023u),
                                                (int)((bl[1] >> (10 * i1)) & 1023u),
                                                (int)((bl[2] >> (10 * i2)) & 1023u)};
-                            int32_t r2 = rhash_head(d, rkey_of(c.epoch, t, lin_cell(bc, d.dim, gwb)));
+                            int32_t r2 = rtab_head(d, c.epoch, t, lin_cell(bc, d.dim, gwb));
                             while (r2 >= 0) {
                                 const Pt64* Q = d.spos + UG_IDX((int64_t)r2 * T + t, (int64_t)d.S_max * T);
                                 if (r2 < r && pair_hit64(d, P.c, Q->c)) add(r2);
