@@ -233,18 +233,20 @@ static int setup_universe(Batch& B, UniHost& h, int64_t dense_budget, int64_t* d
     const int T = c.T;
     d.S_max = (int)std::min<int64_t>(kSmaxCap, std::max<int64_t>(256, (1 << 20) / T));
     if (c.dim == 1) d.S_max = 256;  // 1+1D in-round conflicts are found pairwise
-    // Round-hash block of 2^s cells per axis: a survivor timestep probes the blocks
+    // Round-table block of 2^s cells per axis: a survivor timestep probes the blocks
     // of its 3-cell window (2 per axis at s = 1, 1 + 2 / 2^s on average above) and
     // walks their chains (2^(s dim) cells of at most S_max / gw^dim points each).
-    // The block minimising probes * (1 + 2 * expected chain points) is taken:
-    // sparse universes (large F) get large blocks, crowded ones 2 cells.
+    // The block minimising probes * (1 + expected chain points) is taken: sparse
+    // universes (large F) get large blocks, crowded ones 2 cells (c3 with the direct
+    // table: 366.0 ms of kernels against 369.5 / 370.3 ms with chain points weighted
+    // 2 / 4).
     {
         const double rho = (double)d.S_max / std::pow((double)d.gw, (double)c.dim);
         double best = 1e300;
         for (int sh = 1; sh <= 4; sh++) {
             const double w = (double)(1 << sh);
             const double probes = std::pow(sh == 1 ? 2.0 : 1.0 + 2.0 / w, (double)c.dim);
-            const double cost = probes * (1.0 + 2.0 * std::pow(w, (double)c.dim) * rho);
+            const double cost = probes * (1.0 + std::pow(w, (double)c.dim) * rho);
             if (cost < best) {
                 best = cost;
                 d.rblock_shift = sh;
