@@ -49,3 +49,37 @@ def test_tuned_plan_keeps_accepted_sets(ug, tmp_path):
                 pk.run()
                 ref = [a for a, _ in pk.accepted_all()]
         assert all(np.array_equal(a, b) for a, b in zip(got, ref))
+
+
+def test_tuned_plan_must_beat_retimed_defaults(tmp_path, monkeypatch):
+    """A slow first timing of the defaults (process start) must not make an equal plan
+    look better: the defaults are timed again before a changed plan is kept."""
+    from ugb200 import Universe
+    from ugb200 import autotune as A
+
+    monkeypatch.setattr(A, "device_key", lambda device=-1: "fake GPU x148SM")
+    us = [Universe(dim=2, T=16, seed=1, attempts=1000), Universe(dim=3, T=64, seed=2, attempts=1000)]
+    calls = []
+
+    def flat(us_, plan, *a):  # every plan takes 4.0 s except the very first timing
+        calls.append(plan)
+        return 9.5 if len(calls) == 1 else 4.0
+
+    out = A.tune(us, cache=str(tmp_path / "a.json"), timer=flat, budget_s=1e9)
+    assert all(c["round_size"] == A.DEFAULT["round_size"] and c["surv_scale"] == A.DEFAULT["surv_scale"]
+               for c in out["classes"].values())
+    assert out["rounds_per_sync"] == A.DEFAULT["rounds_per_sync"]
+    assert out["job_s"] == out["default_job_s"] == 4.0
+
+    calls.clear()
+
+    def faster_sync(us_, plan, *a):  # a real gain survives the re-timing
+        calls.append(plan)
+        if len(calls) == 1:
+            return 9.5
+        return 3.0 if plan["rounds_per_sync"] == 16 else 4.0
+
+    out = A.tune(us, cache=str(tmp_path / "b.json"), timer=faster_sync, budget_s=1e9)
+    assert out["rounds_per_sync"] == 16 and out["job_s"] == 3.0 and out["default_job_s"] == 4.0
+    assert all(c["round_size"] == A.DEFAULT["round_size"] and c["surv_scale"] == A.DEFAULT["surv_scale"]
+               for c in out["classes"].values())
