@@ -82,7 +82,7 @@ struct UniDev {
     const int32_t* order;  // [T] endpoint-first
     // main grid
     int32_t grid_kind;
-    int32_t rblock_shift;  // round hash: blocks of 2^rblock_shift cells per axis
+    int32_t rblock_shift;  // round table: blocks of 2^rblock_shift cells per axis
     int32_t* heads;        // dense: chain heads [T * gw^dim]
     ulonglong2* hslot;     // hash [hcap]: x = key t<<40 | cell, y = head slot (low 32 bits)
     uint64_t hmask;        // hcap - 1
@@ -171,7 +171,7 @@ struct UniCtl {
     int32_t trunc;         // survivor rank where the round was truncated (S if none)
     int32_t phase;         // 1 or 2
     int32_t state;         // ST_*
-    int32_t epoch;         // round-hash epoch
+    int32_t epoch;         // round-table epoch
     int32_t n_gray;        // mixed: candidates sent to the FP64 retest this round
     int32_t accepted_round;
     int64_t gray_total;    // mixed: FP64 retests over the run

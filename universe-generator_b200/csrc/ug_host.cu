@@ -801,7 +801,7 @@ int ug_batch_reset(void* h, const uint64_t* seeds) {
         CKR(cudaMemsetAsync(u.d.occ1, 0, (size_t)u.occ1_words * sizeof(uint32_t), B->st));
         const int32_t ep = B->hCtl[i].epoch;
         init_ctl(u.cfg, u.d, B->hCtl[i]);
-        B->hCtl[i].epoch = ep;  // round-hash entries of earlier epochs stay stale
+        B->hCtl[i].epoch = ep;  // round-table entries of earlier epochs stay stale
     }
     B->synced = false;
     CKR(cudaMemcpyAsync(B->dCtl, B->hCtl.data(), sizeof(UniCtl) * B->n, cudaMemcpyHostToDevice, B->st));
@@ -1070,7 +1070,7 @@ int ug_batch_restore(void* h, int32_t u, int64_t n, const int64_t* idx, const in
     if (rc) return rc;
     UniDev& d = U.d;
     const int T = U.cfg.T;
-    // clear the universe's grid, bitmaps and round hash
+    // clear the universe's grid, bitmaps and round table
     if (d.grid_kind == GRID_DENSE) {
         int64_t cpt = 1;
         for (int ax = 0; ax < d.dim; ax++) cpt *= d.gw;
@@ -1158,7 +1158,7 @@ int ug_batch_restore(void* h, int32_t u, int64_t n, const int64_t* idx, const in
     if (filled != saved.filled + saved.round_new)
         return fail(UG_EINVAL, "restore: rebuilt grid holds %lld cells, the state %lld (admissions do not match)",
                     (long long)filled, (long long)(saved.filled + saved.round_new));
-    // the saved block, with this batch's hash usage and round-hash epoch
+    // the saved block, with this batch's hash usage and round-table epoch
     saved.hash_used = k.hash_used;
     saved.epoch = epoch;
     B->hCtl[u] = saved;

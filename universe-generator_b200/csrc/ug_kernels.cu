@@ -10,7 +10,7 @@
 //   k_compact      survivors in candidate-index order (deterministic)
 //   k_surv_gen     FP64 coefficients of the survivors (term-ordered rows)
 //   k_surv_gemm    their FP64 trajectories as a register-tiled product
-//   k_surv_hash    round hash insert of every survivor timestep
+//   k_surv_hash    round-table insert of every survivor timestep
 //   k_conflicts    each survivor's contacts with EARLIER survivors of the round
 //   k_greedy       in-order resolution: survivor i is admitted iff it touches
 //                  no admitted earlier survivor (group rules in group modes)
@@ -656,7 +656,7 @@ __global__ void __launch_bounds__(128) k_surv_gemm(const UniDev* __restrict__ U,
     }
 }
 
-// Round hash block of a cell: 2^rblock_shift cells per axis (host-chosen per
+// Round-table block of a cell: 2^rblock_shift cells per axis (host-chosen per
 // universe, at least 2), so the 3 neighbour cells of a point span at most 2
 // blocks per axis (3 only at the seam of a partial last block).
 static_assert(2 * kMaxF <= 1024, "k_conflicts packs block coordinates in 10 bits");
@@ -665,7 +665,7 @@ __device__ __forceinline__ int rblock_gw(const UniDev& d) {
 }
 
 // k_surv_hash: one thread per survivor timestep inserts the point into the
-// round hash (key: epoch, t, block).
+// round table (entry: t, block; tagged with the epoch).
 __global__ void __launch_bounds__(256) k_surv_hash(const UniDev* __restrict__ U, UniCtl* ctl,
                                                    RoundInfo* info) {
     const int n_uni = info->n_uni, total = info->total_spt;
@@ -980,7 +980,7 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
             const int gw = d.gw, gwb = rblock_gw(d), rbs = d.rblock_shift;
             for (int t = lane; t < T; t += 32) {
                 const Pt64 P = d.spos[UG_IDX((int64_t)r * T + t, (int64_t)d.S_max * T)];
-                // distinct round-hash blocks of the 3 neighbour cells per axis:
+                // distinct round-table blocks of the 3 neighbour cells per axis:
                 // bl[ax] packs up to three 10-bit block coordinates, nbk[ax] counts them
                 // (registers only: every index below is a compile-time constant)
                 uint32_t bl[3] = {0u, 0u, 0u};
