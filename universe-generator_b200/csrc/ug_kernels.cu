@@ -1008,6 +1008,10 @@ __global__ void __launch_bounds__(128) k_conflicts(const UniDev* __restrict__ U,
                                                (int)((bl[2] >> (10 * i2)) & 1023u)};
                             int32_t r2 = rtab_head(d, c.epoch, t, lin_cell(bc, d.dim, gwb));
                             while (r2 >= 0) {
+                                if (r2 == r) {  // this survivor's own point: its link is in P
+                                    r2 = P.next;
+                                    continue;
+                                }
                                 const Pt64* Q = d.spos + UG_IDX((int64_t)r2 * T + t, (int64_t)d.S_max * T);
                                 if (r2 < r && pair_hit64(d, P.c, Q->c)) add(r2);
                                 r2 = Q->next;
