@@ -453,16 +453,14 @@ static int launch_round(Batch& B, bool timed) {
         tb(K_CONFIRM);
         k_gray_compact<<<B.n, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo, 0);
         // the retest: few candidates per round, a block of warps per candidate
-        k_confirm64w<kSurvWarps><<<B.nsm * 4, 32 * kSurvWarps, kConfSmemPerWarp, B.st>>>(B.dU, B.dCtl,
-                                                                                        B.dInfo, 0);
+        launch_confirm64w(0, B.nsm, B.dU, B.dCtl, B.dInfo, B.st);
         te(K_CONFIRM);
     } else {
         // the FP64 form: every candidate of the round, one warp per candidate
         // (coefficients in shared memory, lanes over timesteps in endpoint-first order)
         tb(K_PRE);
         k_gray_compact<<<B.n, 256, 0, B.st>>>(B.dU, B.dCtl, B.dInfo, 1);
-        k_confirm64w<1><<<B.nsm * 4, 32 * kSurvWarps, kSurvWarps * kConfSmemPerWarp, B.st>>>(B.dU, B.dCtl,
-                                                                                              B.dInfo, 1);
+        launch_confirm64w(1, B.nsm, B.dU, B.dCtl, B.dInfo, B.st);
         te(K_PRE);
     }
     tb(K_COMPACT);
@@ -730,10 +728,7 @@ int ug_batch_create(const ug_universe_cfg* cfgs, int32_t n, const ug_run_opts* o
     if (B->any_mixed && (rc = mixed_init_kernels())) return bail(rc);
     B->kernels_per_round = B->any_mixed ? 11 : 10;
     // the warp FP64 test serves both forms (all candidates, or the undecided ones)
-    if (cudaFuncSetAttribute(k_confirm64w<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(kSurvWarps * kConfSmemPerWarp)) != cudaSuccess ||
-        cudaFuncSetAttribute(k_confirm64w<kSurvWarps>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kConfSmemPerWarp) != cudaSuccess)
+    if (confirm64w_set_smem() != cudaSuccess)
         return bail(fail(UG_ECUDA, "smem attribute failed"));
     // one wave per SM, measured on c3 against 8 / 8 / 16 CTAs per SM: k_surv_gen 27.7 ->
     // 24.5 ms, k_surv_hash 33.5 -> 32.0 ms, k_conflicts 85.5 -> 80.2 ms per job.  k_commit

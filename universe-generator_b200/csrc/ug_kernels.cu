@@ -915,8 +915,22 @@ __global__ void __maxnreg__(128) k_confirm64w(const UniDev* __restrict__ U,
         group_sync<WPI>();
     }
 }
-template __global__ void k_confirm64w<1>(const UniDev* __restrict__, UniCtl*, RoundInfo*, int);
-template __global__ void k_confirm64w<kSurvWarps>(const UniDev* __restrict__, UniCtl*, RoundInfo*, int);
+
+cudaError_t confirm64w_set_smem() {
+    cudaError_t e = cudaFuncSetAttribute(k_confirm64w<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(kSurvWarps * kConfSmemPerWarp));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_confirm64w<kSurvWarps>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kConfSmemPerWarp);
+    return e;
+}
+
+void launch_confirm64w(int all, int nsm, const UniDev* U, UniCtl* ctl, RoundInfo* info, cudaStream_t st) {
+    if (all)
+        k_confirm64w<1><<<nsm * 4, 32 * kSurvWarps, kSurvWarps * kConfSmemPerWarp, st>>>(U, ctl, info, 1);
+    else
+        k_confirm64w<kSurvWarps><<<nsm * 4, 32 * kSurvWarps, kConfSmemPerWarp, st>>>(U, ctl, info, 0);
+}
 
 // One warp per survivor r: the set of earlier survivors r' < r that it
 // touches (Chebyshev contact at any timestep; plus crossings in 1+1D).

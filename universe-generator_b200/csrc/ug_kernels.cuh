@@ -53,8 +53,11 @@ __device__ __forceinline__ int find_uni(const int32_t* off, int n, int item) {
 // Kernels (ug_kernels.cu)
 __global__ void k_plan(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_gray_compact(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info, int all);
-template <int WPI>
-__global__ void k_confirm64w(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info, int all);
+// The FP64 test of undecided candidates (k_confirm64w, a template kept inside
+// ug_kernels.cu): every candidate of the round (all = 1, a warp per candidate) or
+// the mixed form's retest (all = 0, a block per candidate).
+cudaError_t confirm64w_set_smem();
+void launch_confirm64w(int all, int nsm, const UniDev* U, UniCtl* ctl, RoundInfo* info, cudaStream_t st);
 __global__ void k_compact(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
 __global__ void k_surv_gen(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info, int warp_bytes);
 __global__ void k_surv_gemm(const UniDev* __restrict__ U, UniCtl* ctl, RoundInfo* info);
