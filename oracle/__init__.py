@@ -70,12 +70,18 @@ class _Result(C.Structure):
 
 _lib = None
 
+# Where the checkers read the reference's sources: UG_REFERENCE, else the default of
+# the build recipe in this folder's Makefile.  Only this module, the Makefile and the
+# test infrastructure that imports REFERENCE_DIR (parity tests, fixture generators)
+# read the reference; nothing in the package does.
+REFERENCE_DIR = os.environ.get("UG_REFERENCE", "/root/reference")
+
 
 def build() -> None:
     """Compile libug_oracle.so (and the reference checkers when the tree exists)."""
     subprocess.run(["make", "-s", "-C", HERE, "libug_oracle.so"], check=True)
-    if os.path.isdir(os.environ.get("UG_REFERENCE", "/root/reference") + "/cuda"):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    if os.path.isdir(REFERENCE_DIR + "/cuda"):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "UG_REFERENCE=" + REFERENCE_DIR], check=True)
 
 
 def lib():

@@ -19,7 +19,10 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("UG_REFERENCE", "/root/reference")
+ROOT_ = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+if ROOT_ not in sys.path:
+    sys.path.insert(0, ROOT_)
+from oracle import REFERENCE_DIR as REF  # noqa: E402
 
 RUN = r"""
 import json, sys

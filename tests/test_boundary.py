@@ -12,7 +12,7 @@ import sys
 import numpy as np
 import pytest
 
-REF = os.environ.get("UG_REFERENCE", "/root/reference")
+from oracle import REFERENCE_DIR as REF  # noqa: E402
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(ROOT, "universe-generator_b200")
 

@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden", "view_reference.json")
-REF = os.environ.get("UG_REFERENCE", "/root/reference")
+from oracle import REFERENCE_DIR as REF  # noqa: E402
 
 
 def test_oracle_matches_reference_golden(oracle):
