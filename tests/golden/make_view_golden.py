@@ -19,9 +19,9 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-ROOT_ = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
-if ROOT_ not in sys.path:
-    sys.path.insert(0, ROOT_)
+ROOT = os.path.dirname(os.path.dirname(HERE))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
 from oracle import REFERENCE_DIR as REF  # noqa: E402
 
 RUN = r"""
